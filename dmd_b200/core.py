@@ -1,0 +1,296 @@
+"""SimulationConfig and Engine -- the drop-in for the reference's pybind module
+``_dmd_core`` (python/dmd/core.cpp:97-430).
+
+``SimulationConfig`` keeps the same attribute names, defaults
+(src/sim/simulation_config.h:27-84) and numpy-array properties as the pybind
+class.  ``Engine`` keeps the EngineWrapper surface (run, run_n, positions,
+velocities, forces, potential_energy, current_step, current_time, box_size,
+n_atoms; python/dmd/core.cpp:417-428) but holds all state on the GPU: run_n(k)
+is ONE call into the C ABI that advances k steps on the device, and the
+getters copy from device memory.
+
+Backend options are keyword arguments (or DMD_PRECISION / DMD_PROFILE /
+DMD_SKIN / DMD_DEVICE environment variables) because the strict config.json
+schema admits no extra keys.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import os
+
+import numpy as np
+
+from . import _capi
+
+
+class ThermostatConfig:
+    """src/sim/simulation_config.h:11-16"""
+
+    def __init__(self):
+        self.type = "none"
+        self.temperature = 300.0
+        self.tau = 0.1
+        self.frequency = 10.0
+
+
+class BarostatConfig:
+    """src/sim/simulation_config.h:18-23"""
+
+    def __init__(self):
+        self.type = "none"
+        self.pressure = 1.0
+        self.tau = 1.0
+        self.compressibility = 4.5e-5
+
+
+def _f64(a):
+    return np.ascontiguousarray(np.asarray(a, dtype=np.float64).ravel())
+
+
+def _i32(a):
+    return np.ascontiguousarray(np.asarray(a, dtype=np.int32).ravel())
+
+
+class SimulationConfig:
+    """Same fields and defaults as the reference's SimulationConfig."""
+
+    _F64 = ("masses", "charges", "pos_x", "pos_y", "pos_z", "vel_x", "vel_y", "vel_z",
+            "lj_sigma", "lj_epsilon", "bond_k", "bond_r0", "angle_k_theta", "angle_theta0",
+            "dihedral_k_phi", "dihedral_phi0", "improper_k_phi", "improper_phi0")
+    _I32 = ("atom_types", "bond_i", "bond_j", "angle_i", "angle_j", "angle_k", "dihedral_i",
+            "dihedral_j", "dihedral_k", "dihedral_l", "dihedral_periodicity", "improper_i",
+            "improper_j", "improper_k", "improper_l")
+
+    def __init__(self):
+        object.__setattr__(self, "_arrays", {})
+        self.dt = 0.002
+        self.n_steps = 1000
+        self.init_temperature = 300.0
+        self.gen_vel = False
+        self.seed = 42
+        self.box_size = 3.0
+        self.lj_cutoff = 1.2
+        self.use_lj = False
+        self.coulomb_type = "cutoff"
+        self.coulomb_cutoff = 1.2
+        self.pme_order = 4
+        self.pme_grid_spacing = 0.12
+        self.ewald_coeff = 0.34
+        self.trajectory_path = "trajectory.h5"
+        self.nstxout = 0
+        self.nstvout = 0
+        self.nstenergy = 10
+        self.energy_path = "energy.h5"
+        self.checkpoint_interval = 500
+        self.checkpoint_path = "checkpoint.bin"
+        self.thermostat = ThermostatConfig()
+        self.barostat = BarostatConfig()
+        self.constraint_type = "none"
+        self.constraint_tolerance = 1e-6
+        self.constraint_i = []
+        self.constraint_j = []
+        self.constraint_dist = []
+        self.excl_i = []
+        self.excl_j = []
+        for k in self._F64:
+            self._arrays[k] = np.zeros(0, np.float64)
+        for k in self._I32:
+            self._arrays[k] = np.zeros(0, np.int32)
+
+    def __getattr__(self, name):
+        arrays = object.__getattribute__(self, "_arrays")
+        if name in arrays:
+            return arrays[name]
+        if name == "mass":
+            return arrays["masses"]
+        raise AttributeError(name)
+
+    def __setattr__(self, name, value):
+        if name == "mass":
+            name = "masses"
+        if name in self._F64:
+            self._arrays[name] = _f64(value)
+        elif name in self._I32:
+            self._arrays[name] = _i32(value)
+        else:
+            object.__setattr__(self, name, value)
+
+    @property
+    def lj_n_types(self) -> int:
+        """n_types = sqrt(len(lj_sigma)) as the pybind setter derives it (core.cpp:196-205)."""
+        return int(math.isqrt(len(self._arrays["lj_sigma"]))) if len(self._arrays["lj_sigma"]) else 0
+
+
+def _options(precision=None, profile=None, skin=None, device=None, rng_seed=None):
+    precision = precision or os.environ.get("DMD_PRECISION", "mixed")
+    profile = profile or os.environ.get("DMD_PROFILE", "ref")
+    if skin is None:
+        skin = float(os.environ.get("DMD_SKIN", "0.1"))
+    if device is None:
+        device = int(os.environ.get("DMD_DEVICE", "0"))
+    if precision not in _capi.PRECISIONS:
+        raise ValueError(f"precision must be one of {list(_capi.PRECISIONS)}")
+    if profile not in _capi.PROFILES:
+        raise ValueError(f"profile must be one of {list(_capi.PROFILES)}")
+    o = _capi.dmdgpu_options()
+    o.profile = _capi.PROFILES[profile]
+    o.precision = _capi.PRECISIONS[precision]
+    o.skin = float(skin)
+    o.device = int(device)
+    o.rng_seed = int(rng_seed if rng_seed is not None else 0x5EED)
+    return o
+
+
+class DmdGpuError(RuntimeError):
+    """A non-zero status from the C ABI (status code in ``.code``)."""
+
+    def __init__(self, code, msg):
+        super().__init__(f"[{_capi.ERR_NAMES.get(code, code)}] {msg}")
+        self.code = code
+
+
+class Engine:
+    """GPU-resident SimulationEngine with the EngineWrapper interface."""
+
+    def __init__(self, cfg: SimulationConfig, precision=None, profile=None, skin=None,
+                 device=None, rng_seed=None):
+        self._lib = _capi.lib()
+        self._desc = _capi.SystemDesc(cfg)
+        self._opt = _options(precision, profile, skin, device, rng_seed)
+        h = C.c_void_p()
+        rc = self._lib.dmdgpu_create(C.byref(self._desc.s), C.byref(self._opt), C.byref(h))
+        if rc != 0:
+            msg = self._lib.dmdgpu_last_error(h)
+            if h:
+                self._lib.dmdgpu_destroy(h)
+            raise DmdGpuError(rc, (msg or b"dmdgpu_create failed").decode())
+        self._h = h
+        self._n = int(len(cfg.masses))
+        self._box0 = float(cfg.box_size)
+        self._n_steps = int(cfg.n_steps)
+        self.precision = precision or os.environ.get("DMD_PRECISION", "mixed")
+        self.profile = profile or os.environ.get("DMD_PROFILE", "ref")
+
+    # -- lifecycle ---------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.dmdgpu_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc):
+        if rc != 0:
+            raise DmdGpuError(rc, (self._lib.dmdgpu_last_error(self._h) or b"").decode())
+
+    # -- EngineWrapper surface --------------------------------------------
+    def run(self):
+        self._check(self._lib.dmdgpu_run(self._h))
+
+    def run_n(self, steps: int):
+        self._check(self._lib.dmdgpu_step(self._h, int(steps)))
+
+    def _state(self, which):
+        x = np.empty(self._n)
+        y = np.empty(self._n)
+        z = np.empty(self._n)
+        self._check(self._lib.dmdgpu_get_state(self._h, which, _capi.dptr(x), _capi.dptr(y),
+                                               _capi.dptr(z)))
+        return np.stack([x, y, z], axis=1)
+
+    @property
+    def positions(self):
+        return self._state(0)
+
+    @property
+    def velocities(self):
+        return self._state(1)
+
+    @property
+    def forces(self):
+        return self._state(2)
+
+    def scalars(self) -> _capi.dmdgpu_scalars:
+        s = _capi.dmdgpu_scalars()
+        self._check(self._lib.dmdgpu_get_scalars(self._h, C.byref(s)))
+        return s
+
+    @property
+    def potential_energy(self) -> float:
+        return self.scalars().potential_energy
+
+    @property
+    def current_step(self) -> int:
+        return int(self.scalars().step)
+
+    @property
+    def current_time(self) -> float:
+        return self.scalars().time
+
+    @property
+    def box_size(self) -> float:
+        # EngineWrapper returns the construction box (python/dmd/core.cpp:23, :46)
+        return self._box0
+
+    @property
+    def n_atoms(self) -> int:
+        return self._n
+
+    # -- extensions (device single-point API, state I/O, checkpoints) -----
+    def energy_terms(self) -> dict:
+        s = self.scalars()
+        return {k: s.e_terms[i] for i, k in enumerate(_capi.E_TERMS)}
+
+    def set_positions(self, pos):
+        pos = np.asarray(pos, dtype=np.float64)
+        x, y, z = (np.ascontiguousarray(pos[:, k]) for k in range(3))
+        self._check(self._lib.dmdgpu_set_state(self._h, 0, _capi.dptr(x), _capi.dptr(y), _capi.dptr(z)))
+
+    def set_velocities(self, vel):
+        vel = np.asarray(vel, dtype=np.float64)
+        x, y, z = (np.ascontiguousarray(vel[:, k]) for k in range(3))
+        self._check(self._lib.dmdgpu_set_state(self._h, 1, _capi.dptr(x), _capi.dptr(y), _capi.dptr(z)))
+
+    def compute_forces(self):
+        """Single-point forces (N x 3) and energy terms at the current positions."""
+        fx, fy, fz = np.empty(self._n), np.empty(self._n), np.empty(self._n)
+        e = np.zeros(8)
+        self._check(self._lib.dmdgpu_compute_forces(self._h, _capi.dptr(fx), _capi.dptr(fy),
+                                                    _capi.dptr(fz), _capi.dptr(e)))
+        return np.stack([fx, fy, fz], axis=1), dict(zip(_capi.E_TERMS, e))
+
+    def component_compute(self, component: int, pos, box, forces=None, energy=0.0):
+        """ForceComponent::compute: accumulate one component's forces/energy."""
+        pos = np.asarray(pos, dtype=np.float64)
+        x, y, z = (np.ascontiguousarray(pos[:, k]) for k in range(3))
+        if forces is None:
+            forces = np.zeros((self._n, 3))
+        fx, fy, fz = (np.ascontiguousarray(forces[:, k]) for k in range(3))
+        e = C.c_double(energy)
+        self._check(self._lib.dmdgpu_component_compute(
+            self._h, int(component), _capi.dptr(x), _capi.dptr(y), _capi.dptr(z), float(box),
+            _capi.dptr(fx), _capi.dptr(fy), _capi.dptr(fz), C.byref(e)))
+        return np.stack([fx, fy, fz], axis=1), e.value
+
+    def pair_list(self):
+        cnt = C.c_int64()
+        self._check(self._lib.dmdgpu_pair_list(self._h, None, None, 0, C.byref(cnt)))
+        pi = np.empty(cnt.value, np.int32)
+        pj = np.empty(cnt.value, np.int32)
+        self._check(self._lib.dmdgpu_pair_list(self._h, _capi.iptr(pi), _capi.iptr(pj), cnt.value,
+                                               C.byref(cnt)))
+        return pi, pj
+
+    def save_checkpoint(self, path: str):
+        self._check(self._lib.dmdgpu_save_checkpoint(self._h, path.encode()))
+
+    def load_checkpoint(self, path: str):
+        self._check(self._lib.dmdgpu_load_checkpoint(self._h, path.encode()))
+
+    def kernel_launches(self) -> int:
+        return int(self._lib.dmdgpu_kernel_launches(self._h))

@@ -1,0 +1,220 @@
+/*
+ * dmdgpu.h -- C ABI of the B200 (sm_100a) implementation of DMD's per-step
+ * force-and-integrate path.
+ *
+ * Plain C: POD descriptors, plain pointers and sizes, int status codes, no
+ * exceptions and no torch types across the boundary.  Every array passed in
+ * is owned by the caller and copied during the call.  A context owns its
+ * device memory, CUDA stream, cuFFT plans and CUDA graphs.  Calls on one
+ * context are not re-entrant; distinct contexts are independent.
+ *
+ * Units are the reference's: nm, ps, amu, kJ/mol, e, K; k_B = 0.008314462618
+ * kJ mol^-1 K^-1, k_e = 138.935456 kJ mol^-1 nm e^-2.
+ */
+#ifndef DMDGPU_H
+#define DMDGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  1..5 mirror ForceError (src/core/error.h:6-12); a non-zero
+ * status leaves a message in dmdgpu_last_error(). */
+enum {
+    DMDGPU_OK = 0,
+    DMDGPU_ERR_NAN = 1,            /* ForceError::NaN: non-finite force/energy seen on device */
+    DMDGPU_ERR_BOND_EXPLOSION = 2, /* ForceError::BondExplosion: fixed-point force range exceeded */
+    DMDGPU_ERR_MISMATCH = 3,       /* ForceError::Mismatch: array sizes / checkpoint disagree */
+    DMDGPU_ERR_PARM = 4,           /* ForceError::ParmError: invalid parameter */
+    DMDGPU_ERR_GPU = 5,            /* ForceError::GPUError: CUDA / cuFFT failure */
+    DMDGPU_ERR_OOM = 6,            /* device allocation failed */
+    DMDGPU_ERR_BUDGET = 7,         /* batch admission: HBM budget or slot table full */
+    DMDGPU_ERR_INVALID = 8,        /* bad handle / call order */
+    DMDGPU_ERR_CAPACITY = 9        /* neighbour-list capacity exceeded on device */
+};
+
+/* coulomb_type (SimulationConfig::coulomb_type, src/sim/simulation_config.h:62) */
+enum { DMDGPU_COULOMB_CUTOFF = 0, /* "cutoff" / "direct" */ DMDGPU_COULOMB_PME = 1 };
+/* ThermostatConfig::type (src/sim/simulation_config.h:11-16) */
+enum { DMDGPU_THERMO_NONE = 0, DMDGPU_THERMO_BERENDSEN = 1, DMDGPU_THERMO_NOSE_HOOVER = 2,
+       DMDGPU_THERMO_ANDERSEN = 3 };
+/* BarostatConfig::type (src/sim/simulation_config.h:18-23); "andersen" is not on this path */
+enum { DMDGPU_BARO_NONE = 0, DMDGPU_BARO_BERENDSEN = 1 };
+/* Semantic profile: REF reproduces the reference's formulas (quirks included);
+ * PHYS uses gradient-consistent forces (skin list, erfc real space with
+ * exclusions, textbook SPME, analytic bonded gradients, atomic virial). */
+enum { DMDGPU_PROFILE_REF = 0, DMDGPU_PROFILE_PHYS = 1 };
+/* MIXED: FP32 pair/mesh/bonded arithmetic, int64 fixed-point force accumulation,
+ * FP64 integration and reductions.  FP64: every stage in FP64. */
+enum { DMDGPU_PRECISION_MIXED = 0, DMDGPU_PRECISION_FP64 = 1 };
+
+/*
+ * System + run description.  Mirrors SimulationConfig
+ * (src/sim/simulation_config.h:27-84) as filled by SystemBuilder/apply_config
+ * (python/dmd/system.py, python/dmd/config.py): a cubic box, per-atom SoA
+ * arrays, one bond / angle / dihedral term set each.  vel_* may be NULL (zero
+ * velocities); atom_types may be NULL (all type 0).
+ */
+typedef struct dmdgpu_system {
+    int32_t n_atoms;
+    double box_size;
+    const double *masses, *charges;
+    const double *pos_x, *pos_y, *pos_z;
+    const double *vel_x, *vel_y, *vel_z;
+    const int32_t *atom_types;
+    /* Lennard-Jones: n_types x n_types row-major sigma / epsilon */
+    int32_t use_lj, lj_n_types;
+    const double *lj_sigma, *lj_epsilon;
+    double lj_cutoff;
+    /* bonded terms */
+    int32_t n_bonds;
+    const int32_t *bond_i, *bond_j;
+    const double *bond_k, *bond_r0;
+    int32_t n_angles;
+    const int32_t *angle_i, *angle_j, *angle_k;
+    const double *angle_k_theta, *angle_theta0;
+    int32_t n_dihedrals;
+    const int32_t *dihedral_i, *dihedral_j, *dihedral_k, *dihedral_l, *dihedral_periodicity;
+    const double *dihedral_k_phi, *dihedral_phi0;
+    int32_t n_impropers; /* must be 0: harmonic impropers are not on this path */
+    /* electrostatics */
+    int32_t coulomb_type;
+    double coulomb_cutoff, ewald_coeff, pme_grid_spacing;
+    int32_t pme_order;
+    /* exclusions (1-2, 1-3, 1-4 pairs) */
+    int32_t n_excl;
+    const int32_t *excl_i, *excl_j;
+    /* run control */
+    double dt;
+    int32_t n_steps, gen_vel, seed;
+    double init_temperature;
+    int32_t thermostat_type;
+    double thermo_temperature, thermo_tau, thermo_frequency;
+    int32_t barostat_type;
+    double baro_pressure, baro_tau, baro_compressibility;
+    int32_t constraint_type; /* must be 0 ("none"): SHAKE/RATTLE are not on this path */
+    int32_t checkpoint_interval;
+    const char *checkpoint_path; /* may be NULL */
+} dmdgpu_system;
+
+typedef struct dmdgpu_options {
+    int32_t profile;    /* DMDGPU_PROFILE_* */
+    int32_t precision;  /* DMDGPU_PRECISION_* */
+    double skin;        /* Verlet skin (nm), PHYS only; REF uses the reference's no-skin list */
+    int32_t device;     /* CUDA device ordinal */
+    uint64_t rng_seed;  /* PHYS Andersen thermostat stream key */
+} dmdgpu_options;
+
+/* Scalars of the last force evaluation / current state. */
+typedef struct dmdgpu_scalars {
+    int64_t step;
+    double time;
+    double potential_energy; /* SystemData::potential_energy after the last evaluation */
+    double box;
+    double kinetic_energy, temperature, pressure, virial;
+    double zeta;             /* Nose-Hoover friction */
+    /* energy terms: lj, coul_real, coul_recip, coul_self, coul_excl, bond, angle, dihedral */
+    double e_terms[8];
+    int64_t list_builds;
+    int32_t lj_step_since_rebuild; /* LennardJones::step_since_rebuild (REF cadence) */
+    int32_t status;
+} dmdgpu_scalars;
+
+typedef struct dmdgpu_ctx dmdgpu_ctx;
+
+/* Replaces build_simulation (src/sim/simulation_engine.cpp:248-386) +
+ * EngineWrapper::EngineWrapper (python/dmd/core.cpp:21-25).  Velocities are
+ * generated as the reference does when gen_vel != 0 (std::mt19937(seed),
+ * std::normal_distribution, COM removal, rescale; simulation_engine.cpp:339-383). */
+int dmdgpu_create(const dmdgpu_system *sys, const dmdgpu_options *opt, dmdgpu_ctx **out);
+
+/* Replaces SimulationEngine::step x n (src/sim/simulation_engine.cpp:53-86) and
+ * EngineWrapper::run_n (python/dmd/core.cpp:29-44): n steps on the device, one call. */
+int dmdgpu_step(dmdgpu_ctx *ctx, int32_t n_steps);
+
+/* Replaces SimulationEngine::run (simulation_engine.cpp:88-106): n_steps steps with
+ * a checkpoint every checkpoint_interval steps (when a path is set). */
+int dmdgpu_run(dmdgpu_ctx *ctx);
+
+/* State copies in the reference's atom order.  which: 0 positions, 1 velocities,
+ * 2 forces (of the last evaluation).  Replaces the EngineWrapper getters
+ * positions / velocities / forces (python/dmd/core.cpp:49-90). */
+int dmdgpu_get_state(dmdgpu_ctx *ctx, int32_t which, double *x, double *y, double *z);
+/* Overwrite positions (which=0) or velocities (which=1). */
+int dmdgpu_set_state(dmdgpu_ctx *ctx, int32_t which, const double *x, const double *y,
+                     const double *z);
+int dmdgpu_get_scalars(dmdgpu_ctx *ctx, dmdgpu_scalars *out);
+
+/* Single-point evaluation of every component at the current positions
+ * (ForceEngine::compute, src/force/force_engine.cpp:10-25) with a freshly built
+ * list.  Forces are written (not accumulated); e_terms receives 8 doubles
+ * (see dmdgpu_scalars.e_terms) and may be NULL. */
+int dmdgpu_compute_forces(dmdgpu_ctx *ctx, double *fx, double *fy, double *fz, double *e_terms);
+
+/* One force component at caller positions, accumulated into caller arrays --
+ * the ForceComponent::compute contract (src/force/force_component.h:12-21):
+ * forces are added (never zeroed) and the energy is added to *energy.
+ * component: 0 LennardJones, 1 HarmonicBond, 2 HarmonicAngle, 3 PeriodicDihedral,
+ * 4 CoulombDirect (real-space Ewald), 5 CoulombPME (reciprocal + self),
+ * 6 CoulombExclusion.  The context's own positions are left unchanged. */
+int dmdgpu_component_compute(dmdgpu_ctx *ctx, int32_t component, const double *pos_x,
+                             const double *pos_y, const double *pos_z, double box,
+                             double *forces_x, double *forces_y, double *forces_z,
+                             double *energy);
+
+/* The current short-range pair list as sorted (i<j) atom pairs: REF = the
+ * LennardJones list (pairs within lj_cutoff at the last rebuild,
+ * lennard_jones.cpp:18-41); PHYS = pairs within max cutoff + skin, exclusions
+ * removed.  Copies min(count, cap) pairs; *count receives the total. */
+int dmdgpu_pair_list(dmdgpu_ctx *ctx, int32_t *pi, int32_t *pj, int64_t cap, int64_t *count);
+
+/* Binary checkpoint v1 (src/sim/checkpoint.cpp:9-75) plus a trailer the v1
+ * reader ignores (box, Nose-Hoover zeta, thermostat call counter, profile).
+ * Replaces SimulationEngine::save_checkpoint / load_checkpoint (:108-137). */
+int dmdgpu_save_checkpoint(dmdgpu_ctx *ctx, const char *path);
+int dmdgpu_load_checkpoint(dmdgpu_ctx *ctx, const char *path);
+
+/* Device bytes a context for this system would hold (admission accounting). */
+int64_t dmdgpu_footprint_bytes(const dmdgpu_system *sys, const dmdgpu_options *opt);
+
+/* Kernel launches issued by this context so far (this library's own kernels). */
+int64_t dmdgpu_kernel_launches(dmdgpu_ctx *ctx);
+
+const char *dmdgpu_last_error(const dmdgpu_ctx *ctx);
+void dmdgpu_destroy(dmdgpu_ctx *ctx);
+
+/* ---------------------------------------------------------------------------
+ * Batched replicas and continuous serving.  A batch packs many independent
+ * systems ("slots") into one device table; one dmdgpu_batch_step advances every
+ * running slot with the same kernel launches.  Slots are admitted while the
+ * HBM budget allows and released when done; results of a slot do not depend
+ * on which other slots share the batch.  No counterpart in the reference
+ * (which is one SimulationEngine per process).
+ * ------------------------------------------------------------------------- */
+typedef struct dmdgpu_batch dmdgpu_batch;
+
+int dmdgpu_batch_create(int64_t budget_bytes, const dmdgpu_options *opt, dmdgpu_batch **out);
+/* Admit a system to run n_steps steps; *slot receives its id.  Returns
+ * DMDGPU_ERR_BUDGET (nothing admitted) when it does not fit. */
+int dmdgpu_batch_admit(dmdgpu_batch *b, const dmdgpu_system *sys, int64_t n_steps, int32_t *slot);
+/* Advance every running slot by up to n_steps (a slot stops at its own n_steps). */
+int dmdgpu_batch_step(dmdgpu_batch *b, int32_t n_steps);
+/* Slots that finished since the last poll: copies up to cap ids into slots. */
+int dmdgpu_batch_poll(dmdgpu_batch *b, int32_t *slots, int32_t cap, int32_t *n_done);
+int dmdgpu_batch_get_state(dmdgpu_batch *b, int32_t slot, int32_t which, double *x, double *y,
+                           double *z);
+int dmdgpu_batch_get_scalars(dmdgpu_batch *b, int32_t slot, dmdgpu_scalars *out);
+int dmdgpu_batch_release(dmdgpu_batch *b, int32_t slot);
+int64_t dmdgpu_batch_used_bytes(dmdgpu_batch *b);
+int32_t dmdgpu_batch_active(dmdgpu_batch *b);
+const char *dmdgpu_batch_last_error(const dmdgpu_batch *b);
+void dmdgpu_batch_destroy(dmdgpu_batch *b);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DMDGPU_H */
