@@ -71,7 +71,8 @@ class dmdgpu_scalars(C.Structure):
                 ("box", C.c_double), ("kinetic_energy", C.c_double), ("temperature", C.c_double),
                 ("pressure", C.c_double), ("virial", C.c_double), ("zeta", C.c_double),
                 ("e_terms", C.c_double * 8), ("list_builds", C.c_int64),
-                ("lj_step_since_rebuild", C.c_int32), ("status", C.c_int32)]
+                ("lj_step_since_rebuild", C.c_int32), ("status", C.c_int32),
+                ("list_chunks", C.c_int64)]
 
 
 _lib = None

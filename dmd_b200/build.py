@@ -1,0 +1,57 @@
+"""Build libdmdgpu.so in-tree with nvcc for sm_100a (B200).
+
+    python -m dmd_b200.build
+
+Each .cu translation unit is compiled in parallel to an object file under
+dmd_b200/_build/, then linked with cuFFT into dmd_b200/libdmdgpu.so.
+"""
+from __future__ import annotations
+
+import concurrent.futures as cf
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+OUT = os.path.join(HERE, "libdmdgpu.so")
+BUILD = os.path.join(HERE, "_build")
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
+         "-Xptxas", "-warn-spills"]
+SOURCES = ["k_list.cu", "k_nonbonded.cu", "k_forces.cu", "k_integrate.cu", "engine.cu", "capi.cu"]
+
+
+def _compile(src: str) -> str:
+    obj = os.path.join(BUILD, src.replace(".cu", ".o"))
+    inp = os.path.join(CSRC, src)
+    deps = [inp] + [os.path.join(CSRC, h) for h in os.listdir(CSRC) if h.endswith((".h", ".cuh"))]
+    deps.append(os.path.join(os.path.dirname(HERE), "include", "dmdgpu.h"))
+    if os.path.exists(obj) and all(os.path.getmtime(obj) >= os.path.getmtime(d) for d in deps):
+        return obj
+    cmd = [NVCC, *ARCH, *FLAGS, "-c", inp, "-o", obj]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"nvcc failed for {src}:\n{r.stdout}\n{r.stderr}")
+    return obj
+
+
+def build(verbose: bool = False) -> str:
+    os.makedirs(BUILD, exist_ok=True)
+    with cf.ThreadPoolExecutor(max_workers=len(SOURCES)) as ex:
+        objs = list(ex.map(_compile, SOURCES))
+    if os.path.exists(OUT) and all(os.path.getmtime(OUT) >= os.path.getmtime(o) for o in objs):
+        return OUT
+    cmd = [NVCC, *ARCH, "-shared", "-o", OUT, *objs, "-lcufft", "-lcudart"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
+    if verbose:
+        print("built", OUT)
+    return OUT
+
+
+if __name__ == "__main__":
+    build(verbose=True)
+    sys.exit(0)

@@ -1,0 +1,1443 @@
+// engine.cu -- host orchestration of the device path.
+//
+// A Batch owns one packed device table of replicas (a single system is a batch
+// of one).  It replaces, on the host side, build_simulation / build_force_engine
+// (src/sim/simulation_engine.cpp:147-386), SimulationEngine::step / run
+// (:53-106) and checkpoint save / load (src/sim/checkpoint.cpp).  Steps are
+// issued as CUDA graphs; run_n(k) is k graph replays with no host sync in
+// between.
+#include <cuda_runtime.h>
+#include <cufft.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <random>
+#include <stdexcept>
+
+#include "engine.h"
+#include "launch.h"
+
+namespace dmd {
+
+DeviceArena::~DeviceArena() {
+    for (void* p : ptrs) cudaFree(p);
+}
+
+template <typename T>
+T* DeviceArena::alloc(size_t n) {
+    if (n == 0) n = 1;
+    void* p = nullptr;
+    if (cudaMalloc(&p, n * sizeof(T)) != cudaSuccess) {
+        throw std::runtime_error("cudaMalloc failed");
+    }
+    cudaMemset(p, 0, n * sizeof(T));
+    ptrs.push_back(p);
+    bytes += n * sizeof(T);
+    return static_cast<T*>(p);
+}
+
+namespace {
+
+template <typename T>
+std::vector<T> vec_of(const T* p, int n) {
+    if (!p || n <= 0) return {};
+    return std::vector<T>(p, p + n);
+}
+
+// Sort grid: square x-y columns 1.2x the edge of a 32-atom cube, z slabs of
+// 0.1 nm; columns and slabs are visited in a snake order (see vox_rank), so
+// 32 consecutive atoms are a compact tile.
+void sort_grid(int n, double L, int& nvx, int& nvz) {
+    const double rho = n / (L * L * L);
+    const double a = 1.2 * std::cbrt(32.0 / std::max(rho, 1e-12));
+    nvx = std::min(std::max(static_cast<int>(std::floor(L / a)), 1), 256);
+    nvz = std::min(std::max(static_cast<int>(std::floor(L / 0.1)), 1), 1024);
+}
+
+}  // namespace
+
+Batch::Batch(const dmdgpu_options& opt, long long budget) : opt_(opt), budget_(budget) {
+    fp64_ = opt.precision == DMDGPU_PRECISION_FP64;
+    phys_ = opt.profile == DMDGPU_PROFILE_PHYS;
+    device_ = opt.device;
+    if (cudaSetDevice(device_) != cudaSuccess) throw std::runtime_error("cudaSetDevice failed");
+    cudaDeviceGetAttribute(&n_sm_, cudaDevAttrMultiProcessorCount, device_);
+    if (cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&body_stream_, cudaStreamNonBlocking) != cudaSuccess)
+        throw std::runtime_error("cudaStreamCreate failed");
+}
+
+Batch::~Batch() {
+    cudaSetDevice(device_);
+    free_device();
+    for (cudaEvent_t e : ev_pool_) cudaEventDestroy(e);
+    if (body_stream_) cudaStreamDestroy(body_stream_);
+    if (stream_) cudaStreamDestroy(stream_);
+}
+
+void Batch::free_device() {
+    if (stream_) cudaStreamSynchronize(stream_);
+    if (graph_) cudaGraphExecDestroy(graph_);
+    graph_ = nullptr;
+    for (auto& kv : plans_) {
+        cufftDestroy(kv.second.first);
+        cufftDestroy(kv.second.second);
+    }
+    plans_.clear();
+    arena_.reset();
+    if (h_st_) cudaFreeHost(h_st_);
+    h_st_ = nullptr;
+    if (h_and_flag_) cudaFreeHost(h_and_flag_);
+    if (h_and_v_) cudaFreeHost(h_and_v_);
+    h_and_flag_ = nullptr;
+    h_and_v_ = nullptr;
+    packed_ = false;
+    used_bytes_ = 0;
+}
+
+int Batch::fail(int code, const std::string& msg) {
+    err_ = msg;
+    return code;
+}
+
+int Batch::check_cuda(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return DMDGPU_OK;
+    return fail(DMDGPU_ERR_GPU, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define CK(call)                                                   \
+    do {                                                           \
+        int rc__ = check_cuda((call), #call);                      \
+        if (rc__) return rc__;                                     \
+    } while (0)
+
+// ---------------------------------------------------------------------------
+// Host replica construction (build_simulation, simulation_engine.cpp:248-386)
+// ---------------------------------------------------------------------------
+int Batch::build_host(HostRep& hr, unsigned mask) {
+    HostSystem& s = hr.sys;
+    Rep& R = hr.rep;
+    R = Rep{};
+    const int n = s.n;
+    R.n_atoms = n;
+    R.n_tiles = (n + 31) / 32;
+    R.profile = phys_ ? 1 : 0;
+    bool anyq = false;
+    for (double v : s.q) anyq |= (v != 0.0);
+    int flags = 0;
+    if (s.use_lj && (mask & C_LJ)) flags |= F_LJ;
+    if (phys_) flags |= F_PHYS;
+    if (phys_ && anyq && (mask & C_CREAL)) flags |= F_COUL_REAL;
+    if (s.coulomb_type == 1 && (mask & C_PME)) flags |= F_PME;
+    if ((s.coulomb_type == 1 || !s.ei.empty()) && (mask & C_EXCL)) flags |= F_EXCL;
+    R.flags = flags;
+    R.rc_lj = s.lj_cutoff;
+    R.rc_c = s.coul_cutoff;
+    R.rc_lj2 = s.lj_cutoff * s.lj_cutoff;
+    R.rc_c2 = s.coul_cutoff * s.coul_cutoff;
+    if (phys_) {
+        double rc = 0.0;
+        if (s.use_lj) rc = std::max(rc, s.lj_cutoff);
+        if (anyq) rc = std::max(rc, s.coul_cutoff);
+        R.rc_list = rc + opt_.skin;
+    } else {
+        R.rc_list = s.lj_cutoff;  // the LennardJones list (no skin)
+    }
+    R.rc_list2 = R.rc_list * R.rc_list;
+    R.half_skin2 = 0.25 * opt_.skin * opt_.skin;
+    R.alpha = s.ewald;
+    R.dt = s.dt;
+    R.thermostat = s.thermostat;
+    R.t_temp = s.t_temp;
+    R.t_tau = s.t_tau;
+    R.t_freq = s.t_freq;
+    double dof = 3.0 * static_cast<double>(n) - 3.0;  // nose_hoover.cpp:9-13
+    if (dof < 1.0) dof = 1.0;
+    R.nh_Q = dof * KB * s.t_temp * s.t_tau * s.t_tau;
+    R.barostat = s.barostat;
+    R.b_pressure = s.b_pressure;
+    R.b_tau = s.b_tau;
+    R.b_compress = s.b_compress;
+    R.n_types = std::max(s.n_types, 1);
+    sort_grid(n, s.box, R.nvx, R.nvz);
+    if (s.coulomb_type == 1) {
+        s.pme_K = std::max(8, static_cast<int>(s.box / s.spacing + 0.5));  // simulation_engine.cpp:183-185
+    }
+    R.pme_K = (flags & F_PME) ? s.pme_K : 0;
+    double sum_q2 = 0.0;  // CoulombPME::calc_self_energy (coulomb_pme.cpp:71-75)
+    for (double v : s.q) sum_q2 += v * v;
+    R.e_self = (flags & F_PME) ? -KE * s.ewald / std::sqrt(M_PI) * sum_q2 : 0.0;
+    const uint64_t key = opt_.rng_seed;
+    R.key0 = static_cast<uint32_t>(key);
+    R.key1 = static_cast<uint32_t>(key >> 32);
+
+    RepState& st = hr.init;
+    st = RepState{};
+    st.L = s.box;
+    st.invL = 1.0 / s.box;
+    st.vscale = 1.0;
+    st.pscale = 1.0;
+    st.rebuild = 1;
+    st.lj_counter = 10;  // LennardJones::step_since_rebuild_ initial value (lennard_jones.cpp:10)
+    return DMDGPU_OK;
+}
+
+long long Batch::footprint(const HostSystem& s) const {
+    const long long n = s.n, tiles = (n + 31) / 32;
+    const double rho = n / (s.box * s.box * s.box);
+    long long per_atom = 8 * 6 + 8 * 2 + 4 * 2 + 8 * 3 + 4 + 8 * 3 + 4 * 4;
+    long long per_slot = 4 + 32 + 4 + 8 * 3;
+    long long chunks = tiles * 64;
+    (void)rho;
+    long long b = n * per_atom + tiles * 32 * per_slot + chunks * (4 + 32 * 8) + tiles * 64;
+    if (s.coulomb_type == 1) {
+        long long K = std::max(8, static_cast<int>(s.box / s.spacing + 0.5));
+        b += K * K * (K + 2) * 8 + K * K * K * 8 + K * K * (K / 2 + 1) * 16 + 3 * K * K * K * 8;
+    }
+    return b + (2 << 20);
+}
+
+int Batch::add(const dmdgpu_system& in, long long n_steps, unsigned comp_mask, int* out_slot) {
+    *out_slot = -1;
+    if (in.n_atoms <= 0) return fail(DMDGPU_ERR_PARM, "n_atoms must be positive");
+    if (!(in.box_size > 0)) return fail(DMDGPU_ERR_PARM, "box_size must be positive");
+    if (!in.masses || !in.pos_x || !in.pos_y || !in.pos_z)
+        return fail(DMDGPU_ERR_PARM, "masses and positions are required");
+    if (in.n_impropers != 0)
+        return fail(DMDGPU_ERR_PARM, "harmonic impropers are not supported on this path");
+    if (in.constraint_type != 0)
+        return fail(DMDGPU_ERR_PARM, "SHAKE/RATTLE constraints are not supported on this path");
+    if (in.thermostat_type < 0 || in.thermostat_type > 3)
+        return fail(DMDGPU_ERR_PARM, "Unknown thermostat type");
+    if (in.barostat_type < 0 || in.barostat_type > 1)
+        return fail(DMDGPU_ERR_PARM, "Unknown barostat type");
+    if (in.n_atoms >= (1 << 26)) return fail(DMDGPU_ERR_PARM, "more than 2^26 atoms in one system");
+    auto hr = std::make_unique<HostRep>();
+    HostSystem& s = hr->sys;
+    const int n = in.n_atoms;
+    s.n = n;
+    s.box = in.box_size;
+    s.mass = vec_of(in.masses, n);
+    s.q = in.charges ? vec_of(in.charges, n) : std::vector<double>(n, 0.0);
+    s.x = vec_of(in.pos_x, n);
+    s.y = vec_of(in.pos_y, n);
+    s.z = vec_of(in.pos_z, n);
+    s.vx = in.vel_x ? vec_of(in.vel_x, n) : std::vector<double>(n, 0.0);
+    s.vy = in.vel_y ? vec_of(in.vel_y, n) : std::vector<double>(n, 0.0);
+    s.vz = in.vel_z ? vec_of(in.vel_z, n) : std::vector<double>(n, 0.0);
+    s.type = in.atom_types ? vec_of(in.atom_types, n) : std::vector<int>(n, 0);
+    s.use_lj = in.use_lj;
+    s.n_types = in.lj_n_types;
+    s.lj_cutoff = in.lj_cutoff;
+    if (s.use_lj) {
+        if (s.n_types <= 0 || !in.lj_sigma || !in.lj_epsilon)
+            return fail(DMDGPU_ERR_PARM, "LJ enabled without a type table");
+        s.sigma = vec_of(in.lj_sigma, s.n_types * s.n_types);
+        s.eps = vec_of(in.lj_epsilon, s.n_types * s.n_types);
+        for (int t : s.type)
+            if (t < 0 || t >= s.n_types) return fail(DMDGPU_ERR_PARM, "atom type outside the LJ table");
+    }
+    auto check_idx = [&](const int32_t* p, int m) {
+        for (int k = 0; k < m; ++k)
+            if (p[k] < 0 || p[k] >= n) return false;
+        return true;
+    };
+    if (in.n_bonds > 0) {
+        if (!check_idx(in.bond_i, in.n_bonds) || !check_idx(in.bond_j, in.n_bonds))
+            return fail(DMDGPU_ERR_PARM, "bond index out of range");
+        s.bi = vec_of(in.bond_i, in.n_bonds);
+        s.bj = vec_of(in.bond_j, in.n_bonds);
+        s.bk = vec_of(in.bond_k, in.n_bonds);
+        s.br0 = vec_of(in.bond_r0, in.n_bonds);
+    }
+    if (in.n_angles > 0) {
+        if (!check_idx(in.angle_i, in.n_angles) || !check_idx(in.angle_j, in.n_angles) ||
+            !check_idx(in.angle_k, in.n_angles))
+            return fail(DMDGPU_ERR_PARM, "angle index out of range");
+        s.ai = vec_of(in.angle_i, in.n_angles);
+        s.aj = vec_of(in.angle_j, in.n_angles);
+        s.ak = vec_of(in.angle_k, in.n_angles);
+        s.akt = vec_of(in.angle_k_theta, in.n_angles);
+        s.at0 = vec_of(in.angle_theta0, in.n_angles);
+    }
+    if (in.n_dihedrals > 0) {
+        const int m = in.n_dihedrals;
+        if (!check_idx(in.dihedral_i, m) || !check_idx(in.dihedral_j, m) ||
+            !check_idx(in.dihedral_k, m) || !check_idx(in.dihedral_l, m))
+            return fail(DMDGPU_ERR_PARM, "dihedral index out of range");
+        s.di = vec_of(in.dihedral_i, m);
+        s.dj = vec_of(in.dihedral_j, m);
+        s.dk = vec_of(in.dihedral_k, m);
+        s.dl = vec_of(in.dihedral_l, m);
+        s.dn = vec_of(in.dihedral_periodicity, m);
+        s.dkp = vec_of(in.dihedral_k_phi, m);
+        s.dp0 = vec_of(in.dihedral_phi0, m);
+    }
+    if (in.n_excl > 0) {
+        if (!check_idx(in.excl_i, in.n_excl) || !check_idx(in.excl_j, in.n_excl))
+            return fail(DMDGPU_ERR_PARM, "exclusion index out of range");
+        s.ei = vec_of(in.excl_i, in.n_excl);
+        s.ej = vec_of(in.excl_j, in.n_excl);
+    }
+    s.coulomb_type = in.coulomb_type;
+    s.coul_cutoff = in.coulomb_cutoff;
+    s.ewald = in.ewald_coeff;
+    s.spacing = in.pme_grid_spacing;
+    s.pme_order = in.pme_order;
+    if (s.coulomb_type == 1 && !(s.spacing > 0)) return fail(DMDGPU_ERR_PARM, "pme_grid_spacing must be positive");
+    s.dt = in.dt;
+    s.n_steps = in.n_steps;
+    s.thermostat = in.thermostat_type;
+    s.t_temp = in.thermo_temperature;
+    s.t_tau = in.thermo_tau;
+    s.t_freq = in.thermo_frequency;
+    s.barostat = in.barostat_type;
+    s.b_pressure = in.baro_pressure;
+    s.b_tau = in.baro_tau;
+    s.b_compress = in.baro_compressibility;
+    s.checkpoint_interval = in.checkpoint_interval;
+    if (in.checkpoint_path) s.checkpoint_path = in.checkpoint_path;
+    // Maxwell-Boltzmann velocities exactly as build_simulation (simulation_engine.cpp:339-383)
+    if (in.gen_vel && n > 0) {
+        std::mt19937 rng(in.seed);
+        std::normal_distribution<double> normal(0.0, 1.0);
+        double kBT = KB * in.init_temperature;
+        for (int i = 0; i < n; ++i) {
+            double sigma = std::sqrt(kBT / s.mass[i]);
+            s.vx[i] = normal(rng) * sigma;
+            s.vy[i] = normal(rng) * sigma;
+            s.vz[i] = normal(rng) * sigma;
+        }
+        double cx = 0, cy = 0, cz = 0, tm = 0;
+        for (int i = 0; i < n; ++i) {
+            cx += s.mass[i] * s.vx[i];
+            cy += s.mass[i] * s.vy[i];
+            cz += s.mass[i] * s.vz[i];
+            tm += s.mass[i];
+        }
+        cx /= tm;
+        cy /= tm;
+        cz /= tm;
+        for (int i = 0; i < n; ++i) {
+            s.vx[i] -= cx;
+            s.vy[i] -= cy;
+            s.vz[i] -= cz;
+        }
+        if (in.init_temperature > 0) {
+            double ek = 0;
+            for (int i = 0; i < n; ++i)
+                ek += 0.5 * s.mass[i] * (s.vx[i] * s.vx[i] + s.vy[i] * s.vy[i] + s.vz[i] * s.vz[i]);
+            double ta = (n < 2) ? 0.0 : 2.0 * ek / ((3.0 * static_cast<double>(n) - 3.0) * KB);
+            double lam = std::sqrt(in.init_temperature / ta);
+            for (int i = 0; i < n; ++i) {
+                s.vx[i] *= lam;
+                s.vy[i] *= lam;
+                s.vz[i] *= lam;
+            }
+        }
+    }
+    int rc = build_host(*hr, comp_mask);
+    if (rc) return rc;
+    hr->target = n_steps;
+    if (budget_ > 0 && used_bytes_ + footprint(s) > budget_)
+        return fail(DMDGPU_ERR_BUDGET, "HBM budget exceeded");
+    // reuse a free slot id
+    int slot = -1;
+    for (size_t k = 0; k < reps_.size(); ++k)
+        if (!reps_[k]) { slot = static_cast<int>(k); break; }
+    if (slot < 0) {
+        slot = static_cast<int>(reps_.size());
+        reps_.emplace_back();
+    }
+    reps_[slot] = std::move(hr);
+    packed_ = false;
+    *out_slot = slot;
+    return DMDGPU_OK;
+}
+
+int Batch::release(int slot) {
+    if (!has(slot)) return fail(DMDGPU_ERR_INVALID, "no such slot");
+    reps_[slot].reset();
+    packed_ = false;
+    return DMDGPU_OK;
+}
+
+int Batch::replica_index(int slot) const {
+    for (size_t k = 0; k < order_.size(); ++k)
+        if (order_[k] == slot) return static_cast<int>(k);
+    return -1;
+}
+
+// ---------------------------------------------------------------------------
+// Packing: host replicas -> one device table
+// ---------------------------------------------------------------------------
+int Batch::pack() {
+    CK(cudaSetDevice(device_));
+    // carry the device state of replicas that were already packed
+    if (arena_ && h_st_) {
+        CK(cudaStreamSynchronize(stream_));
+        launch_finalize_velocities(dev_, stream_, &launches_);
+        CK(cudaMemcpyAsync(h_st_, d_st_, sizeof(RepState) * order_.size(), cudaMemcpyDeviceToHost, stream_));
+        CK(cudaStreamSynchronize(stream_));
+        for (size_t k = 0; k < order_.size(); ++k) {
+            if (!reps_[order_[k]]) continue;
+            HostRep& o = *reps_[order_[k]];
+            HostSystem& s = o.sys;
+            const int a0 = o.rep.atom_begin, n = s.n;
+            CK(cudaMemcpy(s.x.data(), dev_.x + a0, n * 8, cudaMemcpyDeviceToHost));
+            CK(cudaMemcpy(s.y.data(), dev_.y + a0, n * 8, cudaMemcpyDeviceToHost));
+            CK(cudaMemcpy(s.z.data(), dev_.z + a0, n * 8, cudaMemcpyDeviceToHost));
+            CK(cudaMemcpy(s.vx.data(), dev_.vx + a0, n * 8, cudaMemcpyDeviceToHost));
+            CK(cudaMemcpy(s.vy.data(), dev_.vy + a0, n * 8, cudaMemcpyDeviceToHost));
+            CK(cudaMemcpy(s.vz.data(), dev_.vz + a0, n * 8, cudaMemcpyDeviceToHost));
+            RepState st = h_st_[k];
+            st.rebuild = 1;          // slots change: rebuild every list
+            st.have_forces = 0;      // forces are recomputed at the same positions
+            st.n_chunks = 0;
+            o.init = st;
+        }
+    }
+    free_device();
+    order_.clear();
+    for (size_t k = 0; k < reps_.size(); ++k)
+        if (reps_[k]) order_.push_back(static_cast<int>(k));
+    const int R = static_cast<int>(order_.size());
+    if (R == 0) {
+        packed_ = true;
+        return DMDGPU_OK;
+    }
+    // offsets
+    long long n_atoms = 0, n_tiles = 0, n_bins = 0, n_chunks = 0, n_lj = 0, n_bond = 0, n_ang = 0,
+              n_dih = 0, n_excl = 0, mesh_fix = 0, mesh_real = 0, mesh_cplx = 0, n_bsp = 0;
+    int pme_blocks = 0;
+    any_pme_ = any_baro_ = any_ref_lj_ = any_andersen_ref_ = any_andersen_phys_ = false;
+    for (int k = 0; k < R; ++k) {
+        HostRep& h = *reps_[order_[k]];
+        HostSystem& s = h.sys;
+        Rep& P = h.rep;
+        P.atom_begin = static_cast<int>(n_atoms);
+        P.tile_begin = static_cast<int>(n_tiles);
+        P.bin_begin = static_cast<int>(n_bins);
+        P.lj_off = static_cast<int>(n_lj);
+        // chunk capacity: j atoms within rc_list of a tile's box (half), 1.5x margin
+        {
+            const double rho = s.n / (s.box * s.box * s.box);
+            const double at = std::cbrt(32.0 / rho);
+            const double reach = P.rc_list + 1.2 * at;
+            double nj = 0.5 * rho * 4.18879 * reach * reach * reach;
+            nj = std::min(nj, static_cast<double>(s.n));
+            long long per_tile = static_cast<long long>(nj / 32.0) + 3;
+            P.chunk_cap = static_cast<int>(std::max<long long>(1, P.n_tiles * per_tile * 3 / 2 + 8));
+            if (P.rc_list <= 0) P.chunk_cap = 1;
+        }
+        P.chunk_begin = static_cast<int>(n_chunks);
+        n_atoms += s.n;
+        n_tiles += P.n_tiles;
+        n_bins += static_cast<long long>(P.nvx) * P.nvx * P.nvz;
+        n_chunks += P.chunk_cap;
+        n_lj += static_cast<long long>(P.n_types) * P.n_types;
+        n_bond += s.bi.size();
+        n_ang += s.ai.size();
+        n_dih += s.di.size();
+        n_excl += s.ei.size();
+        if (P.flags & F_PME) {
+            const int K = P.pme_K;
+            P.mesh_fix_off = mesh_fix;
+            P.mesh_fix_n = phys_ ? static_cast<long long>(K) * K * K
+                                 : static_cast<long long>(K) * K * 2 * (K / 2 + 1);
+            mesh_fix += P.mesh_fix_n;
+            P.mesh_real_off = mesh_real;
+            mesh_real += static_cast<long long>(K) * K * K + 64;
+            P.mesh_cplx_off = mesh_cplx;
+            mesh_cplx += static_cast<long long>(K) * K * (K / 2 + 1) + 64;
+            P.bsp_off = static_cast<int>(n_bsp);
+            n_bsp += K;
+            P.pme_block_begin = pme_blocks;
+            P.pme_blocks = static_cast<int>((static_cast<long long>(K) * K * (K / 2 + 1) + 255) / 256);
+            pme_blocks += P.pme_blocks;
+            any_pme_ = true;
+        }
+        if (s.barostat) any_baro_ = true;
+        if (!phys_ && (P.flags & F_LJ)) any_ref_lj_ = true;
+        if (s.thermostat == 3 && !phys_) any_andersen_ref_ = true;
+        if (s.thermostat == 3 && phys_) any_andersen_phys_ = true;
+    }
+    n_fix_total_ = mesh_fix;
+    n_pme_blocks_ = pme_blocks;
+    try {
+        arena_ = std::make_unique<DeviceArena>();
+        DeviceArena& A = *arena_;
+        Dev& d = dev_;
+        d = Dev{};
+        d.n_rep = R;
+        d.n_atoms = static_cast<int>(n_atoms);
+        d.n_tiles = static_cast<int>(n_tiles);
+        d.n_slots = static_cast<int>(n_tiles * 32);
+        d.n_bins = static_cast<int>(n_bins);
+        d_rep_ = A.alloc<Rep>(R);
+        d_st_ = A.alloc<RepState>(R);
+        d.rep = d_rep_;
+        d.st = d_st_;
+        d.x = A.alloc<double>(n_atoms);
+        d.y = A.alloc<double>(n_atoms);
+        d.z = A.alloc<double>(n_atoms);
+        d.vx = A.alloc<double>(n_atoms);
+        d.vy = A.alloc<double>(n_atoms);
+        d.vz = A.alloc<double>(n_atoms);
+        double* mass = A.alloc<double>(n_atoms);
+        double* q = A.alloc<double>(n_atoms);
+        int* type = A.alloc<int>(n_atoms);
+        int* atom_rep = A.alloc<int>(n_atoms);
+        d.mass = mass;
+        d.q = q;
+        d.type = type;
+        d.atom_rep = atom_rep;
+        d.fbx = A.alloc<long long>(n_atoms);
+        d.fby = A.alloc<long long>(n_atoms);
+        d.fbz = A.alloc<long long>(n_atoms);
+        d.slot_of_atom = A.alloc<int>(n_atoms);
+        d.xr = A.alloc<double>(n_atoms);
+        d.yr = A.alloc<double>(n_atoms);
+        d.zr = A.alloc<double>(n_atoms);
+        d.imgx = A.alloc<int>(n_atoms);
+        d.imgy = A.alloc<int>(n_atoms);
+        d.imgz = A.alloc<int>(n_atoms);
+        d.atom_bin = A.alloc<int>(n_atoms);
+        d.atom_of_slot = A.alloc<int>(d.n_slots);
+        if (fp64_) d.xq64 = A.alloc<double4>(d.n_slots);
+        else d.xq32 = A.alloc<float4>(d.n_slots);
+        d.type_s = A.alloc<int>(d.n_slots);
+        d.fnx = A.alloc<long long>(d.n_slots);
+        d.fny = A.alloc<long long>(d.n_slots);
+        d.fnz = A.alloc<long long>(d.n_slots);
+        d.tcx = A.alloc<double>(n_tiles);
+        d.tcy = A.alloc<double>(n_tiles);
+        d.tcz = A.alloc<double>(n_tiles);
+        d.thx = A.alloc<float>(n_tiles);
+        d.thy = A.alloc<float>(n_tiles);
+        d.thz = A.alloc<float>(n_tiles);
+        int* tile_rep = A.alloc<int>(n_tiles);
+        d.tile_rep = tile_rep;
+        d.tile_ke = A.alloc<double>(n_tiles);
+        d.tile_vir = A.alloc<double>(n_tiles);
+        d.bin_count = A.alloc<int>(n_bins);
+        d.bin_start = A.alloc<int>(n_bins);
+        d.bin_fill = A.alloc<int>(n_bins);
+        int* vox_rank = A.alloc<int>(n_bins);
+        d.vox_rank = vox_rank;
+        d_bin_rep_ = A.alloc<int>(n_bins);
+        d.sort_buf = A.alloc<int>(d.n_slots);
+        d.chunk_itile = A.alloc<int>(n_chunks);
+        d.chunk_j = A.alloc<uint32_t>(n_chunks * 32);
+        d.chunk_mask = A.alloc<uint32_t>(n_chunks * 32);
+        d.chunk_prefix = A.alloc<int>(R + 1);
+        // host-side staging
+        std::vector<double> hm(n_atoms), hq(n_atoms), hx(n_atoms), hy(n_atoms), hz(n_atoms), hvx(n_atoms),
+            hvy(n_atoms), hvz(n_atoms);
+        std::vector<int> ht(n_atoms), har(n_atoms), htr(n_tiles), hvr(n_bins), hbr(n_bins);
+        std::vector<double2> lj64(n_lj);
+        std::vector<float2> lj32(n_lj);
+        std::vector<int2> bij;
+        std::vector<double2> bkr;
+        std::vector<int4> aijk;
+        std::vector<double2> akt;
+        std::vector<int4> dijkl;
+        std::vector<int> dn;
+        std::vector<double2> dkp;
+        std::vector<int2> ex;
+        std::vector<std::vector<int>> exl(n_atoms);
+        std::vector<double> bsp(std::max<long long>(n_bsp, 1));
+        std::vector<int> pbr(std::max(pme_blocks, 1));
+        std::vector<Rep> hrep(R);
+        for (int k = 0; k < R; ++k) {
+            HostRep& h = *reps_[order_[k]];
+            HostSystem& s = h.sys;
+            Rep& P = h.rep;
+            const int a0 = P.atom_begin;
+            for (int i = 0; i < s.n; ++i) {
+                hm[a0 + i] = s.mass[i];
+                hq[a0 + i] = s.q[i];
+                hx[a0 + i] = s.x[i];
+                hy[a0 + i] = s.y[i];
+                hz[a0 + i] = s.z[i];
+                hvx[a0 + i] = s.vx[i];
+                hvy[a0 + i] = s.vy[i];
+                hvz[a0 + i] = s.vz[i];
+                ht[a0 + i] = s.type[i];
+                har[a0 + i] = k;
+            }
+            for (int t = 0; t < P.n_tiles; ++t) htr[P.tile_begin + t] = k;
+            // snake rank of the replica's sort cells: columns in boustrophedon order
+            // over (x, y), z reversed in every other column, so consecutive cells touch
+            const int nvx = P.nvx, nvz = P.nvz;
+            const int nb = nvx * nvx * nvz;
+            for (int ix = 0; ix < nvx; ++ix)
+                for (int iy = 0; iy < nvx; ++iy) {
+                    const int col = ix * nvx + ((ix & 1) ? nvx - 1 - iy : iy);
+                    for (int iz = 0; iz < nvz; ++iz) {
+                        const int v = (ix * nvx + iy) * nvz + iz;
+                        hvr[P.bin_begin + v] = col * nvz + ((col & 1) ? nvz - 1 - iz : iz);
+                    }
+                }
+            for (int b = 0; b < nb; ++b) hbr[P.bin_begin + b] = k;
+            // LJ tables: (eps, sig^6) with sig2*sig2*sig2 as in lennard_jones.cpp:75-77
+            for (int ti = 0; ti < P.n_types; ++ti)
+                for (int tj = 0; tj < P.n_types; ++tj) {
+                    double sg = 1.0, ep = 0.0;
+                    if (s.use_lj && !s.sigma.empty()) {
+                        sg = s.sigma[ti * s.n_types + tj];
+                        ep = s.eps[ti * s.n_types + tj];
+                    }
+                    const double sig2 = sg * sg;
+                    const double sig6 = sig2 * sig2 * sig2;
+                    lj64[P.lj_off + ti * P.n_types + tj] = make_double2(ep, sig6);
+                    lj32[P.lj_off + ti * P.n_types + tj] =
+                        make_float2(static_cast<float>(4.0 * ep * sig6), static_cast<float>(4.0 * ep * sig6 * sig6));
+                }
+            for (size_t t = 0; t < s.bi.size(); ++t) {
+                bij.push_back(make_int2(a0 + s.bi[t], a0 + s.bj[t]));
+                bkr.push_back(make_double2(s.bk[t], s.br0[t]));
+            }
+            for (size_t t = 0; t < s.ai.size(); ++t) {
+                aijk.push_back(make_int4(a0 + s.ai[t], a0 + s.aj[t], a0 + s.ak[t], 0));
+                akt.push_back(make_double2(s.akt[t], s.at0[t]));
+            }
+            for (size_t t = 0; t < s.di.size(); ++t) {
+                dijkl.push_back(make_int4(a0 + s.di[t], a0 + s.dj[t], a0 + s.dk[t], a0 + s.dl[t]));
+                dn.push_back(s.dn[t]);
+                dkp.push_back(make_double2(s.dkp[t], s.dp0[t]));
+            }
+            for (size_t t = 0; t < s.ei.size(); ++t) {
+                const int gi = a0 + s.ei[t], gj = a0 + s.ej[t];
+                ex.push_back(make_int2(gi, gj));
+                if (gi != gj) {
+                    exl[gi].push_back(gj);
+                    exl[gj].push_back(gi);
+                }
+            }
+            if (P.flags & F_PME) {
+                const int K = P.pme_K;
+                for (int kk = 0; kk < K; ++kk) {
+                    const int m = (kk <= K / 2) ? kk : kk - K;
+                    double b;
+                    if (phys_) {
+                        const double c = 2.0 / 3.0 + std::cos(2.0 * PI * m / K) / 3.0;
+                        b = 1.0 / (c * c);
+                    } else {  // b_factor (coulomb_pme.cpp:159-163)
+                        if (m == 0) b = 1.0;
+                        else {
+                            const double t = M_PI * std::abs(m) / K;
+                            b = std::pow(std::sin(t) / t, 2 * s.pme_order);
+                        }
+                    }
+                    bsp[P.bsp_off + kk] = b;
+                }
+                for (int b = 0; b < P.pme_blocks; ++b) pbr[P.pme_block_begin + b] = k;
+            }
+            hrep[k] = P;
+        }
+        // exclusion CSR
+        std::vector<int> ex_start(n_atoms + 1, 0), ex_list;
+        for (long long a = 0; a < n_atoms; ++a) {
+            std::sort(exl[a].begin(), exl[a].end());
+            exl[a].erase(std::unique(exl[a].begin(), exl[a].end()), exl[a].end());
+            ex_start[a + 1] = ex_start[a] + static_cast<int>(exl[a].size());
+            ex_list.insert(ex_list.end(), exl[a].begin(), exl[a].end());
+        }
+        auto up = [&](void* dst, const void* src, size_t bytes) {
+            if (bytes && cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice) != cudaSuccess)
+                throw std::runtime_error("upload failed");
+        };
+        up(d.x, hx.data(), 8 * n_atoms);
+        up(d.y, hy.data(), 8 * n_atoms);
+        up(d.z, hz.data(), 8 * n_atoms);
+        up(d.vx, hvx.data(), 8 * n_atoms);
+        up(d.vy, hvy.data(), 8 * n_atoms);
+        up(d.vz, hvz.data(), 8 * n_atoms);
+        up(mass, hm.data(), 8 * n_atoms);
+        up(q, hq.data(), 8 * n_atoms);
+        up(type, ht.data(), 4 * n_atoms);
+        up(atom_rep, har.data(), 4 * n_atoms);
+        up(tile_rep, htr.data(), 4 * n_tiles);
+        up(vox_rank, hvr.data(), 4 * n_bins);
+        up(d_bin_rep_, hbr.data(), 4 * n_bins);
+        double2* dlj64 = A.alloc<double2>(n_lj);
+        float2* dlj32 = A.alloc<float2>(n_lj);
+        up(dlj64, lj64.data(), sizeof(double2) * n_lj);
+        up(dlj32, lj32.data(), sizeof(float2) * n_lj);
+        d.lj64 = dlj64;
+        d.lj32 = dlj32;
+        d.n_bonds = static_cast<int>(bij.size());
+        d.n_angles = static_cast<int>(aijk.size());
+        d.n_dih = static_cast<int>(dijkl.size());
+        d.n_excl = static_cast<int>(ex.size());
+        int2* dbij = A.alloc<int2>(bij.size());
+        double2* dbkr = A.alloc<double2>(bkr.size());
+        int4* daijk = A.alloc<int4>(aijk.size());
+        double2* dakt = A.alloc<double2>(akt.size());
+        int4* ddijkl = A.alloc<int4>(dijkl.size());
+        int* ddn = A.alloc<int>(dn.size());
+        double2* ddkp = A.alloc<double2>(dkp.size());
+        int2* dex = A.alloc<int2>(ex.size());
+        int* dexs = A.alloc<int>(ex_start.size());
+        int* dexl = A.alloc<int>(ex_list.size());
+        up(dbij, bij.data(), sizeof(int2) * bij.size());
+        up(dbkr, bkr.data(), sizeof(double2) * bkr.size());
+        up(daijk, aijk.data(), sizeof(int4) * aijk.size());
+        up(dakt, akt.data(), sizeof(double2) * akt.size());
+        up(ddijkl, dijkl.data(), sizeof(int4) * dijkl.size());
+        up(ddn, dn.data(), sizeof(int) * dn.size());
+        up(ddkp, dkp.data(), sizeof(double2) * dkp.size());
+        up(dex, ex.data(), sizeof(int2) * ex.size());
+        up(dexs, ex_start.data(), sizeof(int) * ex_start.size());
+        up(dexl, ex_list.data(), sizeof(int) * ex_list.size());
+        d.bond_ij = dbij;
+        d.bond_kr = dbkr;
+        d.ang_ijk = daijk;
+        d.ang_kt = dakt;
+        d.dih_ijkl = ddijkl;
+        d.dih_n = ddn;
+        d.dih_kp = ddkp;
+        d.excl = dex;
+        d.ex_start = dexs;
+        d.ex_list = dexl;
+        if (any_pme_) {
+            d.mesh_fix = A.alloc<long long>(mesh_fix);
+            if (fp64_) {
+                d.mesh_real = A.alloc<double>(mesh_real);
+                d.mesh_cplx = A.alloc<double2>(mesh_cplx);
+            } else {
+                d.mesh_real = A.alloc<float>(mesh_real);
+                d.mesh_cplx = A.alloc<float2>(mesh_cplx);
+            }
+            double* dbsp = A.alloc<double>(bsp.size());
+            up(dbsp, bsp.data(), 8 * bsp.size());
+            d.bsp = dbsp;
+            d.pme_part = A.alloc<double>(2 * static_cast<size_t>(pme_blocks));
+            int* dpbr = A.alloc<int>(pbr.size());
+            up(dpbr, pbr.data(), 4 * pbr.size());
+            d.pme_block_rep = dpbr;
+        }
+        if (any_andersen_ref_) {
+            d_and_flag_ = A.alloc<int>(n_atoms);
+            d_and_v_ = A.alloc<double>(3 * n_atoms);
+            d.and_flag = d_and_flag_;
+            d.and_v = d_and_v_;
+            if (cudaMallocHost(&h_and_flag_, 4 * n_atoms) != cudaSuccess ||
+                cudaMallocHost(&h_and_v_, 24 * n_atoms) != cudaSuccess)
+                throw std::runtime_error("pinned alloc failed");
+        }
+        up(d_rep_, hrep.data(), sizeof(Rep) * R);
+        std::vector<RepState> hst(R);
+        for (int k = 0; k < R; ++k) {
+            HostRep& h = *reps_[order_[k]];
+            hst[k] = h.init;
+            hst[k].target_step = h.target;
+        }
+        up(d_st_, hst.data(), sizeof(RepState) * R);
+        used_bytes_ = static_cast<long long>(A.bytes);
+    } catch (const std::exception& e) {
+        arena_.reset();
+        return fail(DMDGPU_ERR_OOM, std::string("device allocation/upload failed: ") + e.what());
+    }
+    CK(cudaMallocHost(&h_st_, sizeof(RepState) * R));
+    // cuFFT plans per mesh size
+    for (int k = 0; k < R; ++k) {
+        const Rep& P = reps_[order_[k]]->rep;
+        if (!(P.flags & F_PME) || plans_.count(P.pme_K)) continue;
+        cufftHandle f, b;
+        const int K = P.pme_K;
+        if (cufftPlan3d(&f, K, K, K, fp64_ ? CUFFT_D2Z : CUFFT_R2C) != CUFFT_SUCCESS ||
+            cufftPlan3d(&b, K, K, K, fp64_ ? CUFFT_Z2D : CUFFT_C2R) != CUFFT_SUCCESS)
+            return fail(DMDGPU_ERR_GPU, "cufftPlan3d failed");
+        cufftSetStream(f, stream_);
+        cufftSetStream(b, stream_);
+        plans_[K] = {f, b};
+    }
+    packed_ = true;
+    graph_dirty_ = true;
+    return DMDGPU_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Step orchestration
+// ---------------------------------------------------------------------------
+void Batch::enqueue_eval(int pass) {
+    Dev& d = dev_;
+    launch_eval_begin(d, pass, stream_, &launches_);
+    if (pass != PASS_SECOND) launch_clear_forces(d, stream_, &launches_);
+    enqueue_rebuild();
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (prof_nb_) {
+        e0 = next_event();
+        cudaEventRecord(e0, stream_);
+    }
+    launch_nonbonded(d, fp64_, phys_, n_sm_, stream_, &launches_);
+    if (prof_nb_) {
+        e1 = next_event();
+        cudaEventRecord(e1, stream_);
+        prof_nb_->emplace_back(e0, e1);
+    }
+    launch_bonded(d, fp64_, phys_, stream_, &launches_);
+    if (any_pme_) {
+        if (prof_pme_) {
+            e0 = next_event();
+            cudaEventRecord(e0, stream_);
+        }
+        launch_pme_spread(d, fp64_, stream_, &launches_);
+        launch_pme_convert(d, fp64_, n_fix_total_, stream_, &launches_);
+        for (int k : order_) {
+            const Rep& P = reps_[k]->rep;
+            if (!(P.flags & F_PME)) continue;
+            auto& pl = plans_[P.pme_K];
+            if (fp64_) {
+                cufftExecD2Z(pl.first, static_cast<double*>(d.mesh_real) + P.mesh_real_off,
+                             static_cast<cufftDoubleComplex*>(d.mesh_cplx) + P.mesh_cplx_off);
+            } else {
+                cufftExecR2C(pl.first, static_cast<float*>(d.mesh_real) + P.mesh_real_off,
+                             static_cast<cufftComplex*>(d.mesh_cplx) + P.mesh_cplx_off);
+            }
+        }
+        launch_pme_influence(d, fp64_, n_pme_blocks_, stream_, &launches_);
+        for (int k : order_) {
+            const Rep& P = reps_[k]->rep;
+            if (!(P.flags & F_PME)) continue;
+            auto& pl = plans_[P.pme_K];
+            if (fp64_) {
+                cufftExecZ2D(pl.second, static_cast<cufftDoubleComplex*>(d.mesh_cplx) + P.mesh_cplx_off,
+                             static_cast<double*>(d.mesh_real) + P.mesh_real_off);
+            } else {
+                cufftExecC2R(pl.second, static_cast<cufftComplex*>(d.mesh_cplx) + P.mesh_cplx_off,
+                             static_cast<float*>(d.mesh_real) + P.mesh_real_off);
+            }
+        }
+        launch_pme_gather(d, fp64_, stream_, &launches_);
+        if (prof_pme_) {
+            e1 = next_event();
+            cudaEventRecord(e1, stream_);
+            prof_pme_->emplace_back(e0, e1);
+        }
+    }
+    launch_eval_end(d, stream_, &launches_);
+}
+
+// Neighbour-list rebuild.  Eagerly every kernel is launched and the ones of
+// replicas without a pending rebuild return at once; inside a captured graph
+// the body sits in an IF conditional node that the flag kernel switches on only
+// when some replica rebuilds, so a step without a rebuild costs one launch.
+void Batch::enqueue_rebuild() {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing(stream_, &cs);
+    if (cs != cudaStreamCaptureStatusActive) {
+        launch_rebuild_flag(dev_, cudaGraphConditionalHandle{}, false, stream_, &launches_);
+        launch_rebuild_body(dev_, d_bin_rep_, false, stream_, &launches_);
+        return;
+    }
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    cudaStreamGetCaptureInfo(stream_, &cs, nullptr, &g, nullptr, nullptr);
+    cudaGraphConditionalHandle h;
+    if (cudaGraphConditionalHandleCreate(&h, g, 0, 0) != cudaSuccess) {
+        capture_error_ = true;
+        return;
+    }
+    launch_rebuild_flag(dev_, h, true, stream_, &launches_);
+    cudaStreamGetCaptureInfo(stream_, &cs, nullptr, &g, &deps, &ndeps);
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeIf;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node;
+    if (cudaGraphAddNode(&node, g, deps, ndeps, &cp) != cudaSuccess) {
+        capture_error_ = true;
+        return;
+    }
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    if (cudaStreamBeginCaptureToGraph(body_stream_, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed) !=
+        cudaSuccess) {
+        capture_error_ = true;
+        return;
+    }
+    // counted when they actually run (from the device's list-build counter)
+    long long body_count = 0;
+    launch_rebuild_body(dev_, d_bin_rep_, true, body_stream_, &body_count);
+    cudaGraph_t out = nullptr;
+    if (cudaStreamEndCapture(body_stream_, &out) != cudaSuccess) capture_error_ = true;
+    cudaStreamUpdateCaptureDependencies(stream_, &node, 1, cudaStreamSetCaptureDependencies);
+}
+
+void Batch::enqueue_step() {
+    launch_step_begin(dev_, stream_, &launches_);
+    // The first evaluation repeats the previous step's second one unless the
+    // barostat moved the atoms, the REF list cadence rebuilds now, or no forces
+    // exist yet; only then is it issued (its kernels skip replicas that do not need it).
+    if (need_eval1_) enqueue_eval(PASS_FIRST);
+    launch_kick_drift(dev_, fp64_, stream_, &launches_);
+    enqueue_eval(PASS_SECOND);
+    launch_kick2(dev_, any_andersen_ref_, any_andersen_phys_, stream_, &launches_);
+    launch_replica_update(dev_, stream_, &launches_);
+    if (any_baro_) launch_apply_scale(dev_, fp64_, stream_, &launches_);
+}
+
+// AndersenThermostat::apply (andersen.cpp:14-32): the REF profile reproduces the
+// reference's mt19937_64 stream on the host and uploads the resampled velocities.
+void Batch::andersen_ref_prepare() {
+    std::memset(h_and_flag_, 0, sizeof(int) * dev_.n_atoms);
+    for (int k : order_) {
+        HostRep& h = *reps_[k];
+        const HostSystem& s = h.sys;
+        if (s.thermostat != 3) continue;
+        const double prob = s.t_freq * s.dt;
+        if (prob <= 0.0) continue;
+        std::mt19937_64 rng(h.andersen_seed);
+        std::uniform_real_distribution<double> uni(0.0, 1.0);
+        std::normal_distribution<double> nd(0.0, 1.0);
+        const int a0 = h.rep.atom_begin;
+        for (int i = 0; i < s.n; ++i) {
+            if (uni(rng) < prob) {
+                double sigma = std::sqrt(KB * s.t_temp / s.mass[i]);
+                h_and_flag_[a0 + i] = 1;
+                h_and_v_[3 * (a0 + i)] = nd(rng) * sigma;
+                h_and_v_[3 * (a0 + i) + 1] = nd(rng) * sigma;
+                h_and_v_[3 * (a0 + i) + 2] = nd(rng) * sigma;
+            }
+        }
+        ++h.andersen_seed;
+    }
+    cudaMemcpyAsync(d_and_flag_, h_and_flag_, sizeof(int) * dev_.n_atoms, cudaMemcpyHostToDevice, stream_);
+    cudaMemcpyAsync(d_and_v_, h_and_v_, sizeof(double) * 3 * dev_.n_atoms, cudaMemcpyHostToDevice, stream_);
+}
+
+int Batch::run_steps(int n) {
+    if (n <= 0) return DMDGPU_OK;
+    if (any_andersen_ref_) {
+        // host-generated random stream per step: no graph
+        need_eval1_ = true;
+        for (int i = 0; i < n; ++i) {
+            andersen_ref_prepare();
+            CK(cudaStreamSynchronize(stream_));
+            enqueue_step();
+            CK(cudaGetLastError());
+        }
+        return DMDGPU_OK;
+    }
+    if (graph_dirty_ || !graph_) {
+        // first step eagerly (initial list + forces), then capture the steady-state step
+        need_eval1_ = true;
+        enqueue_step();
+        CK(cudaGetLastError());
+        need_eval1_ = any_baro_ || any_ref_lj_;
+        --n;
+        if (graph_) cudaGraphExecDestroy(graph_);
+        graph_ = nullptr;
+        cudaGraph_t g;
+        long long before = launches_;
+        capture_error_ = false;
+        CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+        enqueue_step();
+        CK(cudaStreamEndCapture(stream_, &g));
+        if (capture_error_) {
+            cudaGraphDestroy(g);
+            return fail(DMDGPU_ERR_GPU, "conditional-node capture failed");
+        }
+        per_step_launches_ = launches_ - before;
+        CK(cudaGraphInstantiate(&graph_, g, 0));
+        cudaGraphDestroy(g);
+        graph_dirty_ = false;
+    }
+    for (int i = 0; i < n; ++i) {
+        CK(cudaGraphLaunch(graph_, stream_));
+        launches_ += per_step_launches_;
+    }
+    return DMDGPU_OK;
+}
+
+int Batch::sync_status() {
+    if (!packed_ || order_.empty()) return DMDGPU_OK;
+    CK(cudaMemcpyAsync(h_st_, d_st_, sizeof(RepState) * order_.size(), cudaMemcpyDeviceToHost, stream_));
+    CK(cudaStreamSynchronize(stream_));
+    int rc = DMDGPU_OK;
+    // rebuild bodies inside graph conditional nodes: 7 kernels per executed body
+    const long long runs = h_st_[0].body_runs;
+    if (runs > body_runs_seen_) launches_ += 7 * (runs - body_runs_seen_);
+    body_runs_seen_ = runs;
+    for (size_t k = 0; k < order_.size(); ++k) {
+        HostRep& h = *reps_[order_[k]];
+        const int st = h_st_[k].status;
+        if (st & ST_NAN) rc = fail(DMDGPU_ERR_NAN, "non-finite force or energy on device");
+        else if (st & ST_RANGE) rc = fail(DMDGPU_ERR_BOND_EXPLOSION, "force outside the fixed-point range");
+        else if (st & ST_CAPACITY) rc = fail(DMDGPU_ERR_CAPACITY, "pair list capacity exceeded");
+        if (!h.done && h.target > 0 && h_st_[k].step >= h.target) {
+            h.done = true;
+            finished_.push_back(order_[k]);
+        }
+    }
+    return rc;
+}
+
+int Batch::step(int n) {
+    CK(cudaSetDevice(device_));
+    if (!packed_) {
+        int rc = pack();
+        if (rc) return rc;
+    }
+    if (order_.empty()) return DMDGPU_OK;
+    int rc = run_steps(n);
+    if (rc) return rc;
+    return sync_status();
+}
+
+cudaEvent_t Batch::next_event() {
+    if (ev_used_ == ev_pool_.size()) {
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        ev_pool_.push_back(e);
+    }
+    return ev_pool_[ev_used_++];
+}
+
+int Batch::extend_targets(long long n) {
+    CK(cudaSetDevice(device_));
+    if (!packed_) {
+        int rc = pack();
+        if (rc) return rc;
+    }
+    CK(cudaStreamSynchronize(stream_));
+    for (size_t k = 0; k < order_.size(); ++k) {
+        long long cur = 0;
+        CK(cudaMemcpy(&cur, &d_st_[k].step, 8, cudaMemcpyDeviceToHost));
+        long long tgt = cur + n;
+        CK(cudaMemcpy(&d_st_[k].target_step, &tgt, 8, cudaMemcpyHostToDevice));
+        reps_[order_[k]]->target = tgt;
+        reps_[order_[k]]->done = false;
+    }
+    return DMDGPU_OK;
+}
+
+// n steps as one captured graph with timing events around the non-bonded kernel
+// and the PME chain of every evaluation.
+int Batch::step_profiled(int n, double* nb_ms, double* pme_ms, double* total_ms, long long* nb_launches) {
+    CK(cudaSetDevice(device_));
+    if (!packed_) {
+        int rc = pack();
+        if (rc) return rc;
+    }
+    if (graph_dirty_ || !graph_ || any_andersen_ref_) {
+        int rc = run_steps(1);  // initial forces / steady-state graph
+        if (rc) return rc;
+        --n;
+    }
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> nb, pme;
+    // events must exist before capture (creating one during capture invalidates it)
+    while (ev_pool_.size() < static_cast<size_t>(8 * n + 8)) {
+        cudaEvent_t ev;
+        CK(cudaEventCreate(&ev));
+        ev_pool_.push_back(ev);
+    }
+    ev_used_ = 0;
+    prof_nb_ = &nb;
+    prof_pme_ = &pme;
+    cudaGraph_t g;
+    cudaGraphExec_t ge;
+    long long before = launches_;
+    cudaError_t e = cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+        for (int i = 0; i < n; ++i) enqueue_step();
+        e = cudaStreamEndCapture(stream_, &g);
+    }
+    prof_nb_ = nullptr;
+    prof_pme_ = nullptr;
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return check_cuda(e, "profiled capture");
+    }
+    CK(cudaGraphInstantiate(&ge, g, 0));
+    cudaGraphDestroy(g);
+    cudaEvent_t t0 = next_event(), t1 = next_event();
+    CK(cudaEventRecord(t0, stream_));
+    CK(cudaGraphLaunch(ge, stream_));
+    CK(cudaEventRecord(t1, stream_));
+    CK(cudaStreamSynchronize(stream_));
+    cudaGraphExecDestroy(ge);
+    float ms = 0.f;
+    double s_nb = 0.0, s_pme = 0.0;
+    for (auto& pr : nb) {
+        CK(cudaEventElapsedTime(&ms, pr.first, pr.second));
+        s_nb += ms;
+    }
+    for (auto& pr : pme) {
+        CK(cudaEventElapsedTime(&ms, pr.first, pr.second));
+        s_pme += ms;
+    }
+    CK(cudaEventElapsedTime(&ms, t0, t1));
+    if (nb_ms) *nb_ms = s_nb;
+    if (pme_ms) *pme_ms = s_pme;
+    if (total_ms) *total_ms = ms;
+    if (nb_launches) *nb_launches = static_cast<long long>(nb.size());
+    (void)before;
+    return sync_status();
+}
+
+int Batch::active() const {
+    int c = 0;
+    for (int k : order_)
+        if (reps_[k] && !reps_[k]->done) ++c;
+    return c;
+}
+
+int Batch::poll(int32_t* slots, int cap, int* n_done) {
+    int c = 0;
+    for (int s : finished_) {
+        if (c < cap && slots) slots[c] = s;
+        ++c;
+    }
+    *n_done = c;
+    finished_.clear();
+    return DMDGPU_OK;
+}
+
+// ---------------------------------------------------------------------------
+// State access
+// ---------------------------------------------------------------------------
+int Batch::get_state(int slot, int which, double* x, double* y, double* z) {
+    CK(cudaSetDevice(device_));
+    if (!has(slot)) return fail(DMDGPU_ERR_INVALID, "no such slot");
+    if (!packed_) {
+        int rc = pack();
+        if (rc) return rc;
+    }
+    const int k = replica_index(slot);
+    const HostRep& h = *reps_[slot];
+    const int a0 = h.rep.atom_begin, n = h.sys.n;
+    if (which == 0) {
+        CK(cudaStreamSynchronize(stream_));
+        CK(cudaMemcpy(x, dev_.x + a0, 8 * n, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(y, dev_.y + a0, 8 * n, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(z, dev_.z + a0, 8 * n, cudaMemcpyDeviceToHost));
+    } else if (which == 1) {
+        launch_finalize_velocities(dev_, stream_, &launches_);
+        CK(cudaStreamSynchronize(stream_));
+        CK(cudaMemcpy(x, dev_.vx + a0, 8 * n, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(y, dev_.vy + a0, 8 * n, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(z, dev_.vz + a0, 8 * n, cudaMemcpyDeviceToHost));
+    } else if (which == 2) {
+        CK(cudaStreamSynchronize(stream_));
+        const Rep& P = h.rep;
+        const int s0 = 32 * P.tile_begin, ns = 32 * P.n_tiles;
+        std::vector<long long> fb(3 * n), fn(3 * ns);
+        std::vector<int> sl(n);
+        CK(cudaMemcpy(fb.data(), dev_.fbx + a0, 8 * n, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(fb.data() + n, dev_.fby + a0, 8 * n, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(fb.data() + 2 * n, dev_.fbz + a0, 8 * n, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(fn.data(), dev_.fnx + s0, 8 * ns, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(fn.data() + ns, dev_.fny + s0, 8 * ns, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(fn.data() + 2 * ns, dev_.fnz + s0, 8 * ns, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(sl.data(), dev_.slot_of_atom + a0, 4 * n, cudaMemcpyDeviceToHost));
+        for (int i = 0; i < n; ++i) {
+            const int s = sl[i] - s0;
+            x[i] = static_cast<double>(fb[i] + fn[s]) * (1.0 / FSCALE);
+            y[i] = static_cast<double>(fb[n + i] + fn[ns + s]) * (1.0 / FSCALE);
+            z[i] = static_cast<double>(fb[2 * n + i] + fn[2 * ns + s]) * (1.0 / FSCALE);
+        }
+    } else {
+        return fail(DMDGPU_ERR_PARM, "which must be 0, 1 or 2");
+    }
+    (void)k;
+    return DMDGPU_OK;
+}
+
+int Batch::set_state(int slot, int which, const double* x, const double* y, const double* z) {
+    CK(cudaSetDevice(device_));
+    if (!has(slot)) return fail(DMDGPU_ERR_INVALID, "no such slot");
+    if (!packed_) {
+        int rc = pack();
+        if (rc) return rc;
+    }
+    HostRep& h = *reps_[slot];
+    const int a0 = h.rep.atom_begin, n = h.sys.n;
+    const int k = replica_index(slot);
+    CK(cudaStreamSynchronize(stream_));
+    if (which == 0) {
+        CK(cudaMemcpy(dev_.x + a0, x, 8 * n, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(dev_.y + a0, y, 8 * n, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(dev_.z + a0, z, 8 * n, cudaMemcpyHostToDevice));
+        // new positions: rebuild the list and recompute forces before the next kick
+        int one = 1, zero = 0;
+        CK(cudaMemcpy(&d_st_[k].rebuild, &one, 4, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(&d_st_[k].have_forces, &zero, 4, cudaMemcpyHostToDevice));
+        graph_dirty_ = true;  // the next step must evaluate forces first
+    } else if (which == 1) {
+        launch_finalize_velocities(dev_, stream_, &launches_);
+        CK(cudaStreamSynchronize(stream_));
+        CK(cudaMemcpy(dev_.vx + a0, x, 8 * n, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(dev_.vy + a0, y, 8 * n, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(dev_.vz + a0, z, 8 * n, cudaMemcpyHostToDevice));
+    } else {
+        return fail(DMDGPU_ERR_PARM, "which must be 0 or 1");
+    }
+    return DMDGPU_OK;
+}
+
+int Batch::get_scalars(int slot, dmdgpu_scalars* out) {
+    CK(cudaSetDevice(device_));
+    if (!has(slot)) return fail(DMDGPU_ERR_INVALID, "no such slot");
+    if (!packed_) {
+        int rc = pack();
+        if (rc) return rc;
+    }
+    const int k = replica_index(slot);
+    CK(cudaMemcpyAsync(h_st_ + k, d_st_ + k, sizeof(RepState), cudaMemcpyDeviceToHost, stream_));
+    CK(cudaStreamSynchronize(stream_));
+    const RepState& s = h_st_[k];
+    const HostRep& h = *reps_[slot];
+    const Rep& P = h.rep;
+    std::memset(out, 0, sizeof(*out));
+    out->step = s.step;
+    out->time = s.time;
+    out->box = s.L;
+    double e[8];
+    e[0] = static_cast<double>(s.e_acc[E_LJ]) / ESCALE;
+    e[1] = static_cast<double>(s.e_acc[E_CREAL]) / ESCALE;
+    e[2] = (P.flags & F_PME) ? s.e_recip : 0.0;
+    e[3] = (P.flags & F_PME) ? P.e_self : 0.0;
+    e[4] = static_cast<double>(s.e_acc[E_CEXCL]) / ESCALE;
+    e[5] = static_cast<double>(s.e_acc[E_BOND]) / ESCALE;
+    e[6] = static_cast<double>(s.e_acc[E_ANGLE]) / ESCALE;
+    e[7] = static_cast<double>(s.e_acc[E_DIH]) / ESCALE;
+    double pe = 0.0;
+    for (int t = 0; t < 8; ++t) {
+        out->e_terms[t] = e[t];
+        pe += e[t];
+    }
+    out->potential_energy = pe;
+    out->kinetic_energy = s.ke;
+    const double nn = static_cast<double>(h.sys.n);
+    out->temperature = h.sys.n < 2 ? 0.0 : 2.0 * s.ke / ((3.0 * nn - 3.0) * KB);
+    out->pressure = s.pressure;
+    out->virial = s.virial;
+    out->zeta = s.zeta;
+    out->list_builds = s.list_builds;
+    out->lj_step_since_rebuild = s.lj_counter;
+    out->status = s.status;
+    out->list_chunks = s.n_chunks;
+    return DMDGPU_OK;
+}
+
+int Batch::compute_forces(int slot, double* fx, double* fy, double* fz, double* e_terms) {
+    CK(cudaSetDevice(device_));
+    if (!has(slot)) return fail(DMDGPU_ERR_INVALID, "no such slot");
+    if (!packed_) {
+        int rc = pack();
+        if (rc) return rc;
+    }
+    const int k = replica_index(slot);
+    int one = 1;
+    CK(cudaStreamSynchronize(stream_));
+    CK(cudaMemcpy(&d_st_[k].rebuild, &one, 4, cudaMemcpyHostToDevice));
+    enqueue_eval(PASS_SINGLE);
+    launch_energy_reduce(dev_, stream_, &launches_);
+    CK(cudaGetLastError());
+    int rc = sync_status();
+    if (rc) return rc;
+    if (fx) {
+        rc = get_state(slot, 2, fx, fy, fz);
+        if (rc) return rc;
+    }
+    if (e_terms) {
+        dmdgpu_scalars s;
+        rc = get_scalars(slot, &s);
+        if (rc) return rc;
+        std::memcpy(e_terms, s.e_terms, sizeof(double) * 8);
+    }
+    return DMDGPU_OK;
+}
+
+int Batch::pair_list(int slot, int32_t* pi, int32_t* pj, long long cap, long long* count) {
+    CK(cudaSetDevice(device_));
+    if (!has(slot)) return fail(DMDGPU_ERR_INVALID, "no such slot");
+    if (!packed_) {
+        int rc = pack();
+        if (rc) return rc;
+    }
+    const int k = replica_index(slot);
+    const HostRep& h = *reps_[slot];
+    const Rep& P = h.rep;
+    CK(cudaStreamSynchronize(stream_));
+    RepState st;
+    CK(cudaMemcpy(&st, d_st_ + k, sizeof(RepState), cudaMemcpyDeviceToHost));
+    const int nc = st.n_chunks;
+    std::vector<int> it(nc);
+    std::vector<uint32_t> je(32LL * nc), mk(32LL * nc);
+    std::vector<int> aos(32 * P.n_tiles);
+    if (nc) {
+        CK(cudaMemcpy(it.data(), dev_.chunk_itile + P.chunk_begin, 4 * nc, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(je.data(), dev_.chunk_j + 32LL * P.chunk_begin, 128LL * nc, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(mk.data(), dev_.chunk_mask + 32LL * P.chunk_begin, 128LL * nc, cudaMemcpyDeviceToHost));
+    }
+    CK(cudaMemcpy(aos.data(), dev_.atom_of_slot + 32 * P.tile_begin, 4 * 32 * P.n_tiles, cudaMemcpyDeviceToHost));
+    const int s0 = 32 * P.tile_begin, a0 = P.atom_begin;
+    std::vector<std::pair<int, int>> pairs;
+    for (int c = 0; c < nc; ++c) {
+        const int I = it[c];
+        for (int l = 0; l < 32; ++l) {
+            uint32_t m = mk[32LL * c + l];
+            if (!m) continue;
+            const int js = static_cast<int>(je[32LL * c + l] & 0x03FFFFFFu);
+            const int aj = aos[js - s0] - a0;
+            for (; m; m &= m - 1) {
+                const int i = __builtin_ctz(m);
+                const int ai = aos[32 * I + i - s0] - a0;
+                pairs.emplace_back(std::min(ai, aj), std::max(ai, aj));
+            }
+        }
+    }
+    std::sort(pairs.begin(), pairs.end());
+    *count = static_cast<long long>(pairs.size());
+    for (long long p = 0; p < std::min<long long>(cap, *count); ++p) {
+        pi[p] = pairs[p].first;
+        pj[p] = pairs[p].second;
+    }
+    return DMDGPU_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Checkpoints: v1 layout of src/sim/checkpoint.cpp:9-38 plus a trailer.
+// ---------------------------------------------------------------------------
+namespace {
+constexpr uint32_t CK_MAGIC = 0x444D4450;   // checkpoint.cpp:6
+constexpr uint32_t CK_VERSION = 1;           // checkpoint.cpp:7
+constexpr uint32_t TR_MAGIC = 0x32474D44;    // trailer tag
+}  // namespace
+
+int Batch::save_checkpoint(int slot, const char* path) {
+    if (!has(slot)) return fail(DMDGPU_ERR_INVALID, "no such slot");
+    const HostRep& h = *reps_[slot];
+    const int n = h.sys.n;
+    std::vector<double> px(n), py(n), pz(n), vx(n), vy(n), vz(n), fx(n), fy(n), fz(n);
+    int rc = get_state(slot, 0, px.data(), py.data(), pz.data());
+    if (!rc) rc = get_state(slot, 1, vx.data(), vy.data(), vz.data());
+    if (!rc) rc = get_state(slot, 2, fx.data(), fy.data(), fz.data());
+    if (rc) return rc;
+    dmdgpu_scalars sc;
+    rc = get_scalars(slot, &sc);
+    if (rc) return rc;
+    std::ofstream os(path, std::ios::binary);
+    if (!os) return fail(DMDGPU_ERR_PARM, std::string("cannot open ") + path);
+    uint64_t nn = static_cast<uint64_t>(n);
+    uint64_t stp = static_cast<uint64_t>(sc.step);
+    double tm = sc.time, pe = sc.potential_energy;
+    os.write(reinterpret_cast<const char*>(&CK_MAGIC), 4);
+    os.write(reinterpret_cast<const char*>(&CK_VERSION), 4);
+    os.write(reinterpret_cast<const char*>(&nn), 8);
+    os.write(reinterpret_cast<const char*>(&stp), 8);
+    os.write(reinterpret_cast<const char*>(&tm), 8);
+    os.write(reinterpret_cast<const char*>(&pe), 8);
+    for (auto* v : {&px, &py, &pz, &vx, &vy, &vz, &fx, &fy, &fz})
+        os.write(reinterpret_cast<const char*>(v->data()), 8 * n);
+    os.write(reinterpret_cast<const char*>(h.sys.mass.data()), 8 * n);
+    os.write(reinterpret_cast<const char*>(h.sys.q.data()), 8 * n);
+    os.write(reinterpret_cast<const char*>(h.sys.type.data()), 4 * n);
+    int32_t ljc = sc.lj_step_since_rebuild;
+    os.write(reinterpret_cast<const char*>(&ljc), 4);
+    // trailer: box, Nose-Hoover zeta, Andersen call counter, profile
+    uint32_t tv = 2;
+    double box = sc.box, zeta = sc.zeta;
+    int k = replica_index(slot);
+    int64_t acalls = h_st_[k].andersen_calls;
+    int32_t prof = phys_ ? 1 : 0;
+    uint32_t aseed = h.andersen_seed;
+    os.write(reinterpret_cast<const char*>(&TR_MAGIC), 4);
+    os.write(reinterpret_cast<const char*>(&tv), 4);
+    os.write(reinterpret_cast<const char*>(&box), 8);
+    os.write(reinterpret_cast<const char*>(&zeta), 8);
+    os.write(reinterpret_cast<const char*>(&acalls), 8);
+    os.write(reinterpret_cast<const char*>(&aseed), 4);
+    os.write(reinterpret_cast<const char*>(&prof), 4);
+    return os.good() ? DMDGPU_OK : fail(DMDGPU_ERR_PARM, "checkpoint write failed");
+}
+
+int Batch::load_checkpoint(int slot, const char* path) {
+    CK(cudaSetDevice(device_));
+    if (!has(slot)) return fail(DMDGPU_ERR_INVALID, "no such slot");
+    if (!packed_) {
+        int rc = pack();
+        if (rc) return rc;
+    }
+    std::ifstream is(path, std::ios::binary);
+    if (!is) return fail(DMDGPU_ERR_PARM, std::string("cannot open ") + path);
+    HostRep& h = *reps_[slot];
+    const int n = h.sys.n;
+    uint32_t magic = 0, version = 0;
+    uint64_t nn = 0, stp = 0;
+    double tm = 0, pe = 0;
+    is.read(reinterpret_cast<char*>(&magic), 4);
+    is.read(reinterpret_cast<char*>(&version), 4);
+    is.read(reinterpret_cast<char*>(&nn), 8);
+    if (!is || nn != static_cast<uint64_t>(n))
+        return fail(DMDGPU_ERR_MISMATCH, "checkpoint atom count differs from the system");
+    is.read(reinterpret_cast<char*>(&stp), 8);
+    is.read(reinterpret_cast<char*>(&tm), 8);
+    is.read(reinterpret_cast<char*>(&pe), 8);
+    std::vector<double> v[11];
+    for (int i = 0; i < 11; ++i) {
+        v[i].resize(n);
+        is.read(reinterpret_cast<char*>(v[i].data()), 8 * n);
+    }
+    std::vector<int> types(n);
+    is.read(reinterpret_cast<char*>(types.data()), 4 * n);
+    int32_t ljc = 0;
+    is.read(reinterpret_cast<char*>(&ljc), 4);
+    if (!is) return fail(DMDGPU_ERR_MISMATCH, "truncated checkpoint");
+    uint32_t tmagic = 0, tv = 0;
+    double box = 0, zeta = 0;
+    int64_t acalls = 0;
+    uint32_t aseed = 42;
+    int32_t prof = -1;
+    bool trailer = false;
+    if (is.read(reinterpret_cast<char*>(&tmagic), 4) && tmagic == TR_MAGIC) {
+        is.read(reinterpret_cast<char*>(&tv), 4);
+        is.read(reinterpret_cast<char*>(&box), 8);
+        is.read(reinterpret_cast<char*>(&zeta), 8);
+        is.read(reinterpret_cast<char*>(&acalls), 8);
+        is.read(reinterpret_cast<char*>(&aseed), 4);
+        is.read(reinterpret_cast<char*>(&prof), 4);
+        trailer = static_cast<bool>(is);
+    }
+    const int k = replica_index(slot);
+    const int a0 = h.rep.atom_begin;
+    CK(cudaStreamSynchronize(stream_));
+    double* dst[6] = {dev_.x, dev_.y, dev_.z, dev_.vx, dev_.vy, dev_.vz};
+    for (int i = 0; i < 6; ++i) CK(cudaMemcpy(dst[i] + a0, v[i].data(), 8 * n, cudaMemcpyHostToDevice));
+    // SystemData masses are restored (checkpoint.cpp:66); the components keep the
+    // charges / types they were built with.
+    h.sys.mass = v[9];
+    CK(cudaMemcpy(const_cast<double*>(dev_.mass) + a0, v[9].data(), 8 * n, cudaMemcpyHostToDevice));
+    RepState st;
+    CK(cudaMemcpy(&st, d_st_ + k, sizeof(RepState), cudaMemcpyDeviceToHost));
+    st.step = static_cast<long long>(stp);
+    st.time = tm;
+    st.lj_counter = ljc;
+    st.rebuild = 1;
+    st.have_forces = 0;
+    st.vscale = 1.0;
+    st.target_step = st.step;
+    if (trailer) {
+        st.L = box;
+        st.invL = 1.0 / box;
+        st.zeta = zeta;
+        st.andersen_calls = acalls;
+        h.andersen_seed = aseed;
+    }
+    CK(cudaMemcpy(d_st_ + k, &st, sizeof(RepState), cudaMemcpyHostToDevice));
+    h.target = st.step;
+    h.done = false;
+    graph_dirty_ = true;  // the next step must evaluate forces first
+    return DMDGPU_OK;
+}
+
+}  // namespace dmd

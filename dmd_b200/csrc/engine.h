@@ -1,0 +1,156 @@
+// engine.h -- host orchestration of the device path (one Batch = one packed table).
+#pragma once
+
+#include <cufft.h>
+
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/dmdgpu.h"
+#include "layout.h"
+
+namespace dmd {
+
+// Component selection for single-component evaluation (ForceComponent parity).
+enum CompMask : unsigned {
+    C_LJ = 1u << 0, C_BOND = 1u << 1, C_ANGLE = 1u << 2, C_DIH = 1u << 3, C_CREAL = 1u << 4,
+    C_PME = 1u << 5, C_EXCL = 1u << 6, C_ALL = 0x7fu
+};
+
+// Host copy of one system (a SimulationConfig) plus its packing metadata.
+struct HostSystem {
+    int n = 0;
+    double box = 0;
+    std::vector<double> mass, q, x, y, z, vx, vy, vz;
+    std::vector<int> type;
+    int use_lj = 0, n_types = 0;
+    std::vector<double> sigma, eps;
+    double lj_cutoff = 1.2;
+    std::vector<int> bi, bj;
+    std::vector<double> bk, br0;
+    std::vector<int> ai, aj, ak;
+    std::vector<double> akt, at0;
+    std::vector<int> di, dj, dk, dl, dn;
+    std::vector<double> dkp, dp0;
+    std::vector<int> ei, ej;
+    int coulomb_type = 0;
+    double coul_cutoff = 1.2, ewald = 0.34, spacing = 0.12;
+    int pme_order = 4, pme_K = 0;
+    double dt = 0.002;
+    int n_steps = 0;
+    int thermostat = 0;
+    double t_temp = 300, t_tau = 0.1, t_freq = 10;
+    int barostat = 0;
+    double b_pressure = 1, b_tau = 1, b_compress = 4.5e-5;
+    int checkpoint_interval = 0;
+    std::string checkpoint_path;
+};
+
+// Per-replica bookkeeping kept on the host.
+struct HostRep {
+    HostSystem sys;
+    Rep rep{};
+    RepState init{};
+    long long target = 0;      // step count to reach (served jobs)
+    unsigned andersen_seed = 42;
+    bool done = false;
+    bool polled = false;
+};
+
+struct DeviceArena {
+    std::vector<void*> ptrs;
+    size_t bytes = 0;
+    ~DeviceArena();
+    template <typename T>
+    T* alloc(size_t n);
+};
+
+class Batch {
+  public:
+    Batch(const dmdgpu_options& opt, long long budget_bytes);
+    ~Batch();
+
+    // Replica management (host side; the device table is rebuilt by pack()).
+    int add(const dmdgpu_system& sys, long long n_steps, unsigned comp_mask, int* slot);
+    int release(int slot);
+    int pack();                 // (re)build the packed device table from host replicas
+    long long footprint(const HostSystem& s) const;
+
+    int step(int n);            // advance every running replica by up to n steps
+    int extend_targets(long long n);  // single-system API: allow n more steps
+    int step_profiled(int n, double* nb_ms, double* pme_ms, double* total_ms, long long* nb_launches);
+    cudaStream_t stream() const { return stream_; }
+    int compute_forces(int slot, double* fx, double* fy, double* fz, double* e_terms);
+    int get_state(int slot, int which, double* x, double* y, double* z);
+    int set_state(int slot, int which, const double* x, const double* y, const double* z);
+    int get_scalars(int slot, dmdgpu_scalars* out);
+    int pair_list(int slot, int32_t* pi, int32_t* pj, long long cap, long long* count);
+    int save_checkpoint(int slot, const char* path);
+    int load_checkpoint(int slot, const char* path);
+    int poll(int32_t* slots, int cap, int* n_done);
+
+    long long used_bytes() const { return used_bytes_; }
+    long long launches() const { return launches_; }
+    int active() const;
+    const std::string& error() const { return err_; }
+    int fail(int code, const std::string& msg);
+    const HostSystem& system(int slot) const { return reps_.at(slot)->sys; }
+    bool has(int slot) const { return slot >= 0 && slot < (int)reps_.size() && reps_[slot]; }
+
+  private:
+    int check_cuda(cudaError_t e, const char* what);
+    int build_host(HostRep& hr, unsigned comp_mask);
+    void enqueue_eval(int pass);
+    void enqueue_rebuild();
+    void enqueue_step();
+    int run_steps(int n);
+    int sync_status();
+    int replica_index(int slot) const;
+    void free_device();
+    void andersen_ref_prepare();
+
+    dmdgpu_options opt_;
+    long long budget_;
+    bool fp64_, phys_;
+    int device_ = 0, n_sm_ = 148;
+    cudaStream_t stream_ = nullptr, body_stream_ = nullptr;
+    bool capture_error_ = false;
+    std::vector<std::unique_ptr<HostRep>> reps_;   // indexed by slot (nullptr = free)
+    std::vector<int> order_;                        // packed replica index -> slot
+    std::unique_ptr<DeviceArena> arena_;
+    Dev dev_{};
+    Rep* d_rep_ = nullptr;
+    RepState* d_st_ = nullptr;
+    RepState* h_st_ = nullptr;                      // pinned mirror of the state table
+    int* d_bin_rep_ = nullptr;
+    long long n_fix_total_ = 0;
+    int n_pme_blocks_ = 0;
+    bool any_pme_ = false, any_baro_ = false, any_ref_lj_ = false, any_andersen_ref_ = false,
+         any_andersen_phys_ = false;
+    std::map<int, std::pair<cufftHandle, cufftHandle>> plans_;
+    cudaGraphExec_t graph_ = nullptr;
+    bool packed_ = false;
+    bool graph_dirty_ = true;
+    bool need_eval1_ = true;
+    long long launches_ = 0;
+    long long per_step_launches_ = 0;
+    long long body_runs_seen_ = 0;
+    long long used_bytes_ = 0;
+    // per-kernel timing (step_profiled): event pairs recorded around launches
+    std::vector<cudaEvent_t> ev_pool_;
+    size_t ev_used_ = 0;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>>* prof_nb_ = nullptr;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>>* prof_pme_ = nullptr;
+    cudaEvent_t next_event();
+    std::string err_;
+    std::vector<int> finished_;
+    // Andersen REF override buffers
+    int* h_and_flag_ = nullptr;
+    double* h_and_v_ = nullptr;
+    int* d_and_flag_ = nullptr;
+    double* d_and_v_ = nullptr;
+};
+
+}  // namespace dmd

@@ -1,0 +1,416 @@
+// k_integrate.cu -- Velocity Verlet with fused thermostat / barostat bookkeeping.
+//
+// Reference sequence (SimulationEngine::step, src/sim/simulation_engine.cpp:53-86):
+//   compute; half_kick; advance; compute; half_kick; thermostat; barostat.
+// Device form (per step, every replica of the batch in the same launches):
+//   k_step_begin        which replicas advance
+//   [eval #1]           only where the first evaluation would differ from the
+//                       previous step's second one (barostat moved the atoms,
+//                       no forces yet, or the REF list cadence rebuilds now)
+//   k_kick_drift        pending thermostat scale, half kick, drift, clear forces,
+//                       write the sorted FP32/FP64 mirror, skin check
+//   [eval #2]
+//   k_kick2             half kick (+ Andersen), per-tile KE / virial partials
+//   k_replica_update    KE, thermostat (Berendsen / Nose-Hoover scale, applied
+//                       lazily in the next kick), Berendsen barostat factor
+//   k_apply_scale       barostat position scaling (only when a barostat exists)
+// Integration arithmetic is FP64 with the reference's operation order
+// (src/integrate/integrator.cpp:4-20) and no FMA contraction.
+#include "device.cuh"
+#include "launch.h"
+
+namespace dmd {
+
+namespace {
+
+__global__ void k_step_begin(Dev d) {
+    int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= d.n_rep) return;
+    RepState* s = d.st + r;
+    s->active = (s->step < s->target_step) ? 1 : 0;
+    s->pscale = 1.0;
+}
+
+__global__ void k_eval_begin(Dev d, int pass) {
+    int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= d.n_rep) return;
+    RepState* s = d.st + r;
+    const Rep& R = d.rep[r];
+    const bool ref_lj = !(R.flags & F_PHYS) && (R.flags & F_LJ);
+    int ev;
+    if (pass == PASS_FIRST) {
+        ev = s->active && (R.barostat != 0 || !s->have_forces || (ref_lj && s->lj_counter >= 10));
+        // LennardJones::compute advances its counter on every call (lennard_jones.cpp:91)
+        if (s->active && !ev && ref_lj) s->lj_counter += 1;
+    } else if (pass == PASS_SECOND) {
+        ev = s->active;
+        s->vscale = 1.0;  // consumed by k_kick_drift
+    } else {
+        ev = 1;
+    }
+    s->eval = ev;
+    if (ev) {
+        for (int k = 0; k < N_EACC; ++k) s->e_acc[k] = 0;
+        s->e_recip = 0.0;
+        s->vir_recip = 0.0;
+        if (ref_lj && s->lj_counter >= 10) s->rebuild = 1;
+    }
+}
+
+__global__ void k_eval_end(Dev d) {
+    int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= d.n_rep) return;
+    RepState* s = d.st + r;
+    const Rep& R = d.rep[r];
+    if (!s->eval) return;
+    if (!(R.flags & F_PHYS) && (R.flags & F_LJ)) s->lj_counter += 1;
+    s->have_forces = 1;
+}
+
+__global__ void k_clear_forces(Dev d) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < d.n_slots) {
+        int r = d.tile_rep[i >> 5];
+        if (d.st[r].eval) {
+            d.fnx[i] = 0;
+            d.fny[i] = 0;
+            d.fnz[i] = 0;
+        }
+    }
+    if (i < d.n_atoms) {
+        int r = d.atom_rep[i];
+        if (d.st[r].eval) {
+            d.fbx[i] = 0;
+            d.fby[i] = 0;
+            d.fbz[i] = 0;
+        }
+    }
+}
+
+__device__ __forceinline__ void write_mirror(const Dev& d, int slot, int a, double x, double y, double z,
+                                             double L) {
+    if (d.xq32) {
+        const int t = slot >> 5;
+        d.xq32[slot] = make_float4(static_cast<float>((x - d.imgx[a] * L) - d.tcx[t]),
+                                   static_cast<float>((y - d.imgy[a] * L) - d.tcy[t]),
+                                   static_cast<float>((z - d.imgz[a] * L) - d.tcz[t]),
+                                   static_cast<float>(d.q[a]));
+    }
+    if (d.xq64) d.xq64[slot] = make_double4(x, y, z, d.q[a]);
+}
+
+__device__ __forceinline__ void skin_check(const Dev& d, RepState* s, const Rep& R, int a, double x,
+                                           double y, double z) {
+    if (!(R.flags & F_PHYS)) return;
+    const double dx = x - d.xr[a], dy = y - d.yr[a], dz = z - d.zr[a];
+    if (dx * dx + dy * dy + dz * dz > R.half_skin2) s->rebuild = 1;
+}
+
+// Integrator::half_kick + advance (integrator.cpp:4-20), with the pending
+// thermostat scale of the previous step applied first.
+__global__ void k_kick_drift(Dev d) {
+    const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= d.n_slots) return;
+    const int r = d.tile_rep[slot >> 5];
+    RepState* s = d.st + r;
+    if (!s->active) return;
+    const int a = d.atom_of_slot[slot];
+    if (a < 0) return;
+    const Rep& R = d.rep[r];
+    const double dt = R.dt, half_dt = 0.5 * dt;
+    const double inv_mass = 1.0 / d.mass[a];
+    const double lam = s->vscale;
+    const double fx = from_fix(d.fnx[slot] + d.fbx[a], FSCALE);
+    const double fy = from_fix(d.fny[slot] + d.fby[a], FSCALE);
+    const double fz = from_fix(d.fnz[slot] + d.fbz[a], FSCALE);
+    double vx = __dmul_rn(d.vx[a], lam), vy = __dmul_rn(d.vy[a], lam), vz = __dmul_rn(d.vz[a], lam);
+    vx = __dadd_rn(vx, __dmul_rn(__dmul_rn(fx, inv_mass), half_dt));
+    vy = __dadd_rn(vy, __dmul_rn(__dmul_rn(fy, inv_mass), half_dt));
+    vz = __dadd_rn(vz, __dmul_rn(__dmul_rn(fz, inv_mass), half_dt));
+    const double x = __dadd_rn(d.x[a], __dmul_rn(vx, dt));
+    const double y = __dadd_rn(d.y[a], __dmul_rn(vy, dt));
+    const double z = __dadd_rn(d.z[a], __dmul_rn(vz, dt));
+    d.vx[a] = vx;
+    d.vy[a] = vy;
+    d.vz[a] = vz;
+    d.x[a] = x;
+    d.y[a] = y;
+    d.z[a] = z;
+    d.fnx[slot] = 0;
+    d.fny[slot] = 0;
+    d.fnz[slot] = 0;
+    d.fbx[a] = 0;
+    d.fby[a] = 0;
+    d.fbz[a] = 0;
+    write_mirror(d, slot, a, x, y, z, s->L);
+    skin_check(d, s, R, a, x, y, z);
+}
+
+// Philox4x32-10 (Salmon et al., SC'11) for the PHYS Andersen thermostat.
+__device__ __forceinline__ void philox(uint32_t c[4], uint32_t k0, uint32_t k1) {
+#pragma unroll
+    for (int i = 0; i < 10; ++i) {
+        const uint32_t hi0 = __umulhi(0xD2511F53u, c[0]), lo0 = 0xD2511F53u * c[0];
+        const uint32_t hi1 = __umulhi(0xCD9E8D57u, c[2]), lo1 = 0xCD9E8D57u * c[2];
+        const uint32_t n0 = hi1 ^ c[1] ^ k0, n2 = hi0 ^ c[3] ^ k1;
+        c[0] = n0;
+        c[1] = lo1;
+        c[2] = n2;
+        c[3] = lo0;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+}
+
+// Second half kick, optional Andersen collisions, per-tile KE and r.F partials.
+__global__ void k_kick2(Dev d, int andersen_ref, int andersen_phys) {
+    const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    const int t = slot >> 5;
+    const int r = (t < d.n_tiles) ? d.tile_rep[t] : 0;
+    RepState* s = d.st + r;
+    double ke = 0.0, w = 0.0;
+    if (slot < d.n_slots && s->active) {
+        const int a = d.atom_of_slot[slot];
+        if (a >= 0) {
+            const Rep& R = d.rep[r];
+            const double half_dt = 0.5 * R.dt;
+            const double m = d.mass[a];
+            const double inv_mass = 1.0 / m;
+            const double fx = from_fix(d.fnx[slot] + d.fbx[a], FSCALE);
+            const double fy = from_fix(d.fny[slot] + d.fby[a], FSCALE);
+            const double fz = from_fix(d.fnz[slot] + d.fbz[a], FSCALE);
+            double vx = __dadd_rn(d.vx[a], __dmul_rn(__dmul_rn(fx, inv_mass), half_dt));
+            double vy = __dadd_rn(d.vy[a], __dmul_rn(__dmul_rn(fy, inv_mass), half_dt));
+            double vz = __dadd_rn(d.vz[a], __dmul_rn(__dmul_rn(fz, inv_mass), half_dt));
+            if (R.thermostat == 3 && R.t_freq * R.dt > 0.0) {
+                if (andersen_ref && d.and_flag && d.and_flag[a]) {
+                    vx = d.and_v[3 * a];
+                    vy = d.and_v[3 * a + 1];
+                    vz = d.and_v[3 * a + 2];
+                } else if (andersen_phys && (R.flags & F_PHYS)) {
+                    const uint32_t call = static_cast<uint32_t>(s->andersen_calls);
+                    const uint32_t callh = static_cast<uint32_t>(s->andersen_calls >> 32);
+                    const uint32_t li = static_cast<uint32_t>(a - R.atom_begin);
+                    uint32_t c[4] = {li, call, callh, 0x414E4400u};
+                    philox(c, R.key0, R.key1);
+                    const double u = c[0] * 2.3283064365386963e-10;
+                    if (u < R.t_freq * R.dt) {
+                        const double sg = sqrt(KB * R.t_temp / m);
+                        const double u1 = (c[1] + 1.0) * 2.3283064365386963e-10;
+                        const double u2 = c[2] * 2.3283064365386963e-10;
+                        const double rr = sqrt(-2.0 * log(u1));
+                        uint32_t e[4] = {li, call, callh, 0x414E4401u};
+                        philox(e, R.key0, R.key1);
+                        const double u3 = (e[0] + 1.0) * 2.3283064365386963e-10;
+                        const double u4 = e[1] * 2.3283064365386963e-10;
+                        vx = rr * cos(2.0 * PI * u2) * sg;
+                        vy = rr * sin(2.0 * PI * u2) * sg;
+                        vz = sqrt(-2.0 * log(u3)) * cos(2.0 * PI * u4) * sg;
+                    }
+                }
+            }
+            d.vx[a] = vx;
+            d.vy[a] = vy;
+            d.vz[a] = vz;
+            // kinetic_energy (thermostat.cpp:6-15) and virial (barostat.cpp:6-14) terms
+            ke = __dmul_rn(__dmul_rn(0.5, m),
+                           __dadd_rn(__dadd_rn(__dmul_rn(vx, vx), __dmul_rn(vy, vy)), __dmul_rn(vz, vz)));
+            w = __dadd_rn(__dadd_rn(__dmul_rn(d.x[a], fx), __dmul_rn(d.y[a], fy)), __dmul_rn(d.z[a], fz));
+        }
+    }
+    ke = warp_sum_d(ke);
+    w = warp_sum_d(w);
+    if (lane == 0 && t < d.n_tiles) {
+        d.tile_ke[t] = ke;
+        d.tile_vir[t] = w;
+    }
+}
+
+__device__ double block_sum(double v, double* sh) {
+    sh[threadIdx.x] = v;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+        __syncthreads();
+    }
+    double r = sh[0];
+    __syncthreads();
+    return r;
+}
+
+// PME energy / virial partial sums of replica r (fixed order).
+__device__ void reduce_pme(const Dev& d, int r, double* sh) {
+    const Rep& R = d.rep[r];
+    double e = 0.0, v = 0.0;
+    if (R.flags & F_PME) {
+        for (int b = threadIdx.x; b < R.pme_blocks; b += blockDim.x) {
+            e += d.pme_part[2 * (R.pme_block_begin + b)];
+            v += d.pme_part[2 * (R.pme_block_begin + b) + 1];
+        }
+    }
+    e = block_sum(e, sh);
+    v = block_sum(v, sh);
+    if (threadIdx.x == 0) {
+        d.st[r].e_recip = e;
+        d.st[r].vir_recip = v;
+    }
+}
+
+__global__ void k_energy_reduce(Dev d) {
+    __shared__ double sh[256];
+    const int r = blockIdx.x;
+    if (!d.st[r].eval) return;
+    reduce_pme(d, r, sh);
+}
+
+// Thermostat (berendsen.cpp:13-28, nose_hoover.cpp:6-32) and Berendsen barostat
+// (berendsen_barostat.cpp:14-66); one block per replica.
+__global__ void k_replica_update(Dev d) {
+    __shared__ double sh[256];
+    const int r = blockIdx.x;
+    RepState* s = d.st + r;
+    if (!s->active) return;
+    const Rep& R = d.rep[r];
+    double ke = 0.0, w = 0.0;
+    for (int t = R.tile_begin + threadIdx.x; t < R.tile_begin + R.n_tiles; t += blockDim.x) {
+        ke += d.tile_ke[t];
+        w += d.tile_vir[t];
+    }
+    ke = block_sum(ke, sh);
+    w = block_sum(w, sh);
+    reduce_pme(d, r, sh);
+    if (threadIdx.x != 0) return;
+    const double n = static_cast<double>(R.n_atoms);
+    const double dt = R.dt;
+    auto temp = [&](double ek) { return R.n_atoms < 2 ? 0.0 : 2.0 * ek / ((3.0 * n - 3.0) * KB); };
+    double lam = 1.0;
+    if (R.thermostat == 1) {
+        if (R.t_tau > 0.0 && ke > 0.0) {
+            const double T = temp(ke);
+            const double l = sqrt(1.0 + dt / R.t_tau * (R.t_temp / T - 1.0));
+            if (!(l <= 0.0)) lam = l;
+        }
+    } else if (R.thermostat == 2) {
+        const double T = temp(ke);
+        s->zeta += 0.5 * dt * KB * (T - R.t_temp) / R.nh_Q;
+        lam = exp(-s->zeta * 0.5 * dt);
+    } else if (R.thermostat == 3) {
+        if (R.t_freq * dt > 0.0) s->andersen_calls += 1;
+    }
+    s->vscale = lam;
+    const double ke_after = ke * lam * lam;
+    s->ke = ke_after;
+    const double L = s->L;
+    const double V = L * (L * L);
+    double W;
+    if (R.flags & F_PHYS) W = from_fix(s->e_acc[E_VIR], ESCALE) + s->vir_recip;
+    else W = w;
+    s->virial = W;
+    s->pressure = (V <= 0.0) ? 0.0 : (2.0 * ke_after + W) / (3.0 * V);
+    if (R.barostat == 1 && R.b_tau > 0.0 && V > 0.0) {
+        double mu;
+        if (R.flags & F_PHYS) mu = 1.0 - (dt / R.b_tau) * R.b_compress * (R.b_pressure - s->pressure / BAR);
+        else mu = 1.0 - (dt / R.b_tau) * (R.b_compress / BAR) * (R.b_pressure - s->pressure);
+        if (mu <= 0.0) mu = 0.0;
+        const double sc = cbrt(mu);
+        s->pscale = sc;
+        s->L = L * sc;
+        s->invL = 1.0 / s->L;
+    }
+    s->step += 1;
+    s->time += dt;
+}
+
+// BerendsenBarostat position scaling (berendsen_barostat.cpp:60-65).
+__global__ void k_apply_scale(Dev d) {
+    const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= d.n_slots) return;
+    const int r = d.tile_rep[slot >> 5];
+    RepState* s = d.st + r;
+    if (!s->active || s->pscale == 1.0) return;
+    const int a = d.atom_of_slot[slot];
+    if (a < 0) return;
+    const double sc = s->pscale;
+    const double x = d.x[a] * sc, y = d.y[a] * sc, z = d.z[a] * sc;
+    d.x[a] = x;
+    d.y[a] = y;
+    d.z[a] = z;
+    write_mirror(d, slot, a, x, y, z, s->L);
+    skin_check(d, s, d.rep[r], a, x, y, z);
+}
+
+__global__ void k_finalize_v(Dev d) {
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= d.n_atoms) return;
+    const double lam = d.st[d.atom_rep[a]].vscale;
+    if (lam == 1.0) return;
+    d.vx[a] = __dmul_rn(d.vx[a], lam);
+    d.vy[a] = __dmul_rn(d.vy[a], lam);
+    d.vz[a] = __dmul_rn(d.vz[a], lam);
+}
+
+__global__ void k_finalize_reset(Dev d) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r < d.n_rep) d.st[r].vscale = 1.0;
+}
+
+__global__ void k_write_mirror(Dev d) {
+    const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= d.n_slots) return;
+    const int a = d.atom_of_slot[slot];
+    if (a < 0) return;
+    const int r = d.tile_rep[slot >> 5];
+    write_mirror(d, slot, a, d.x[a], d.y[a], d.z[a], d.st[r].L);
+}
+
+}  // namespace
+
+void launch_step_begin(const Dev& d, cudaStream_t st, long long* n) {
+    k_step_begin<<<(d.n_rep + 127) / 128, 128, 0, st>>>(d);
+    ++*n;
+}
+void launch_eval_begin(const Dev& d, int pass, cudaStream_t st, long long* n) {
+    k_eval_begin<<<(d.n_rep + 127) / 128, 128, 0, st>>>(d, pass);
+    ++*n;
+}
+void launch_clear_forces(const Dev& d, cudaStream_t st, long long* n) {
+    const int m = d.n_slots > d.n_atoms ? d.n_slots : d.n_atoms;
+    k_clear_forces<<<(m + 255) / 256, 256, 0, st>>>(d);
+    ++*n;
+}
+void launch_eval_end(const Dev& d, cudaStream_t st, long long* n) {
+    k_eval_end<<<(d.n_rep + 127) / 128, 128, 0, st>>>(d);
+    ++*n;
+}
+void launch_kick_drift(const Dev& d, bool, cudaStream_t st, long long* n) {
+    k_kick_drift<<<(d.n_slots + 255) / 256, 256, 0, st>>>(d);
+    ++*n;
+}
+void launch_kick2(const Dev& d, bool andersen_ref, bool andersen_phys, cudaStream_t st, long long* n) {
+    k_kick2<<<(d.n_slots + 255) / 256, 256, 0, st>>>(d, andersen_ref ? 1 : 0, andersen_phys ? 1 : 0);
+    ++*n;
+}
+void launch_replica_update(const Dev& d, cudaStream_t st, long long* n) {
+    k_replica_update<<<d.n_rep, 256, 0, st>>>(d);
+    ++*n;
+}
+void launch_apply_scale(const Dev& d, bool, cudaStream_t st, long long* n) {
+    k_apply_scale<<<(d.n_slots + 255) / 256, 256, 0, st>>>(d);
+    ++*n;
+}
+void launch_finalize_velocities(const Dev& d, cudaStream_t st, long long* n) {
+    k_finalize_v<<<(d.n_atoms + 255) / 256, 256, 0, st>>>(d);
+    k_finalize_reset<<<(d.n_rep + 127) / 128, 128, 0, st>>>(d);
+    *n += 2;
+}
+void launch_energy_reduce(const Dev& d, cudaStream_t st, long long* n) {
+    k_energy_reduce<<<d.n_rep, 256, 0, st>>>(d);
+    ++*n;
+}
+void launch_write_mirror(const Dev& d, bool, cudaStream_t st, long long* n) {
+    k_write_mirror<<<(d.n_slots + 255) / 256, 256, 0, st>>>(d);
+    ++*n;
+}
+
+}  // namespace dmd

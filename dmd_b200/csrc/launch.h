@@ -1,0 +1,47 @@
+// launch.h -- host-side launchers of the kernel translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "layout.h"
+
+namespace dmd {
+
+// k_list.cu: rebuild pipeline for replicas whose `rebuild` flag is set.  The
+// flag kernel resets their list counters and (in a graph) sets `cond` to
+// whether any replica rebuilds; the body kernels are no-ops for the others.
+void launch_rebuild_flag(const Dev& d, cudaGraphConditionalHandle cond, bool use_cond, cudaStream_t st,
+                         long long* nlaunch);
+void launch_rebuild_body(const Dev& d, const int* bin_rep, bool in_graph, cudaStream_t st,
+                         long long* nlaunch);
+
+// k_nonbonded.cu: LJ + real-space Ewald over the chunk list (replicas with `eval`).
+void launch_nonbonded(const Dev& d, bool fp64, bool phys, int n_sm, cudaStream_t st,
+                      long long* nlaunch);
+
+// k_forces.cu
+// bonds, angles, dihedrals and the exclusion correction in one launch
+void launch_bonded(const Dev& d, bool fp64, bool phys, cudaStream_t st, long long* nlaunch);
+void launch_pme_spread(const Dev& d, bool fp64, cudaStream_t st, long long* nlaunch);
+void launch_pme_convert(const Dev& d, bool fp64, long long n_fix_total, cudaStream_t st,
+                        long long* nlaunch);
+void launch_pme_influence(const Dev& d, bool fp64, int n_blocks, cudaStream_t st,
+                          long long* nlaunch);
+void launch_pme_gather(const Dev& d, bool fp64, cudaStream_t st, long long* nlaunch);
+
+// k_integrate.cu
+enum EvalPass { PASS_FIRST = 1, PASS_SECOND = 2, PASS_SINGLE = 3 };
+void launch_step_begin(const Dev& d, cudaStream_t st, long long* nlaunch);
+void launch_eval_begin(const Dev& d, int pass, cudaStream_t st, long long* nlaunch);
+void launch_clear_forces(const Dev& d, cudaStream_t st, long long* nlaunch);
+void launch_eval_end(const Dev& d, cudaStream_t st, long long* nlaunch);
+void launch_kick_drift(const Dev& d, bool fp64, cudaStream_t st, long long* nlaunch);
+void launch_kick2(const Dev& d, bool andersen_ref, bool andersen_phys, cudaStream_t st,
+                  long long* nlaunch);
+void launch_replica_update(const Dev& d, cudaStream_t st, long long* nlaunch);
+void launch_apply_scale(const Dev& d, bool fp64, cudaStream_t st, long long* nlaunch);
+void launch_finalize_velocities(const Dev& d, cudaStream_t st, long long* nlaunch);
+void launch_energy_reduce(const Dev& d, cudaStream_t st, long long* nlaunch);
+void launch_write_mirror(const Dev& d, bool fp64, cudaStream_t st, long long* nlaunch);
+
+}  // namespace dmd

@@ -1,0 +1,154 @@
+// layout.h -- device data layout shared by the kernels and the host engine.
+//
+// A "batch" packs R independent systems (replicas) into one set of device
+// arrays.  Replica r owns
+//   atoms  [atom_begin, atom_begin + n_atoms)          reference atom order, FP64 state
+//   tiles  [tile_begin, tile_begin + n_tiles)          32 sorted slots per tile
+//   slots  [32*tile_begin, 32*(tile_begin + n_tiles))  spatially sorted mirror
+//   bins   [bin_begin, bin_begin + nvx^2 nvz)          snake-ranked sort cells
+//   chunks [chunk_begin, chunk_begin + chunk_cap)      pair list segment
+//   mesh   PME buffers at per-replica offsets
+// A single system is a batch of one.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace dmd {
+
+constexpr double KB = 0.008314462618;   // kJ mol^-1 K^-1 (src/core/constants.h:6)
+constexpr double KE = 138.935456;       // kJ mol^-1 nm e^-2 (coulomb_pme.h:45)
+constexpr double PI = 3.14159265358979323846;
+constexpr double BAR = 0.0602214086;    // kJ mol^-1 nm^-3 per bar
+
+// Fixed-point scales (int64 two's complement accumulators).
+constexpr double FSCALE = 4294967296.0;        // 2^32 per kJ mol^-1 nm^-1 (forces)
+constexpr double ESCALE = 4294967296.0;        // 2^32 per kJ mol^-1 (energies, virial)
+constexpr double MSCALE = 1099511627776.0;     // 2^40 per e (PME mesh charge)
+constexpr double FMAX = 1.0e9;                 // |F| above this -> BondExplosion status
+
+enum RepFlags : int {
+    F_LJ = 1,          // Lennard-Jones component present
+    F_COUL_REAL = 2,   // real-space Ewald on the shared list (phys)
+    F_PME = 4,         // SPME reciprocal part
+    F_EXCL = 8,        // exclusion correction component
+    F_PHYS = 16,       // gradient-consistent profile
+    F_BONDED = 32,
+};
+
+enum Status : int {
+    ST_NAN = 1, ST_RANGE = 2, ST_CAPACITY = 4, ST_LIST = 8,
+};
+
+enum ETerm : int { E_LJ = 0, E_CREAL = 1, E_CRECIP = 2, E_CSELF = 3, E_CEXCL = 4, E_BOND = 5,
+                   E_ANGLE = 6, E_DIH = 7, E_VIR = 8, N_EACC = 9 };
+
+// Per-replica constants.
+struct Rep {
+    int atom_begin, n_atoms, tile_begin, n_tiles;
+    int bin_begin, nvx, nvz;            // sort grid: nvx x nvx columns, nvz slabs
+    int chunk_begin, chunk_cap;
+    int n_types, lj_off;
+    int flags, profile;
+    int thermostat, barostat;
+    int pme_K;
+    long long mesh_fix_off, mesh_fix_n;  // int64 spread buffer (REF: K*K*2(K/2+1), PHYS: K^3)
+    long long mesh_real_off;             // K^3 reals
+    long long mesh_cplx_off;             // K*K*(K/2+1) complex
+    int bsp_off;                         // K doubles: B-spline factor per mesh index
+    int pme_block_begin, pme_blocks;     // influence-kernel blocks
+    double rc_lj, rc_c, rc_list;
+    double rc_lj2, rc_c2, rc_list2, half_skin2;
+    double alpha;
+    double dt;
+    double t_temp, t_tau, t_freq, nh_Q;
+    double b_pressure, b_tau, b_compress;
+    double e_self;
+    uint32_t key0, key1;                 // Andersen (phys) Philox key
+};
+
+// Per-replica mutable state.
+struct RepState {
+    double L, invL;
+    double zeta;
+    double vscale;        // pending thermostat velocity scale (applied in the next kick)
+    double pscale;        // pending barostat position scale
+    double ke, pressure, virial;
+    double e_recip, vir_recip;
+    double time;
+    long long e_acc[N_EACC];
+    long long step, target_step;
+    long long andersen_calls;
+    long long list_builds;
+    long long body_runs;  // replica 0 only: graph-executed rebuild bodies
+    int active;           // advances this step
+    int eval;             // forces evaluated in the current evaluation pass
+    int rebuild;          // neighbour list rebuild requested
+    int lj_counter;       // LennardJones::step_since_rebuild_ (REF cadence)
+    int have_forces;
+    int status;
+    int n_chunks;
+};
+
+// Kernel view of the whole batch (passed by value).
+struct Dev {
+    int n_rep, n_atoms, n_tiles, n_slots, n_bins;
+    const Rep* rep;
+    RepState* st;
+    // atoms (reference order)
+    double *x, *y, *z, *vx, *vy, *vz;
+    const double *mass, *q;
+    const int *type, *atom_rep;
+    long long *fbx, *fby, *fbz;        // bonded + PME + exclusion forces (fixed point)
+    int* slot_of_atom;
+    double *xr, *yr, *zr;              // positions at the last list build
+    int *imgx, *imgy, *imgz;           // periodic image frozen at the last build
+    int* atom_bin;
+    // sorted slots
+    int* atom_of_slot;
+    float4* xq32;                      // tile-local FP32 coordinates + charge
+    double4* xq64;                     // unwrapped FP64 coordinates + charge
+    int* type_s;
+    long long *fnx, *fny, *fnz;        // non-bonded forces (fixed point, slot order)
+    // tiles
+    double *tcx, *tcy, *tcz;
+    float *thx, *thy, *thz;
+    const int* tile_rep;
+    double *tile_ke, *tile_vir;
+    // voxel bins
+    int *bin_count, *bin_start, *bin_fill;
+    const int* vox_rank;
+    int* sort_buf;                     // slot-indexed scratch for the counting sort
+    // exclusions
+    const int *ex_start, *ex_list;     // CSR per atom (global indices)
+    int n_excl;
+    const int2* excl;
+    // pair list
+    int* chunk_itile;
+    uint32_t *chunk_j, *chunk_mask;
+    int* chunk_prefix;                 // [n_rep + 1] flat chunk numbering
+    // bonded terms (global atom indices)
+    int n_bonds, n_angles, n_dih;
+    const int2* bond_ij;
+    const double2* bond_kr;
+    const int4* ang_ijk;
+    const double2* ang_kt;
+    const int4* dih_ijkl;
+    const int* dih_n;
+    const double2* dih_kp;
+    // LJ tables per type pair
+    const double2* lj64;               // (eps, sig^6)
+    const float2* lj32;                // (c6, c12) = (4 eps sig^6, 4 eps sig^12)
+    // PME
+    long long* mesh_fix;
+    void* mesh_real;
+    void* mesh_cplx;
+    const double* bsp;
+    double* pme_part;                  // per influence block: energy, virial
+    const int* pme_block_rep;
+    // Andersen (REF): host-generated overrides
+    const int* and_flag;
+    const double* and_v;
+};
+
+}  // namespace dmd

@@ -248,46 +248,84 @@ DECANE = dict(sig_ch3=0.375, eps_ch3=0.814, sig_ch2=0.395, eps_ch2=0.382, m_ch3=
 
 
 def decane_melt(n_chains: int, seed: int, chains_per_nm3: float = 3.09, n_steps: int = 1000,
-                dt: float = 0.002, T: float = 300.0) -> Workload:
-    """United-atom n-decane melt.  Chains start on a lattice and grow as seeded
-    random walks with fixed bond length and angle (torsions drawn from
-    trans/gauche); 1-2, 1-3 and 1-4 exclusions; Lorentz-Berthelot cross pair
+                dt: float = 0.002, T: float = 300.0, d_min: float = 0.25) -> Workload:
+    """United-atom n-decane melt.  Chains grow as seeded random walks with fixed
+    bond length and angle and torsions drawn near trans/gauche; a site is
+    accepted only if it is at least d_min from every site placed before it
+    (other than the preceding sites of its own chain), so the melt has no
+    overlaps.  1-2, 1-3 and 1-4 exclusions; the Lorentz-Berthelot cross pair is
     written explicitly (the engine has no combining rule)."""
     D = DECANE
     rng = np.random.default_rng(seed)
     box = (n_chains / chains_per_nm3) ** (1.0 / 3.0)
-    ns = int(math.ceil(n_chains ** (1.0 / 3.0) - 1e-9))
-    a = box / ns
-    g = np.arange(ns)
-    starts = (np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)[:n_chains] + 0.5) * a
     th = math.radians(D["th0_deg"])
     b = D["b0"]
-    pos = np.zeros((n_chains, 10, 3))
+    nc = max(1, int(box / d_min))
+    cs = box / nc
+    grid: dict = {}
+    placed: list = []
+    d2 = d_min * d_min
+
+    def cell(p):
+        c = np.floor(p / cs).astype(int) % nc
+        return int(c[0]), int(c[1]), int(c[2])
+
+    def clear(p, first_own):
+        cx, cy, cz = cell(p)
+        for dx in (-1, 0, 1):
+            for dy in (-1, 0, 1):
+                for dz in (-1, 0, 1):
+                    for k in grid.get(((cx + dx) % nc, (cy + dy) % nc, (cz + dz) % nc), ()):
+                        if k >= first_own:
+                            continue  # own chain: bonded geometry keeps these apart
+                        d = placed[k] - p
+                        d -= box * np.round(d / box)
+                        if d @ d < d2:
+                            return False
+        return True
+
+    def unit(v):
+        return v / np.linalg.norm(v)
+
     for c in range(n_chains):
-        p = [starts[c]]
-        d0 = rng.normal(size=3)
-        d0 /= np.linalg.norm(d0)
-        p.append(p[0] + b * d0)
-        # second bond at the fixed angle
-        t = rng.normal(size=3)
-        t -= t.dot(d0) * d0
-        t /= np.linalg.norm(t)
-        d1 = math.cos(math.pi - th) * d0 + math.sin(math.pi - th) * t
-        p.append(p[1] + b * d1)
-        for k in range(3, 10):
-            u1 = p[k - 2] - p[k - 3]
-            u2 = p[k - 1] - p[k - 2]
-            u2n = u2 / np.linalg.norm(u2)
-            nrm = np.cross(u1, u2)
-            nrm /= np.linalg.norm(nrm)
-            phi = rng.choice([math.pi, math.pi / 3, -math.pi / 3], p=[0.6, 0.2, 0.2])
-            m = np.cross(nrm, u2n)
-            # bond direction with bond angle th and torsion phi (IUPAC, trans = pi)
-            dirv = (math.cos(math.pi - th) * u2n + math.sin(math.pi - th) *
-                    (-math.cos(phi) * m + math.sin(phi) * nrm))
-            p.append(p[k - 1] + b * dirv / np.linalg.norm(dirv))
-        pos[c] = np.array(p)
-    pos = pos.reshape(-1, 3)
+        base = len(placed)
+        for attempt in range(500):
+            chain = [rng.uniform(0, box, 3)]
+            if not clear(chain[0], base):
+                continue
+            for k in range(1, 10):
+                for _ in range(60):
+                    if k == 1:
+                        cand = chain[0] + b * unit(rng.normal(size=3))
+                    else:
+                        u2 = unit(chain[k - 1] - chain[k - 2])
+                        if k == 2:
+                            t = rng.normal(size=3)
+                            t = unit(t - (t @ u2) * u2)
+                            dirv = math.cos(math.pi - th) * u2 + math.sin(math.pi - th) * t
+                        else:
+                            u1 = chain[k - 2] - chain[k - 3]
+                            nrm = unit(np.cross(u1, u2))
+                            m = np.cross(nrm, u2)
+                            phi = rng.choice([math.pi, math.pi / 3, -math.pi / 3], p=[0.6, 0.2, 0.2])
+                            phi += rng.normal(0, 0.2)
+                            dirv = (math.cos(math.pi - th) * u2 + math.sin(math.pi - th) *
+                                    (-math.cos(phi) * m + math.sin(phi) * nrm))
+                        cand = chain[k - 1] + b * unit(dirv)
+                    own_far = all(float((q - cand) @ (q - cand)) >= d2 for q in chain[:max(0, k - 3)])
+                    if own_far and clear(cand, base):
+                        chain.append(cand)
+                        break
+                else:
+                    break
+            if len(chain) == 10:
+                for p in chain:
+                    grid.setdefault(cell(p), []).append(len(placed))
+                    placed.append(p)
+                break
+        else:
+            raise RuntimeError("decane_melt: could not place a chain without overlaps")
+    pos = np.array(placed).reshape(-1, 3)
     n = 10 * n_chains
     names = (["CH3"] + ["CH2"] * 8 + ["CH3"]) * n_chains
     mass = np.tile([D["m_ch3"]] + [D["m_ch2"]] * 8 + [D["m_ch3"]], n_chains)

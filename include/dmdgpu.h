@@ -121,6 +121,7 @@ typedef struct dmdgpu_scalars {
     int64_t list_builds;
     int32_t lj_step_since_rebuild; /* LennardJones::step_since_rebuild (REF cadence) */
     int32_t status;
+    int64_t list_chunks;           /* 32-entry pair-list chunks of the current list */
 } dmdgpu_scalars;
 
 typedef struct dmdgpu_ctx dmdgpu_ctx;
@@ -182,6 +183,17 @@ int64_t dmdgpu_footprint_bytes(const dmdgpu_system *sys, const dmdgpu_options *o
 
 /* Kernel launches issued by this context so far (this library's own kernels). */
 int64_t dmdgpu_kernel_launches(dmdgpu_ctx *ctx);
+
+/* The CUDA stream (cudaStream_t) every launch of this context is issued on, so a
+ * caller can order its own work or record timing events on it. */
+void *dmdgpu_stream(dmdgpu_ctx *ctx);
+
+/* dmdgpu_step with per-kernel device timing: the n steps are issued as one CUDA
+ * graph with event nodes around the non-bonded and PME kernels.  Receives the
+ * summed device milliseconds of all non-bonded launches, of the PME chains and
+ * of the whole sequence, and the number of non-bonded launches. */
+int dmdgpu_step_profiled(dmdgpu_ctx *ctx, int32_t n_steps, double *nonbonded_ms, double *pme_ms,
+                         double *total_ms, int64_t *nonbonded_launches);
 
 const char *dmdgpu_last_error(const dmdgpu_ctx *ctx);
 void dmdgpu_destroy(dmdgpu_ctx *ctx);

@@ -1,0 +1,183 @@
+"""GPU parity: the CUDA path through the C ABI against the CPU oracle.
+
+Tolerances (relative RMS force error = |F - F_oracle|_2 / |F_oracle|_2 over 3N
+components, energy error = |E - E_oracle| / |E_oracle|):
+  fp64  path: 1e-9 force, 1e-9 energy (fixed-point accumulation at 2^-32)
+  mixed path: 1e-5 force, 1e-5 energy (the stated target)
+Pair lists must be identical as sorted integer (i<j) pair sets.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from dmd_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+TOL = {"fp64": 1e-9, "mixed": 1e-5}
+
+
+def rel_rms(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def _engine(cfg, precision, profile, **kw):
+    from dmd_b200.core import Engine
+    return Engine(cfg, precision=precision, profile=profile, **kw)
+
+
+def _argon(nc=5):
+    return W.argon_fcc(n_cells=nc, a=0.575).config()
+
+
+def _water(n_mol=1000, seed=3):
+    box = (n_mol / 33.43) ** (1 / 3)
+    return W.water_box(n_mol=n_mol, box=box, seed=seed, spacing=box / round(box / 0.1045)).config()
+
+
+def _decane(n=30, seed=5):
+    return W.decane_melt(n, seed).config()
+
+
+def _jitter(cfg, s=0.01, seed=0):
+    rng = np.random.default_rng(seed)
+    n = len(cfg.masses)
+    cfg.pos_x = cfg.pos_x + rng.normal(0, s, n)
+    cfg.pos_y = cfg.pos_y + rng.normal(0, s, n)
+    cfg.pos_z = cfg.pos_z + rng.normal(0, s, n)
+    return cfg
+
+
+SYSTEMS = {"argon": lambda: _jitter(_argon()), "water": lambda: _water(),
+           "decane": lambda: _jitter(_decane(), 0.005)}
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("profile", ["ref", "phys"])
+@pytest.mark.parametrize("system", ["argon", "water", "decane"])
+def test_single_point_forces(oracle, system, profile, precision):
+    cfg = SYSTEMS[system]()
+    F_o, e_o = oracle.forces(cfg, profile)
+    eng = _engine(cfg, precision, profile)
+    F, e = eng.compute_forces()
+    tol = TOL[precision]
+    assert rel_rms(F, F_o) < tol, (system, profile, precision, rel_rms(F, F_o))
+    tot = sum(e.values())
+    assert abs(tot - e_o["total"]) <= tol * max(abs(e_o["total"]), 1.0) * 10, (tot, e_o["total"])
+
+
+COMPONENTS = [(0, "lj"), (1, "bond"), (2, "angle"), (3, "dihedral"), (4, "creal"), (5, "pme"),
+              (6, "excl")]
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("profile", ["ref", "phys"])
+def test_components_water_decane(oracle, profile, precision):
+    for cfg in (_jitter(_water(600), 0.01), _jitter(_decane(20), 0.005)):
+        pos = np.stack([cfg.pos_x, cfg.pos_y, cfg.pos_z], 1)
+        eng = _engine(cfg, precision, profile)
+        for comp, name in COMPONENTS:
+            f_o, e_o, _ = oracle.component(cfg, profile, comp)
+            f, e = eng.component_compute(comp, pos, cfg.box_size)
+            if np.linalg.norm(f_o) == 0 and e_o == 0:
+                assert np.abs(f).max() < 1e-6 and abs(e) < 1e-6, name
+                continue
+            # fp64: the 2^-32 fixed-point step dominates for the small PME forces
+            tol = TOL[precision] * ((30 if precision == "fp64" else 3) if name == "pme" else 1)
+            assert rel_rms(f, f_o) < tol, (name, profile, precision, rel_rms(f, f_o))
+            assert abs(e - e_o) <= tol * max(abs(e_o), 1.0) * 10, (name, e, e_o)
+
+
+@pytest.mark.parametrize("profile", ["ref", "phys"])
+@pytest.mark.parametrize("system", ["argon", "water", "decane"])
+def test_pair_set_identical(oracle, system, profile):
+    cfg = SYSTEMS[system]()
+    eng = _engine(cfg, "mixed", profile, skin=0.1)
+    eng.compute_forces()
+    pi, pj = eng.pair_list()
+    pos = np.stack([cfg.pos_x, cfg.pos_y, cfg.pos_z], 1)
+    if profile == "ref":
+        oi, oj = oracle.pairs(pos, cfg.box_size, cfg.lj_cutoff)
+    else:
+        rc = cfg.lj_cutoff
+        if np.any(cfg.charges != 0):
+            rc = max(rc, cfg.coulomb_cutoff)
+        oi, oj = oracle.pairs(pos, cfg.box_size, rc + 0.1)
+        ex = set(zip(np.minimum(cfg.excl_i, cfg.excl_j), np.maximum(cfg.excl_i, cfg.excl_j)))
+        keep = np.array([(a, b) not in ex for a, b in zip(oi, oj)], bool)
+        oi, oj = oi[keep], oj[keep]
+    assert len(pi) == len(oi)
+    assert np.array_equal(pi, oi) and np.array_equal(pj, oj)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_argon_trajectory_ref(oracle, precision):
+    """REF profile argon NVE (the reference's LJ is correct): positions/velocities
+    follow the FP64 oracle step by step, list cadence and counter included."""
+    cfg = W.argon_fcc(n_cells=4, a=0.575, T=120.0, seed=5).config()
+    oe = oracle.engine(cfg, "ref")
+    eng = _engine(cfg, precision, "ref")
+    tol = {"fp64": 1e-9, "mixed": 2e-5}[precision]
+    for k in range(4):
+        oe.step(6)
+        eng.run_n(6)
+        for which, name in ((0, "positions"), (1, "velocities")):
+            g = eng.positions if which == 0 else eng.velocities
+            o = oe.get(which)
+            if which == 0:
+                err = np.abs(g - o).max() / cfg.box_size
+            else:
+                err = rel_rms(g, o)
+            assert err < tol, (k, name, err)
+        s = eng.scalars()
+        assert s.lj_step_since_rebuild == oe.scalars()["lj_counter"]
+        assert abs(s.potential_energy - oe.scalars()["pe"]) < 1e-6 * abs(oe.scalars()["pe"]) * (100 if precision == "mixed" else 1)
+
+
+@pytest.mark.parametrize("thermo,baro", [("nose-hoover", "none"), ("berendsen", "none"),
+                                         ("berendsen", "berendsen")])
+def test_water_trajectory_phys(oracle, thermo, baro):
+    cfg = _water(300, seed=9)
+    cfg.thermostat.type = thermo
+    cfg.barostat.type = baro
+    cfg.barostat.tau = 0.5
+    oe = oracle.engine(cfg, "phys")
+    eng = _engine(cfg, "fp64", "phys")
+    oe.step(10)
+    eng.run_n(10)
+    assert np.abs(eng.positions - oe.get(0)).max() < 1e-8
+    assert rel_rms(eng.velocities, oe.get(1)) < 1e-7
+    s, so = eng.scalars(), oe.scalars()
+    assert abs(s.box - so["box"]) < 1e-12 * so["box"] + 1e-14
+    assert abs(s.zeta - so["zeta"]) <= 1e-7 * abs(so["zeta"]) + 1e-12
+
+
+def test_run_to_run_bitwise():
+    cfg = _water(500, seed=2)
+    a = _engine(cfg, "mixed", "phys")
+    b = _engine(cfg, "mixed", "phys")
+    a.run_n(25)
+    b.run_n(25)
+    assert np.array_equal(a.positions, b.positions)
+    assert np.array_equal(a.velocities, b.velocities)
+    assert a.potential_energy == b.potential_energy
+
+
+def test_checkpoint_restart_bitwise(tmp_path):
+    """tests/integration/test_checkpoint_restart.cpp: N steps == N/2 + save/load + N/2."""
+    cfg = W.argon_fcc(n_cells=2, a=0.575, T=85.0, seed=4).config()
+    cfg.lj_cutoff = 0.5
+    full = _engine(cfg, "fp64", "ref")
+    full.run_n(200)
+    half = _engine(cfg, "fp64", "ref")
+    half.run_n(100)
+    p = str(tmp_path / "ck.bin")
+    half.save_checkpoint(p)
+    fresh = _engine(cfg, "fp64", "ref")
+    fresh.load_checkpoint(p)
+    assert fresh.current_step == 100
+    fresh.run_n(100)
+    assert fresh.current_step == 200
+    assert np.array_equal(full.positions, fresh.positions)
+    assert np.array_equal(full.velocities, fresh.velocities)
