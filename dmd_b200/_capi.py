@@ -66,6 +66,11 @@ class dmdgpu_options(C.Structure):
                 ("device", C.c_int32), ("rng_seed", C.c_uint64)]
 
 
+class dmdgpu_timing(C.Structure):
+    _fields_ = [("step_ms", C.c_double), ("nonbonded_ms", C.c_double), ("pme_ms", C.c_double),
+                ("nonbonded_launches", C.c_int64), ("kernel_launches", C.c_int64)]
+
+
 class dmdgpu_scalars(C.Structure):
     _fields_ = [("step", C.c_int64), ("time", C.c_double), ("potential_energy", C.c_double),
                 ("box", C.c_double), ("kinetic_energy", C.c_double), ("temperature", C.c_double),
@@ -103,6 +108,8 @@ def lib() -> C.CDLL:
         "dmdgpu_load_checkpoint": (C.c_int, [vp, C.c_char_p]),
         "dmdgpu_footprint_bytes": (C.c_int64, [C.POINTER(dmdgpu_system), C.POINTER(dmdgpu_options)]),
         "dmdgpu_kernel_launches": (C.c_int64, [vp]),
+        "dmdgpu_stream": (C.c_void_p, [vp]),
+        "dmdgpu_step_timed": (C.c_int, [vp, C.c_int32, C.c_int64, C.POINTER(dmdgpu_timing)]),
         "dmdgpu_last_error": (C.c_char_p, [vp]),
         "dmdgpu_destroy": (None, [vp]),
         "dmdgpu_batch_create": (C.c_int, [C.c_int64, C.POINTER(dmdgpu_options), C.POINTER(vp)]),

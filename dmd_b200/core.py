@@ -294,3 +294,14 @@ class Engine:
 
     def kernel_launches(self) -> int:
         return int(self._lib.dmdgpu_kernel_launches(self._h))
+
+    def stream(self) -> int:
+        """cudaStream_t (as an integer) every launch of this engine is issued on."""
+        return int(self._lib.dmdgpu_stream(self._h) or 0)
+
+    def step_timed(self, steps: int, l2_flush_bytes: int = 0) -> dict:
+        """Advance `steps` steps as one CUDA graph with device timing of every step
+        and of every non-bonded / PME launch (optional L2 flush between steps)."""
+        t = _capi.dmdgpu_timing()
+        self._check(self._lib.dmdgpu_step_timed(self._h, int(steps), int(l2_flush_bytes), C.byref(t)))
+        return {k: getattr(t, k) for k, _ in t._fields_}

@@ -265,13 +265,10 @@ int64_t dmdgpu_kernel_launches(dmdgpu_ctx* c) { return (c && c->b) ? c->b->launc
 
 void* dmdgpu_stream(dmdgpu_ctx* c) { return (c && c->b) ? static_cast<void*>(c->b->stream()) : nullptr; }
 
-int dmdgpu_step_profiled(dmdgpu_ctx* c, int32_t n, double* nb_ms, double* pme_ms, double* total_ms,
-                         int64_t* nb_launches) {
-    if (!c || !c->b || n <= 0) return DMDGPU_ERR_INVALID;
+int dmdgpu_step_timed(dmdgpu_ctx* c, int32_t n, int64_t flush_bytes, dmdgpu_timing* out) {
+    if (!c || !c->b || n <= 0 || !out) return DMDGPU_ERR_INVALID;
     int rc = c->b->extend_targets(n);
-    long long nl = 0;
-    if (!rc) rc = c->b->step_profiled(n, nb_ms, pme_ms, total_ms, &nl);
-    if (nb_launches) *nb_launches = nl;
+    if (!rc) rc = c->b->step_timed(n, flush_bytes, out);
     return rc ? ctx_fail(c, rc) : DMDGPU_OK;
 }
 

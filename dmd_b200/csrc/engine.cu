@@ -12,6 +12,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <fstream>
 #include <random>
@@ -73,6 +74,7 @@ Batch::Batch(const dmdgpu_options& opt, long long budget) : opt_(opt), budget_(b
 Batch::~Batch() {
     cudaSetDevice(device_);
     free_device();
+    if (flush_buf_) cudaFree(flush_buf_);
     for (cudaEvent_t e : ev_pool_) cudaEventDestroy(e);
     if (body_stream_) cudaStreamDestroy(body_stream_);
     if (stream_) cudaStreamDestroy(stream_);
@@ -773,19 +775,19 @@ void Batch::enqueue_eval(int pass) {
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (prof_nb_) {
         e0 = next_event();
-        cudaEventRecord(e0, stream_);
+        record(e0);
     }
     launch_nonbonded(d, fp64_, phys_, n_sm_, stream_, &launches_);
     if (prof_nb_) {
         e1 = next_event();
-        cudaEventRecord(e1, stream_);
+        record(e1);
         prof_nb_->emplace_back(e0, e1);
     }
     launch_bonded(d, fp64_, phys_, stream_, &launches_);
     if (any_pme_) {
         if (prof_pme_) {
             e0 = next_event();
-            cudaEventRecord(e0, stream_);
+            record(e0);
         }
         launch_pme_spread(d, fp64_, stream_, &launches_);
         launch_pme_convert(d, fp64_, n_fix_total_, stream_, &launches_);
@@ -817,7 +819,7 @@ void Batch::enqueue_eval(int pass) {
         launch_pme_gather(d, fp64_, stream_, &launches_);
         if (prof_pme_) {
             e1 = next_event();
-            cudaEventRecord(e1, stream_);
+            record(e1);
             prof_pme_->emplace_back(e0, e1);
         }
     }
@@ -915,6 +917,21 @@ void Batch::andersen_ref_prepare() {
 
 int Batch::run_steps(int n) {
     if (n <= 0) return DMDGPU_OK;
+    static const bool eager = [] {
+        const char* e = std::getenv("DMD_EAGER");
+        return e && e[0] == '1';
+    }();
+    if (eager && !any_andersen_ref_) {
+        // every launch issued from the host (profilers see each kernel); same work
+        need_eval1_ = true;
+        for (int i = 0; i < n; ++i) {
+            enqueue_step();
+            CK(cudaGetLastError());
+            if (i == 0) need_eval1_ = any_baro_ || any_ref_lj_;
+        }
+        graph_dirty_ = true;
+        return DMDGPU_OK;
+    }
     if (any_andersen_ref_) {
         // host-generated random stream per step: no graph
         need_eval1_ = true;
@@ -1019,68 +1036,94 @@ int Batch::extend_targets(long long n) {
     return DMDGPU_OK;
 }
 
-// n steps as one captured graph with timing events around the non-bonded kernel
-// and the PME chain of every evaluation.
-int Batch::step_profiled(int n, double* nb_ms, double* pme_ms, double* total_ms, long long* nb_launches) {
+// Event record usable for timing inside a captured graph: an external event
+// node (a plain record during capture only becomes a graph dependency).
+void Batch::record(cudaEvent_t e) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing(stream_, &cs);
+    if (cs == cudaStreamCaptureStatusActive) cudaEventRecordWithFlags(e, stream_, cudaEventRecordExternal);
+    else cudaEventRecord(e, stream_);
+}
+
+// n steps as one captured graph with timing events around every step and every
+// non-bonded / PME launch; optional L2 flush between steps (outside the events).
+int Batch::step_timed(int n, long long flush_bytes, dmdgpu_timing* out) {
     CK(cudaSetDevice(device_));
+    std::memset(out, 0, sizeof(*out));
     if (!packed_) {
         int rc = pack();
         if (rc) return rc;
     }
+    if (n <= 0) return DMDGPU_OK;
     if (graph_dirty_ || !graph_ || any_andersen_ref_) {
-        int rc = run_steps(1);  // initial forces / steady-state graph
+        int rc = run_steps(1);  // initial forces / steady-state configuration
         if (rc) return rc;
+        CK(cudaStreamSynchronize(stream_));
         --n;
+        if (n == 0) return sync_status();
     }
-    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> nb, pme;
-    // events must exist before capture (creating one during capture invalidates it)
-    while (ev_pool_.size() < static_cast<size_t>(8 * n + 8)) {
+    if (flush_bytes > 0 && flush_bytes != flush_bytes_) {
+        if (flush_buf_) cudaFree(flush_buf_);
+        flush_buf_ = nullptr;
+        CK(cudaMalloc(&flush_buf_, flush_bytes));
+        flush_bytes_ = flush_bytes;
+    }
+    const size_t need = static_cast<size_t>(8 * n + 8);
+    while (ev_pool_.size() < need) {  // events must exist before capture
         cudaEvent_t ev;
         CK(cudaEventCreate(&ev));
         ev_pool_.push_back(ev);
     }
     ev_used_ = 0;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> nb, pme, steps;
     prof_nb_ = &nb;
     prof_pme_ = &pme;
     cudaGraph_t g;
     cudaGraphExec_t ge;
-    long long before = launches_;
+    const long long before = launches_;
+    capture_error_ = false;
     cudaError_t e = cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal);
     if (e == cudaSuccess) {
-        for (int i = 0; i < n; ++i) enqueue_step();
+        for (int i = 0; i < n; ++i) {
+            if (flush_buf_) cudaMemsetAsync(flush_buf_, i & 0xff, flush_bytes_, stream_);
+            cudaEvent_t a = next_event(), b = next_event();
+            record(a);
+            enqueue_step();
+            record(b);
+            steps.emplace_back(a, b);
+        }
         e = cudaStreamEndCapture(stream_, &g);
     }
     prof_nb_ = nullptr;
     prof_pme_ = nullptr;
-    if (e != cudaSuccess) {
+    if (e != cudaSuccess || capture_error_) {
         cudaGetLastError();
-        return check_cuda(e, "profiled capture");
+        return fail(DMDGPU_ERR_GPU, std::string("timed capture failed: ") + cudaGetErrorString(e));
     }
+    const long long captured = launches_ - before;
     CK(cudaGraphInstantiate(&ge, g, 0));
     cudaGraphDestroy(g);
-    cudaEvent_t t0 = next_event(), t1 = next_event();
-    CK(cudaEventRecord(t0, stream_));
+    const long long runs0 = body_runs_seen_;
     CK(cudaGraphLaunch(ge, stream_));
-    CK(cudaEventRecord(t1, stream_));
     CK(cudaStreamSynchronize(stream_));
     cudaGraphExecDestroy(ge);
     float ms = 0.f;
-    double s_nb = 0.0, s_pme = 0.0;
+    for (auto& pr : steps) {
+        CK(cudaEventElapsedTime(&ms, pr.first, pr.second));
+        out->step_ms += ms;
+    }
     for (auto& pr : nb) {
         CK(cudaEventElapsedTime(&ms, pr.first, pr.second));
-        s_nb += ms;
+        out->nonbonded_ms += ms;
     }
     for (auto& pr : pme) {
         CK(cudaEventElapsedTime(&ms, pr.first, pr.second));
-        s_pme += ms;
+        out->pme_ms += ms;
     }
-    CK(cudaEventElapsedTime(&ms, t0, t1));
-    if (nb_ms) *nb_ms = s_nb;
-    if (pme_ms) *pme_ms = s_pme;
-    if (total_ms) *total_ms = ms;
-    if (nb_launches) *nb_launches = static_cast<long long>(nb.size());
-    (void)before;
-    return sync_status();
+    out->nonbonded_launches = static_cast<long long>(nb.size());
+    int rc = sync_status();  // adds the rebuild bodies that executed
+    out->kernel_launches = captured + 7 * (body_runs_seen_ - runs0);
+    return rc;
 }
 
 int Batch::active() const {

@@ -80,7 +80,7 @@ class Batch {
 
     int step(int n);            // advance every running replica by up to n steps
     int extend_targets(long long n);  // single-system API: allow n more steps
-    int step_profiled(int n, double* nb_ms, double* pme_ms, double* total_ms, long long* nb_launches);
+    int step_timed(int n, long long flush_bytes, dmdgpu_timing* out);
     cudaStream_t stream() const { return stream_; }
     int compute_forces(int slot, double* fx, double* fy, double* fz, double* e_terms);
     int get_state(int slot, int which, double* x, double* y, double* z);
@@ -143,6 +143,9 @@ class Batch {
     size_t ev_used_ = 0;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>>* prof_nb_ = nullptr;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>>* prof_pme_ = nullptr;
+    void* flush_buf_ = nullptr;
+    long long flush_bytes_ = 0;
+    void record(cudaEvent_t e);
     cudaEvent_t next_event();
     std::string err_;
     std::vector<int> finished_;

@@ -188,12 +188,20 @@ int64_t dmdgpu_kernel_launches(dmdgpu_ctx *ctx);
  * caller can order its own work or record timing events on it. */
 void *dmdgpu_stream(dmdgpu_ctx *ctx);
 
-/* dmdgpu_step with per-kernel device timing: the n steps are issued as one CUDA
- * graph with event nodes around the non-bonded and PME kernels.  Receives the
- * summed device milliseconds of all non-bonded launches, of the PME chains and
- * of the whole sequence, and the number of non-bonded launches. */
-int dmdgpu_step_profiled(dmdgpu_ctx *ctx, int32_t n_steps, double *nonbonded_ms, double *pme_ms,
-                         double *total_ms, int64_t *nonbonded_launches);
+/* Device timing of a run of steps. */
+typedef struct dmdgpu_timing {
+    double step_ms;            /* summed device time of the n steps (flushes excluded) */
+    double nonbonded_ms;       /* summed device time of every non-bonded pair-kernel launch */
+    double pme_ms;             /* summed device time of the PME chains (spread .. gather) */
+    int64_t nonbonded_launches;
+    int64_t kernel_launches;   /* this library's kernels executed during the n steps */
+} dmdgpu_timing;
+
+/* dmdgpu_step with device timing: the n steps are issued as one CUDA graph with
+ * event records around every step and every non-bonded / PME launch.  When
+ * l2_flush_bytes > 0 a buffer of that size is overwritten between steps (outside
+ * the timed intervals) so each step starts with a cold L2. */
+int dmdgpu_step_timed(dmdgpu_ctx *ctx, int32_t n_steps, int64_t l2_flush_bytes, dmdgpu_timing *out);
 
 const char *dmdgpu_last_error(const dmdgpu_ctx *ctx);
 void dmdgpu_destroy(dmdgpu_ctx *ctx);

@@ -138,38 +138,72 @@ void factorize(int n, std::vector<int>& f) {
 }
 
 // Decimation in time: X[k + q m] = sum_r W_n^{r(k+qm)} Y_r[k], Y_r = DFT_m(x[r::p]).
-void fft_rec(const cd* in, int is, cd* out, int n, int sign, const int* f, std::vector<cd>& tmp) {
+// One plan per length: factors and a table of the N-th roots of unity (twiddles
+// of every sub-length n | N are W_n^e = W_N^{e N/n}); one scratch buffer.
+struct FFTPlan {
+    int n = 0;
+    std::vector<int> f;
+    std::vector<cd> w;        // exp(-2 pi i k / n)
+    std::vector<cd> scratch, tmp;
+};
+
+FFTPlan& plan_for(int n) {
+    static thread_local std::vector<FFTPlan> plans;
+    for (auto& p : plans)
+        if (p.n == n) return p;
+    FFTPlan p;
+    p.n = n;
+    factorize(n, p.f);
+    p.w.resize(n);
+    for (int k = 0; k < n; ++k) {
+        double a = -2.0 * PI * static_cast<double>(k) / n;
+        p.w[k] = cd(std::cos(a), std::sin(a));
+    }
+    p.scratch.resize(n);
+    p.tmp.resize(n);
+    plans.push_back(std::move(p));
+    return plans.back();
+}
+
+void fft_rec(const cd* in, int is, cd* out, int n, int level, FFTPlan& P, bool inv) {
     if (n == 1) {
         out[0] = in[0];
         return;
     }
-    int p = f[0], m = n / p;
-    for (int r = 0; r < p; ++r) fft_rec(in + r * is, is * p, out + r * m, m, sign, f + 1, tmp);
-    std::vector<cd> t(p), res(n);
+    const int p = P.f[level], m = n / p;
+    for (int r = 0; r < p; ++r) fft_rec(in + r * is, is * p, out + r * m, m, level + 1, P, inv);
+    const int N = P.n, step = N / n;
+    cd* res = P.scratch.data();
+    cd t[64];
+    std::vector<cd> big;
+    cd* tt = t;
+    if (p > 64) {
+        big.resize(p);
+        tt = big.data();
+    }
     for (int k = 0; k < m; ++k) {
         for (int r = 0; r < p; ++r) {
-            long e = (static_cast<long>(r) * k) % n;
-            double a = sign * 2.0 * PI * static_cast<double>(e) / n;
-            t[r] = out[r * m + k] * cd(std::cos(a), std::sin(a));
+            cd wv = P.w[(static_cast<long>(r) * k % n) * step];
+            if (inv) wv = std::conj(wv);
+            tt[r] = out[r * m + k] * wv;
         }
         for (int q = 0; q < p; ++q) {
-            cd s = 0;
+            cd acc = 0;
             for (int r = 0; r < p; ++r) {
-                long e = (static_cast<long>(r) * q) % p;
-                double a = sign * 2.0 * PI * static_cast<double>(e) / p;
-                s += t[r] * cd(std::cos(a), std::sin(a));
+                cd wv = P.w[(static_cast<long>(r) * q % p) * (N / p)];
+                if (inv) wv = std::conj(wv);
+                acc += tt[r] * wv;
             }
-            res[k + q * m] = s;
+            res[k + q * m] = acc;
         }
     }
-    std::copy(res.begin(), res.end(), out);
+    std::copy(res, res + n, out);
 }
 
 void fft1d(cd* a, int n, int sign) {
-    std::vector<int> f;
-    factorize(n, f);
-    std::vector<cd> in(a, a + n), tmp;
-    fft_rec(in.data(), 1, a, n, sign, f.data(), tmp);
+    FFTPlan& P = plan_for(n);
+    std::copy(a, a + n, P.tmp.begin());
+    fft_rec(P.tmp.data(), 1, a, n, 0, P, sign > 0);
 }
 
 // 3-D complex transform in place over a K*K*K array, index (z*K + y)*K + x.
@@ -906,6 +940,7 @@ struct orc_run {
     int barostat;    // 0 none 1 berendsen
     double b_pressure, b_tau, b_compress;
     uint64_t rng_seed;  // phys Andersen (Philox key)
+    int brute_list;     // ref profile: rebuild the LJ list with the reference's O(N^2) loop
 };
 
 struct OrcEngine {
@@ -1017,7 +1052,26 @@ void eng_compute(OrcEngine* E) {
     if (E->s.profile == 0 && E->s.use_lj) {
         // LennardJones::compute rebuild cadence (lennard_jones.cpp:53-55, :91)
         if (E->lj_counter >= 10) {
-            pairs_within(n, E->x.data(), E->y.data(), E->z.data(), E->L, E->s.lj_cutoff, E->lpi, E->lpj);
+            if (E->run.brute_list) {
+                // LennardJones::rebuild_pair_list (lennard_jones.cpp:18-41), O(N^2)
+                E->lpi.clear();
+                E->lpj.clear();
+                const double rc2 = E->s.lj_cutoff * E->s.lj_cutoff;
+                const double* x = E->x.data();
+                const double* y = E->y.data();
+                const double* z = E->z.data();
+                for (int i = 0; i < n; ++i)
+                    for (int j = i + 1; j < n; ++j) {
+                        double dx = x[j] - x[i], dy = y[j] - y[i], dz = z[j] - z[i];
+                        min_image(E->L, dx, dy, dz);
+                        if (dx * dx + dy * dy + dz * dz < rc2) {
+                            E->lpi.push_back(i);
+                            E->lpj.push_back(j);
+                        }
+                    }
+            } else {
+                pairs_within(n, E->x.data(), E->y.data(), E->z.data(), E->L, E->s.lj_cutoff, E->lpi, E->lpj);
+            }
             E->lj_counter = 0;
         }
     }

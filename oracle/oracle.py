@@ -72,7 +72,7 @@ class orc_run(C.Structure):
                 ("init_temperature", C.c_double), ("thermostat", C.c_int),
                 ("t_temp", C.c_double), ("t_tau", C.c_double), ("t_freq", C.c_double),
                 ("barostat", C.c_int), ("b_pressure", C.c_double), ("b_tau", C.c_double),
-                ("b_compress", C.c_double), ("rng_seed", C.c_uint64)]
+                ("b_compress", C.c_double), ("rng_seed", C.c_uint64), ("brute_list", C.c_int)]
 
 
 THERMO = {"none": 0, "berendsen": 1, "nose-hoover": 2, "andersen": 3}
@@ -248,14 +248,14 @@ class Oracle:
         return np.stack([fx, fy, fz], 1), e.value, v.value
 
     # -- engine ---------------------------------------------------------------
-    def engine(self, cfg, profile, rng_seed=0x5EED):
-        return OracleEngine(self, cfg, profile, rng_seed)
+    def engine(self, cfg, profile, rng_seed=0x5EED, brute_list=False):
+        return OracleEngine(self, cfg, profile, rng_seed, brute_list)
 
 
 class OracleEngine:
     """The reference step sequence (SimulationEngine::step) in FP64 on the CPU."""
 
-    def __init__(self, o: Oracle, cfg, profile, rng_seed):
+    def __init__(self, o: Oracle, cfg, profile, rng_seed, brute_list=False):
         self.o = o
         self.S = _Sys(cfg, profile)
         k = []
@@ -279,6 +279,7 @@ class OracleEngine:
         r.barostat = BARO[cfg.barostat.type]
         r.b_pressure, r.b_tau, r.b_compress = cfg.barostat.pressure, cfg.barostat.tau, cfg.barostat.compressibility
         r.rng_seed = rng_seed
+        r.brute_list = int(bool(brute_list))
         self.n = len(cfg.masses)
         self.h = o.L.orc_engine_create(C.byref(self.S.s), C.byref(r))
         self._k = k
