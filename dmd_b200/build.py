@@ -20,7 +20,8 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
          "-Xptxas", "-warn-spills"]
-SOURCES = ["k_list.cu", "k_nonbonded.cu", "k_forces.cu", "k_integrate.cu", "engine.cu", "capi.cu"]
+SOURCES = ["k_list.cu", "k_nonbonded.cu", "k_forces.cu", "k_integrate.cu", "engine.cu", "capi.cu",
+           "noalloc.cu"]
 
 
 def _compile(src: str) -> str:

@@ -233,6 +233,58 @@ int32_t dmdgpu_batch_active(dmdgpu_batch *b);
 const char *dmdgpu_batch_last_error(const dmdgpu_batch *b);
 void dmdgpu_batch_destroy(dmdgpu_batch *b);
 
+/* ---------------------------------------------------------------------------
+ * Non-bonded forces without any device allocation.
+ *
+ * No counterpart in the reference.  For callers that cannot call cudaMalloc:
+ * code issuing work while a stream is being captured, hosts whose device memory
+ * belongs to another allocator or a fixed arena, callers that must not pay for
+ * an allocation per call.  It computes what dmdgpu_component_compute gives for
+ * components 0 (Lennard-Jones) and 4 (real-space Coulomb) -- the same kernels --
+ * on caller-owned device buffers: d_x/d_y/d_z (positions), d_q (charges) and
+ * d_type (LJ type per atom) in; d_fx/d_fy/d_fz (forces, written, not
+ * accumulated) and d_energies (2 doubles: LJ, real-space Coulomb; may be NULL)
+ * out.  Every intermediate buffer lives in one static device array of about
+ * 6 MB that each GPU holds from the first use of the library until the process
+ * exits; no device memory is allocated or freed.  Atom types must lie in
+ * [0, n_types): a type outside it returns DMDGPU_ERR_PARM (and is never used
+ * to index the LJ table).
+ *
+ * Limits (sizes beyond them return DMDGPU_ERR_PARM): n_atoms <=
+ * DMDGPU_NOALLOC_MAX_ATOMS, n_types <= DMDGPU_NOALLOC_MAX_TYPES, n_excl <=
+ * DMDGPU_NOALLOC_MAX_EXCLUSIONS; a pair list longer than
+ * DMDGPU_NOALLOC_MAX_CHUNKS chunks returns DMDGPU_ERR_CAPACITY.
+ *
+ * The first call on a device resolves the array's device address (one-time
+ * set-up): make that first call before any stream capture.  Calls run on
+ * `stream` (a cudaStream_t, NULL = legacy default stream) and return after it
+ * has synchronised.  All calls share the one array: calls that overlap on the
+ * GPU (other threads, other streams) race and must be serialised by the caller.
+ */
+#define DMDGPU_NOALLOC_MAX_ATOMS 8192
+#define DMDGPU_NOALLOC_MAX_TYPES 16
+#define DMDGPU_NOALLOC_MAX_EXCLUSIONS 32768
+#define DMDGPU_NOALLOC_MAX_SORT_CELLS 32768
+#define DMDGPU_NOALLOC_MAX_CHUNKS 16384
+
+typedef struct dmdgpu_nb_params {
+    int32_t n_atoms;
+    double box;                        /* cubic box length */
+    int32_t n_types;
+    const double *lj_sigma, *lj_epsilon; /* host, n_types x n_types */
+    double lj_cutoff, coul_cutoff, ewald_coeff;
+    int32_t n_excl;                    /* exclusion pairs (host); PHYS skips them */
+    const int32_t *excl_i, *excl_j;
+    int32_t profile;                   /* DMDGPU_PROFILE_* */
+    int32_t precision;                 /* DMDGPU_PRECISION_* */
+    double skin;                       /* PHYS list skin (nm) */
+} dmdgpu_nb_params;
+
+int dmdgpu_nonbonded_noalloc(const dmdgpu_nb_params *p, const double *d_x, const double *d_y,
+                             const double *d_z, const double *d_q, const int32_t *d_type,
+                             double *d_fx, double *d_fy, double *d_fz, double *d_energies,
+                             void *stream);
+
 #ifdef __cplusplus
 }
 #endif
