@@ -541,7 +541,7 @@ int Batch::pack() {
             hvy(n_atoms), hvz(n_atoms);
         std::vector<int> ht(n_atoms), har(n_atoms), htr(n_tiles), hvr(n_bins), hbr(n_bins);
         std::vector<double2> lj64(n_lj);
-        std::vector<float2> lj32(n_lj);
+        std::vector<float4> lj32(n_lj);
         std::vector<int2> bij;
         std::vector<double2> bkr;
         std::vector<int4> aijk;
@@ -596,8 +596,7 @@ int Batch::pack() {
                     const double sig2 = sg * sg;
                     const double sig6 = sig2 * sig2 * sig2;
                     lj64[P.lj_off + ti * P.n_types + tj] = make_double2(ep, sig6);
-                    lj32[P.lj_off + ti * P.n_types + tj] =
-                        make_float2(static_cast<float>(4.0 * ep * sig6), static_cast<float>(4.0 * ep * sig6 * sig6));
+                    lj32[P.lj_off + ti * P.n_types + tj] = lj_coeffs32(ep, sig6);
                 }
             for (size_t t = 0; t < s.bi.size(); ++t) {
                 bij.push_back(make_int2(a0 + s.bi[t], a0 + s.bj[t]));
@@ -667,11 +666,12 @@ int Batch::pack() {
         up(vox_rank, hvr.data(), 4 * n_bins);
         up(d_bin_rep_, hbr.data(), 4 * n_bins);
         double2* dlj64 = A.alloc<double2>(n_lj);
-        float2* dlj32 = A.alloc<float2>(n_lj);
+        float4* dlj32 = A.alloc<float4>(n_lj);
         up(dlj64, lj64.data(), sizeof(double2) * n_lj);
-        up(dlj32, lj32.data(), sizeof(float2) * n_lj);
+        up(dlj32, lj32.data(), sizeof(float4) * n_lj);
         d.lj64 = dlj64;
         d.lj32 = dlj32;
+        d.n_lj = static_cast<int>(n_lj);
         d.n_bonds = static_cast<int>(bij.size());
         d.n_angles = static_cast<int>(aijk.size());
         d.n_dih = static_cast<int>(dijkl.size());

@@ -49,6 +49,12 @@ __global__ void k_eval_begin(Dev d, int pass) {
         ev = 1;
     }
     s->eval = ev;
+    // Pair energies and the pair virial are needed by single-point evaluations,
+    // by the evaluation that ends a run (its energies are what the host reads) and,
+    // with the PHYS barostat, every step (its pressure uses the atomic virial).
+    // Eval #1 never needs them: eval #2 of the same step overwrites its sums.
+    s->want_e = (pass == PASS_SINGLE) ||
+                (pass == PASS_SECOND && (s->step + 1 >= s->target_step || ((R.flags & F_PHYS) && R.barostat)));
     if (ev) {
         for (int k = 0; k < N_EACC; ++k) s->e_acc[k] = 0;
         s->e_recip = 0.0;

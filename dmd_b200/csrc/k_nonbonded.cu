@@ -5,7 +5,8 @@
 // chunk: lane i holds i-atom i of the tile; the chunk's 32 j atoms are staged
 // in shared memory and visited in a rotated order ((lane + k) & 31) so every
 // lane touches a different j at each of the 32 steps; the j forces rotate with
-// warp shuffles and are flushed once per chunk, i forces once per chunk.
+// warp shuffles and are flushed once per chunk, i forces once per chunk.  The
+// chunk's 32 masks are transposed in registers into each lane's visiting order.
 // Forces go to int64 fixed point (deterministic), energies/virial to per-lane
 // int64 accumulators flushed per warp.
 //
@@ -30,10 +31,27 @@ struct Acc {
     long long lj, c, v;
 };
 
+// Single-instruction approximations (PTX .approx forms, flush-to-zero).
+__device__ __forceinline__ float rsqrt_ap(float x) {
+    float y;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float ex2_ap(float x) {
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float rcp_ap(float x) {
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
 // erfc(x) for x >= 0 given e = exp(-x*x): Abramowitz & Stegun, Handbook of
 // Mathematical Functions, eq. 7.1.26 (absolute error <= 1.5e-7).
 __device__ __forceinline__ float erfc_as(float x, float e) {
-    const float t = __fdividef(1.0f, fmaf(0.3275911f, x, 1.0f));
+    const float t = rcp_ap(fmaf(0.3275911f, x, 1.0f));
     const float p = fmaf(fmaf(fmaf(fmaf(1.061405429f, t, -1.453152027f), t, 1.421413741f), t,
                               -0.284496736f), t, 0.254829592f);
     return t * p * e;
@@ -58,14 +76,209 @@ __device__ __forceinline__ bool exact_inside(const Dev& d, int ai, int aj, doubl
     return r2_ref(dx, dy, dz) < rc2;
 }
 
+// Rotated transpose of the chunk's masks: entry j's mask has bit i set when
+// (i, j) interacts; lane l receives the bits it visits, bit k = (l, entry (l+k)&31).
+// Butterfly transpose of the 32x32 bit matrix over five shuffle stages, then a
+// rotation by the lane index.
+__device__ __forceinline__ uint32_t rotated_columns(uint32_t x, int lane) {
+    const uint32_t m[5] = {0x0000FFFFu, 0x00FF00FFu, 0x0F0F0F0Fu, 0x33333333u, 0x55555555u};
+#pragma unroll
+    for (int s = 0; s < 5; ++s) {
+        const int w = 16 >> s;
+        const uint32_t y = __shfl_xor_sync(FULL, x, w);
+        x = (lane & w) ? ((x & ~m[s]) | ((y >> w) & m[s])) : ((x & m[s]) | ((y << w) & ~m[s]));
+    }
+    return __funnelshift_r(x, x, lane);
+}
+
+// Per-warp staging of one chunk's 32 j entries.  Coordinates and LJ columns are
+// stored twice (entry l at l and l + 32) so round k of lane l reads index l + k
+// with an immediate offset instead of (l + k) & 31.
+struct ChunkStage {
+    float4 xq[64];
+    int tj[64];
+    int js[32];
+    int aj[32];
+};
+
+// Force of one pair over r (f: F_j = f (r_j - r_i)) and its energy terms.
+// c12f/c6f are the force-scaled LJ coefficients (12 c12, 6 c6) and qq the
+// Coulomb prefactor, each already zero when the term does not apply.
 template <bool PHYS>
-__global__ void __launch_bounds__(256) k_nb_f32(Dev d) {
+__device__ __forceinline__ float pair_f(float r2, float c6f, float c12f, float qq, float alpha,
+                                        float a2l2e, float c2a, float& ir6, float& rinv,
+                                        float& erfc_ar) {
+    rinv = rsqrt_ap(r2);
+    const float ir2 = rinv * rinv;
+    ir6 = ir2 * ir2 * ir2;
+    float fr = ir6 * fmaf(c12f, ir6, -c6f);
+    if (PHYS) {
+        const float ex = ex2_ap(a2l2e * r2);
+        erfc_ar = erfc_as(alpha * (r2 * rinv), ex);
+        fr = fmaf(qq, fmaf(erfc_ar, rinv, c2a * ex), fr);
+    }
+    return fr * ir2;
+}
+
+// One chunk (an i-tile against 32 j entries) for one warp.  Lane l owns i atom l
+// and j entry l; in round k it pairs its i atom with entry (l+k)&31 and passes the
+// j forces it accumulated on to lane l-1, so after 32 rounds they are back home.
+// The loop is branch-free: a pair that is masked out or outside a cutoff gets
+// zero coefficients.  Pairs whose FP32 r^2 lies within 1e-5 (relative) of a
+// cutoff are left out of the loop and redone afterwards with the FP64 reference
+// membership test, so the interacting set is exactly the reference's.
+template <bool PHYS, bool ENERGY>
+__device__ __forceinline__ void nb_chunk(const Dev& d, const Rep& R, RepState* s, int c, int lane,
+                                         ChunkStage& S, const float4* lj_tab, Acc& acc) {
+    const double L = s->L;
+    const int I = d.chunk_itile[c];
+    const int si = 32 * I + lane;
+    const float4 xi = d.xq32[si];
+    const int ti = d.type_s[si];
+    const uint32_t e = d.chunk_j[32 * c + lane];
+    const uint32_t mk = d.chunk_mask[32 * c + lane];
+    const int js = static_cast<int>(e & 0x03FFFFFFu);
+    float4 xj = make_float4(1e6f, 1e6f, 1e6f, 0.f);
+    int tj = 0, aj = -1;
+    if (mk) {
+        xj = d.xq32[js];
+        tj = d.type_s[js];
+        aj = d.atom_of_slot[js];
+        const int J = js >> 5;
+        const int mx = static_cast<int>((e >> 26) & 3u) - 1;
+        const int my = static_cast<int>((e >> 28) & 3u) - 1;
+        const int mz = static_cast<int>((e >> 30) & 3u) - 1;
+        xj.x += static_cast<float>(d.tcx[J] - d.tcx[I] + mx * L);
+        xj.y += static_cast<float>(d.tcy[J] - d.tcy[I] + my * L);
+        xj.z += static_cast<float>(d.tcz[J] - d.tcz[I] + mz * L);
+    }
+    S.xq[lane] = xj;
+    S.xq[lane + 32] = xj;
+    S.tj[lane] = tj;
+    S.tj[lane + 32] = tj;
+    S.js[lane] = js;
+    S.aj[lane] = aj;
+    uint32_t rm = rotated_columns(mk, lane);
+    __syncwarp();
+    const bool has_lj = (R.flags & F_LJ) != 0;
+    const bool has_c = PHYS && (R.flags & F_COUL_REAL) != 0;
+    // an absent term gets a cutoff (and band) at r^2 = 0, so its tests are false
+    const float rl2 = has_lj ? static_cast<float>(R.rc_lj2) : 0.f;
+    const float rcc2 = has_c ? static_cast<float>(R.rc_c2) : 0.f;
+    const float wl = rl2 * 1e-5f, wc = rcc2 * 1e-5f;
+    const float alpha = static_cast<float>(R.alpha);
+    const float a2l2e = -alpha * alpha * 1.4426950408889634f;  // -alpha^2 log2(e)
+    const float c2a = TWO_OVER_SQRTPI_F * alpha;
+    const float keqi = static_cast<float>(KE) * xi.w;
+    const float4* lj = lj_tab + R.lj_off + ti * R.n_types;
+    float fix = 0.f, fiy = 0.f, fiz = 0.f;
+    float fjx = 0.f, fjy = 0.f, fjz = 0.f;
+    float el = 0.f, ec = 0.f, vir = 0.f;
+    uint32_t band = 0;
+    const int src_lane = (lane + 1) & 31;
+#pragma unroll 1
+    for (int kk = 0; kk < 32; kk += 8) {
+        const float4* px = S.xq + lane + kk;
+        const int* pt = S.tj + lane + kk;
+        uint32_t b8 = 0;
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const bool bit = (rm >> u) & 1u;
+            const float4 pj = px[u];
+            const float4 p = lj[pt[u]];
+            const float dx = pj.x - xi.x, dy = pj.y - xi.y, dz = pj.z - xi.z;
+            const float r2 = fmaxf(dx * dx + dy * dy + dz * dz, 1e-6f);
+            const bool near = bit & ((fabsf(r2 - rl2) < wl) | (fabsf(r2 - rcc2) < wc));
+            b8 |= static_cast<uint32_t>(near) << u;
+            const bool use = bit & !near;
+            const bool in_l = use & (r2 < rl2);
+            const bool in_c = use & (r2 < rcc2);
+            const float c6f = in_l ? p.z : 0.f, c12f = in_l ? p.w : 0.f;
+            const float qq = (PHYS && in_c) ? keqi * pj.w : 0.f;
+            float ir6, rinv, erfc_ar;
+            const float f = pair_f<PHYS>(r2, c6f, c12f, qq, alpha, a2l2e, c2a, ir6, rinv, erfc_ar);
+            if (ENERGY) {
+                const float c6 = in_l ? p.x : 0.f, c12 = in_l ? p.y : 0.f;
+                el = fmaf(ir6, fmaf(c12, ir6, -c6), el);
+                if (PHYS) ec = fmaf(qq * erfc_ar, rinv, ec);
+                vir = fmaf(f, r2, vir);
+            }
+            fix = fmaf(-f, dx, fix);
+            fiy = fmaf(-f, dy, fiy);
+            fiz = fmaf(-f, dz, fiz);
+            fjx = fmaf(f, dx, fjx);
+            fjy = fmaf(f, dy, fjy);
+            fjz = fmaf(f, dz, fjz);
+            fjx = __shfl_sync(FULL, fjx, src_lane);
+            fjy = __shfl_sync(FULL, fjy, src_lane);
+            fjz = __shfl_sync(FULL, fjz, src_lane);
+        }
+        band |= b8 << kk;
+        rm >>= 8;
+    }
+    // after 32 rounds lane l holds the forces of entry l again
+    const int ai = d.atom_of_slot[si];
+    while (band) {  // pairs at a cutoff (rare): FP64 reference membership
+        const int k = __ffs(band) - 1;
+        band &= band - 1;
+        const int src = (lane + k) & 31;
+        const float4 pj = S.xq[src];
+        const float4 p = lj[S.tj[src]];
+        const int aj2 = S.aj[src];
+        const bool in_l = has_lj && exact_inside(d, ai, aj2, L, s->invL, R.rc_lj2);
+        const bool in_c = has_c && exact_inside(d, ai, aj2, L, s->invL, R.rc_c2);
+        const float dx = pj.x - xi.x, dy = pj.y - xi.y, dz = pj.z - xi.z;
+        const float r2 = fmaxf(dx * dx + dy * dy + dz * dz, 1e-6f);
+        const float qq = (PHYS && in_c) ? keqi * pj.w : 0.f;
+        float ir6, rinv, erfc_ar;
+        const float f = pair_f<PHYS>(r2, in_l ? p.z : 0.f, in_l ? p.w : 0.f, qq, alpha, a2l2e, c2a, ir6,
+                                     rinv, erfc_ar);
+        if (ENERGY) {
+            el = fmaf(ir6, fmaf(in_l ? p.y : 0.f, ir6, in_l ? -p.x : 0.f), el);
+            if (PHYS) ec = fmaf(qq * erfc_ar, rinv, ec);
+            vir = fmaf(f, r2, vir);
+        }
+        fix = fmaf(-f, dx, fix);
+        fiy = fmaf(-f, dy, fiy);
+        fiz = fmaf(-f, dz, fiz);
+        const int js2 = S.js[src];
+        fix_add(d.fnx + js2, to_fix(f * dx, FSCALE, s));
+        fix_add(d.fny + js2, to_fix(f * dy, FSCALE, s));
+        fix_add(d.fnz + js2, to_fix(f * dz, FSCALE, s));
+    }
+    if (ai >= 0) {
+        fix_add(d.fnx + si, to_fix(fix, FSCALE, s));
+        fix_add(d.fny + si, to_fix(fiy, FSCALE, s));
+        fix_add(d.fnz + si, to_fix(fiz, FSCALE, s));
+    }
+    if (mk) {
+        fix_add(d.fnx + js, to_fix(fjx, FSCALE, s));
+        fix_add(d.fny + js, to_fix(fjy, FSCALE, s));
+        fix_add(d.fnz + js, to_fix(fjz, FSCALE, s));
+    }
+    if (ENERGY) {
+        acc.lj += to_fix(el, ESCALE, s);
+        acc.c += to_fix(ec, ESCALE, s);
+        acc.v += to_fix(vir, ESCALE, s);
+    }
+    __syncwarp();
+}
+
+// LJ table entries staged in shared memory per block (larger tables are read
+// from global memory).
+constexpr int LJ_SMEM = 512;
+
+template <bool PHYS>
+__global__ void __launch_bounds__(256, 3) k_nb_f32(Dev d) {
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
-    __shared__ float4 s_xj[8][32];
-    __shared__ int s_tj[8][32];
-    __shared__ int s_aj[8][32];
-    __shared__ uint32_t s_mk[8][32];
+    __shared__ ChunkStage s_stage[8];
+    __shared__ float4 s_lj[LJ_SMEM];
+    const bool lj_shared = d.n_lj <= LJ_SMEM;
+    if (lj_shared)
+        for (int k = threadIdx.x; k < d.n_lj; k += blockDim.x) s_lj[k] = d.lj32[k];
+    __syncthreads();
+    const float4* lj_tab = lj_shared ? s_lj : d.lj32;
     const int nw = (gridDim.x * blockDim.x) >> 5;
     const int total = d.chunk_prefix[d.n_rep];
     Acc acc{0, 0, 0};
@@ -80,109 +293,8 @@ __global__ void __launch_bounds__(256) k_nb_f32(Dev d) {
         if (!s->eval) continue;
         const Rep& R = d.rep[r];
         const int c = R.chunk_begin + (w - d.chunk_prefix[r]);
-        const double L = s->L, invL = s->invL;
-        const int I = d.chunk_itile[c];
-        const int si = 32 * I + lane;
-        const float4 xi = d.xq32[si];
-        const int ti = d.type_s[si];
-        const uint32_t e = d.chunk_j[32 * c + lane];
-        const uint32_t mk = d.chunk_mask[32 * c + lane];
-        const int js = static_cast<int>(e & 0x03FFFFFFu);
-        float4 xj = make_float4(1e6f, 1e6f, 1e6f, 0.f);
-        int tj = 0, aj = -1;
-        if (mk) {
-            xj = d.xq32[js];
-            tj = d.type_s[js];
-            aj = d.atom_of_slot[js];
-            const int J = js >> 5;
-            const int mx = static_cast<int>((e >> 26) & 3u) - 1;
-            const int my = static_cast<int>((e >> 28) & 3u) - 1;
-            const int mz = static_cast<int>((e >> 30) & 3u) - 1;
-            xj.x += static_cast<float>(d.tcx[J] - d.tcx[I] + mx * L);
-            xj.y += static_cast<float>(d.tcy[J] - d.tcy[I] + my * L);
-            xj.z += static_cast<float>(d.tcz[J] - d.tcz[I] + mz * L);
-        }
-        s_xj[wib][lane] = xj;
-        s_tj[wib][lane] = tj;
-        s_aj[wib][lane] = aj;
-        s_mk[wib][lane] = mk;
-        __syncwarp();
-        const int ai = d.atom_of_slot[si];
-        const bool has_lj = (R.flags & F_LJ) != 0;
-        const bool has_c = PHYS && (R.flags & F_COUL_REAL) != 0;
-        // a term that is absent gets a cutoff of 0 so its test is always false
-        const float rl2 = has_lj ? static_cast<float>(R.rc_lj2) : 0.f;
-        const float rcc2 = has_c ? static_cast<float>(R.rc_c2) : 0.f;
-        const float bl_lo = rl2 * (1.f - 1e-5f), bl_hi = rl2 * (1.f + 1e-5f);
-        const float bc_lo = rcc2 * (1.f - 1e-5f), bc_hi = rcc2 * (1.f + 1e-5f);
-        const float alpha = static_cast<float>(R.alpha);
-        const float a2l2e = -alpha * alpha * 1.4426950408889634f;  // -alpha^2 log2(e)
-        const float keqi = static_cast<float>(KE) * xi.w;
-        const float2* lj = d.lj32 + R.lj_off + ti * R.n_types;
-        float fix = 0.f, fiy = 0.f, fiz = 0.f;
-        float fjx = 0.f, fjy = 0.f, fjz = 0.f;
-        float el = 0.f, ec = 0.f, vir = 0.f;
-#pragma unroll 2
-        for (int k = 0; k < 32; ++k) {
-            const int src = (lane + k) & 31;
-            const uint32_t m = s_mk[wib][src];
-            if ((m >> lane) & 1u) {
-                const float4 pj = s_xj[wib][src];
-                const float dx = pj.x - xi.x, dy = pj.y - xi.y, dz = pj.z - xi.z;
-                const float r2 = dx * dx + dy * dy + dz * dz;
-                bool in_l = r2 < rl2;
-                bool in_c = r2 < rcc2;
-                if ((r2 > bl_lo && r2 < bl_hi) || (r2 > bc_lo && r2 < bc_hi)) {
-                    // within 1e-5 of a cutoff: the reference's FP64 test decides
-                    const int aj2 = s_aj[wib][src];
-                    if (has_lj) in_l = exact_inside(d, ai, aj2, L, invL, R.rc_lj2);
-                    if (has_c) in_c = exact_inside(d, ai, aj2, L, invL, R.rc_c2);
-                }
-                float f = 0.f;
-                const float rinv = rsqrtf(r2);
-                const float ir2 = rinv * rinv;
-                if (in_l) {
-                    const float2 p = lj[s_tj[wib][src]];
-                    const float ir6 = ir2 * ir2 * ir2;
-                    const float c12 = p.y * ir6;
-                    f += (12.f * c12 - 6.f * p.x) * ir6 * ir2;
-                    el += (c12 - p.x) * ir6;
-                }
-                if (in_c) {
-                    const float qq = keqi * pj.w;
-                    const float ar = alpha * (r2 * rinv);
-                    const float ex = exp2f(a2l2e * r2);
-                    const float erfc_ar = erfc_as(ar, ex);
-                    f += qq * (erfc_ar * rinv + TWO_OVER_SQRTPI_F * alpha * ex) * ir2;
-                    ec += qq * erfc_ar * rinv;
-                }
-                vir += f * r2;
-                fix -= f * dx;
-                fiy -= f * dy;
-                fiz -= f * dz;
-                fjx += f * dx;
-                fjy += f * dy;
-                fjz += f * dz;
-            }
-            fjx = __shfl_sync(FULL, fjx, (lane + 1) & 31);
-            fjy = __shfl_sync(FULL, fjy, (lane + 1) & 31);
-            fjz = __shfl_sync(FULL, fjz, (lane + 1) & 31);
-        }
-        // after 32 rotations lane l again holds the forces of entry l
-        if (ai >= 0) {
-            fix_add(d.fnx + si, to_fix(fix, FSCALE, s));
-            fix_add(d.fny + si, to_fix(fiy, FSCALE, s));
-            fix_add(d.fnz + si, to_fix(fiz, FSCALE, s));
-        }
-        if (mk) {
-            fix_add(d.fnx + js, to_fix(fjx, FSCALE, s));
-            fix_add(d.fny + js, to_fix(fjy, FSCALE, s));
-            fix_add(d.fnz + js, to_fix(fjz, FSCALE, s));
-        }
-        acc.lj += to_fix(el, ESCALE, s);
-        acc.c += to_fix(ec, ESCALE, s);
-        acc.v += to_fix(vir, ESCALE, s);
-        __syncwarp();
+        if (s->want_e) nb_chunk<PHYS, true>(d, R, s, c, lane, s_stage[wib], lj_tab, acc);
+        else nb_chunk<PHYS, false>(d, R, s, c, lane, s_stage[wib], lj_tab, acc);
     }
     flush_acc(d, cur, acc);
 }
@@ -291,15 +403,14 @@ __global__ void __launch_bounds__(256) k_nb_f64(Dev d) {
 
 }  // namespace
 
-void launch_nonbonded(const Dev& d, bool fp64, bool phys, int n_sm, cudaStream_t st,
-                      long long* nlaunch) {
-    const int blocks = n_sm * 8;
+void launch_nonbonded(const Dev& d, bool fp64, bool phys, int n_sm, cudaStream_t st, long long* nlaunch) {
     if (fp64) {
-        if (phys) k_nb_f64<true><<<blocks, 256, 0, st>>>(d);
-        else k_nb_f64<false><<<blocks, 256, 0, st>>>(d);
+        if (phys) k_nb_f64<true><<<n_sm * 8, 256, 0, st>>>(d);
+        else k_nb_f64<false><<<n_sm * 8, 256, 0, st>>>(d);
     } else {
-        if (phys) k_nb_f32<true><<<blocks, 256, 0, st>>>(d);
-        else k_nb_f32<false><<<blocks, 256, 0, st>>>(d);
+        // persistent: exactly the 4 resident blocks per SM its 64 registers allow
+        if (phys) k_nb_f32<true><<<n_sm * 3, 256, 0, st>>>(d);
+        else k_nb_f32<false><<<n_sm * 3, 256, 0, st>>>(d);
     }
     *nlaunch += 1;
 }

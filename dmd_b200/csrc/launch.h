@@ -16,6 +16,7 @@ void launch_rebuild_body(const Dev& d, const int* bin_rep, bool in_graph, cudaSt
                          long long* nlaunch);
 
 // k_nonbonded.cu: LJ + real-space Ewald over the chunk list (replicas with `eval`).
+// Pair energies and virial are summed only for replicas whose `want_e` is set.
 void launch_nonbonded(const Dev& d, bool fp64, bool phys, int n_sm, cudaStream_t st,
                       long long* nlaunch);
 

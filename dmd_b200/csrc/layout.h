@@ -67,6 +67,14 @@ struct Rep {
     uint32_t key0, key1;                 // Andersen (phys) Philox key
 };
 
+// FP32 LJ coefficients of one type pair, (c6, c12, 6 c6, 12 c12) with
+// c6 = 4 eps sig^6 and c12 = 4 eps sig^12, each rounded once from FP64.
+inline float4 lj_coeffs32(double eps, double sig6) {
+    const double c6 = 4.0 * eps * sig6, c12 = 4.0 * eps * sig6 * sig6;
+    return make_float4(static_cast<float>(c6), static_cast<float>(c12), static_cast<float>(6.0 * c6),
+                       static_cast<float>(12.0 * c12));
+}
+
 // Per-replica mutable state.
 struct RepState {
     double L, invL;
@@ -88,6 +96,7 @@ struct RepState {
     int have_forces;
     int status;
     int n_chunks;
+    int want_e;           // the current evaluation's pair energies / virial are read
 };
 
 // Kernel view of the whole batch (passed by value).
@@ -138,7 +147,8 @@ struct Dev {
     const double2* dih_kp;
     // LJ tables per type pair
     const double2* lj64;               // (eps, sig^6)
-    const float2* lj32;                // (c6, c12) = (4 eps sig^6, 4 eps sig^12)
+    const float4* lj32;                // (c6, c12, 6 c6, 12 c12), c6 = 4 eps sig^6, c12 = 4 eps sig^12
+    int n_lj;                          // entries of the LJ tables (all replicas)
     // PME
     long long* mesh_fix;
     void* mesh_real;

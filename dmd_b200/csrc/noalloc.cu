@@ -63,7 +63,7 @@ constexpr size_t scratch_bytes() {
     b += 5 * up256(NB * sizeof(int));              // bin count/start/fill, vox_rank, bin_rep
     b += up256((NA + 1) * sizeof(int)) + up256(2 * NEX * sizeof(int));  // exclusion CSR
     b += up256(NC * sizeof(int)) + 2 * up256(static_cast<size_t>(NC) * 32 * sizeof(uint32_t));
-    b += up256(NTY * NTY * sizeof(double2)) + up256(NTY * NTY * sizeof(float2));
+    b += up256(NTY * NTY * sizeof(double2)) + up256(NTY * NTY * sizeof(float4));
     return b;
 }
 
@@ -216,21 +216,22 @@ extern "C" int dmdgpu_nonbonded_noalloc(const dmdgpu_nb_params* p, const double*
     d.chunk_j = reinterpret_cast<uint32_t*>(at(static_cast<size_t>(NC) * 32 * sizeof(uint32_t)));
     d.chunk_mask = reinterpret_cast<uint32_t*>(at(static_cast<size_t>(NC) * 32 * sizeof(uint32_t)));
     double2* lj64 = reinterpret_cast<double2*>(at(NTY * NTY * sizeof(double2)));
-    float2* lj32 = reinterpret_cast<float2*>(at(NTY * NTY * sizeof(float2)));
+    float4* lj32 = reinterpret_cast<float4*>(at(NTY * NTY * sizeof(float4)));
     d.lj64 = lj64;
     d.lj32 = lj32;
+    d.n_lj = p->n_types * p->n_types;
 
     if (lay.off > scratch_bytes()) return DMDGPU_ERR_GPU;  // layout and size disagree
 
     // host-side tables (no device allocation: all go into the static array)
     const int nt = p->n_types;
     std::vector<double2> h64(nt * nt);
-    std::vector<float2> h32(nt * nt);
+    std::vector<float4> h32(nt * nt);
     for (int k = 0; k < nt * nt; ++k) {
         const double sg = p->lj_sigma[k], ep = p->lj_epsilon[k];
         const double sig2 = sg * sg, sig6 = sig2 * sig2 * sig2;
         h64[k] = make_double2(ep, sig6);
-        h32[k] = make_float2(static_cast<float>(4.0 * ep * sig6), static_cast<float>(4.0 * ep * sig6 * sig6));
+        h32[k] = lj_coeffs32(ep, sig6);
     }
     std::vector<int> hvr(nbins);
     for (int ix = 0; ix < nvx; ++ix)
@@ -279,6 +280,7 @@ extern "C" int dmdgpu_nonbonded_noalloc(const dmdgpu_nb_params* p, const double*
     S.invL = 1.0 / L;
     S.rebuild = 1;
     S.eval = 1;
+    S.want_e = 1;
     S.active = 1;
     S.vscale = 1.0;
     S.pscale = 1.0;
@@ -288,7 +290,7 @@ extern "C" int dmdgpu_nonbonded_noalloc(const dmdgpu_nb_params* p, const double*
     bool good = ok(cudaMemcpyAsync(d_rep, &R, sizeof(R), cudaMemcpyHostToDevice, st)) &&
                 ok(cudaMemcpyAsync(d_st, &S, sizeof(S), cudaMemcpyHostToDevice, st)) &&
                 ok(cudaMemcpyAsync(lj64, h64.data(), sizeof(double2) * h64.size(), cudaMemcpyHostToDevice, st)) &&
-                ok(cudaMemcpyAsync(lj32, h32.data(), sizeof(float2) * h32.size(), cudaMemcpyHostToDevice, st)) &&
+                ok(cudaMemcpyAsync(lj32, h32.data(), sizeof(float4) * h32.size(), cudaMemcpyHostToDevice, st)) &&
                 ok(cudaMemcpyAsync(vox_rank, hvr.data(), sizeof(int) * nbins, cudaMemcpyHostToDevice, st)) &&
                 ok(cudaMemcpyAsync(ex_start, hes.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice, st)) &&
                 (hel.empty() ||
