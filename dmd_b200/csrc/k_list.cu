@@ -81,26 +81,33 @@ __global__ void k_bin_scatter(Dev d) {
     d.sort_buf[pos] = a;
 }
 
-// R4: sort each bin by atom index (deterministic order) and reset its counters.
+// R4: order each bin by atom index (deterministic slot order) and reset its
+// counters.  One warp per bin: every member's rank is the number of smaller
+// atom indices in the bin (indices are distinct), and it is written straight
+// to its slot in atom_of_slot.
 __global__ void k_bin_sort(Dev d, const int* bin_rep) {
-    int b = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    const int b = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (b >= d.n_bins) return;
     if (!d.st[bin_rep[b]].rebuild) return;
-    int n = d.bin_count[b];
-    if (n > 1) {
-        int* p = d.sort_buf + d.bin_start[b];
-        for (int i = 1; i < n; ++i) {
-            int v = p[i];
-            int j = i - 1;
-            while (j >= 0 && p[j] > v) {
-                p[j + 1] = p[j];
-                --j;
-            }
-            p[j + 1] = v;
+    const int n = d.bin_count[b];
+    const int* p = d.sort_buf + d.bin_start[b];
+    int* out = d.atom_of_slot + d.bin_start[b];
+    for (int base = 0; base < n; base += 32) {
+        const int v = (base + lane < n) ? p[base + lane] : 0x7fffffff;
+        int rank = 0;
+        for (int c0 = 0; c0 < n; c0 += 32) {
+            const int w = (c0 + lane < n) ? p[c0 + lane] : 0x7fffffff;
+#pragma unroll 8
+            for (int k = 0; k < 32; ++k) rank += (__shfl_sync(FULL, w, k) < v) ? 1 : 0;
         }
+        if (base + lane < n) out[rank] = v;
     }
-    d.bin_count[b] = 0;
-    d.bin_fill[b] = 0;
+    __syncwarp();
+    if (lane == 0) {
+        d.bin_count[b] = 0;
+        d.bin_fill[b] = 0;
+    }
 }
 
 // R5: tiles -- slot<->atom maps, reference positions, bounding boxes, mirror.
@@ -115,7 +122,7 @@ __global__ void k_tiles(Dev d) {
     const double L = s->L;
     const int slot = 32 * t + lane;
     const int local = slot - 32 * R.tile_begin;
-    const int a = (local < R.n_atoms) ? d.sort_buf[slot] : -1;
+    const int a = (local < R.n_atoms) ? d.atom_of_slot[slot] : -1;  // ordered by R4
     d.atom_of_slot[slot] = a;
     double w[3] = {0.0, 0.0, 0.0};
     double xa = 0, ya = 0, za = 0, qa = 0;
@@ -161,22 +168,50 @@ __global__ void k_tiles(Dev d) {
 
 // Entry encoding: bits 0..25 j slot, 26..31 image shift (mx+1, my+1, mz+1), 2 bits each.
 //
-// R6: chunk list.  A block of BW warps per i-tile; candidate j-tiles (J >= I,
-// same replica) come from a conservative bounding-box test and are dealt
-// round-robin to the warps.  Per pair: FP32 on tile-local coordinates, the
-// reference's FP64 expression within 1e-5 of the cutoff.  Each warp packs its
-// (j, mask) entries into 32-entry chunks; leftovers are merged through shared
-// memory so each i-tile ends with at most one partial chunk.
+// R6: chunk list.  A block of BW warps per i-tile, in batches of up to MAXC
+// candidate j-tiles (J >= I, same replica, conservative bounding-box test,
+// enumerated in tile order):
+//  1. enumerate the batch's candidates into shared memory;
+//  2. stage their j atoms in the i-tile's frame (all threads, independent loads);
+//  3. per candidate (round-robin over warps), lane = i atom: one ballot per j
+//     atom gives that j's 32-bit mask.  A candidate whose two tiles need more
+//     than one periodic image (small boxes) takes the general per-pair path;
+//  4. compact the non-empty entries in order and write whole chunks with one
+//     counter update per batch; fewer than 32 left over carry to the next batch.
+// Per pair: FP32 on tile-local coordinates, the reference's FP64 expression
+// within 1e-5 of the cutoff; PHYS drops excluded pairs.
 constexpr int BW = 4;
+constexpr int NT_B = 32 * BW;
+constexpr int MAXC = 48;
+constexpr float FAR = 1e18f;  // coordinate of padding atoms: r^2 overflows to +inf
+constexpr int ONE_IMAGE = 1 << 6;
 
-__global__ void __launch_bounds__(32 * BW) k_build_pairs(Dev d) {
-    const int lane = threadIdx.x & 31;
-    const int wib = threadIdx.x >> 5;
+// The reference's minimum-image r^2 < rc2 test in FP64 (src/core/pbc.h semantics).
+__device__ __forceinline__ bool ref_member(const Dev& d, int ai, int aj, double L, double invL, double rc2) {
+    double ex = __dsub_rn(d.x[aj], d.x[ai]), ey = __dsub_rn(d.y[aj], d.y[ai]), ez = __dsub_rn(d.z[aj], d.z[ai]);
+    ex = __dsub_rn(ex, __dmul_rn(round(__dmul_rn(ex, invL)), L));
+    ey = __dsub_rn(ey, __dmul_rn(round(__dmul_rn(ey, invL)), L));
+    ez = __dsub_rn(ez, __dmul_rn(round(__dmul_rn(ez, invL)), L));
+    return r2_ref(ex, ey, ez) < rc2;
+}
+
+__global__ void __launch_bounds__(NT_B, 5) k_build_pairs(Dev d) {
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const int wib = tid >> 5;
     const int I = blockIdx.x;
     __shared__ float s_lx[32], s_ly[32], s_lz[32];
     __shared__ int s_a[32];
-    __shared__ uint32_t s_e[BW][64], s_m[BW][64];
+    __shared__ uint32_t s_e[BW][64], s_m[BW][64];   // general path: per-warp entry buffers
     __shared__ int s_left[BW];
+    __shared__ int s_cand[MAXC], s_cinfo[MAXC];
+    __shared__ float4 s_jx[MAXC * 32];               // staged j atoms (w = atom index bits);
+                                                     // reused for compaction
+    __shared__ uint32_t s_je[MAXC * 32];             // staged j entry words
+    __shared__ uint32_t s_msk[MAXC * 32];
+    __shared__ uint32_t s_carry_e[32], s_carry_m[32];
+    __shared__ int s_wcnt[4][BW];
+    __shared__ int s_jnext, s_c0;
     if (I >= d.n_tiles) return;
     const int r = d.tile_rep[I];
     RepState* s = d.st + r;
@@ -200,9 +235,27 @@ __global__ void __launch_bounds__(32 * BW) k_build_pairs(Dev d) {
     __syncthreads();
     const float hIx = d.thx[I], hIy = d.thy[I], hIz = d.thz[I];
     const int t_end = R.tile_begin + R.n_tiles;
-    int nbuf = 0;        // entries buffered in s_e/s_m[wib] (warp-uniform)
-    int cand_seen = 0;   // candidates enumerated so far (round-robin over warps)
+    // this lane's i atom and (PHYS) its exclusion partners, sorted ascending
+    const int ai = s_a[lane];
+    // a padding i lane sits far away (+FAR), padding j atoms at -FAR: no pair
+    const float lix = ai >= 0 ? s_lx[lane] : FAR, liy = ai >= 0 ? s_ly[lane] : FAR,
+                liz = ai >= 0 ? s_lz[lane] : FAR;
+    int iex[8];
+    // exclusion partners span [i_lo, i_lo + i_span]; an empty set never matches
+    int i_e0 = 0, i_e1 = 0, i_lo = 0x7fffffff, i_span = 0;
+    if (phys && ai >= 0) {
+        i_e0 = d.ex_start[ai];
+        i_e1 = d.ex_start[ai + 1];
+        if (i_e1 > i_e0) {
+            i_lo = d.ex_list[i_e0];
+            i_span = d.ex_list[i_e1 - 1] - i_lo;
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 8; ++k) iex[k] = (i_e0 + k < i_e1) ? d.ex_list[i_e0 + k] : -1;
 
+    // ---- general path (several periodic images per tile pair) ----------------
+    int nbuf = 0;  // entries buffered in s_e/s_m[wib] (warp-uniform)
     auto flush_chunk = [&](const uint32_t* be, const uint32_t* bm, int count) {
         int c = 0;
         if (lane == 0) c = atomicAdd(&s->n_chunks, 1);
@@ -236,104 +289,302 @@ __global__ void __launch_bounds__(32 * BW) k_build_pairs(Dev d) {
             __syncwarp();
         }
     };
-
-    for (int J0 = I; J0 < t_end; J0 += 32) {
-        const int Jl = J0 + lane;
-        bool cand = false;
-        if (Jl < t_end) {
-            double dx = d.tcx[Jl] - cIx, dy = d.tcy[Jl] - cIy, dz = d.tcz[Jl] - cIz;
-            dx -= L * round(dx * invL);
-            dy -= L * round(dy * invL);
-            dz -= L * round(dz * invL);
-            double gx = fmax(fabs(dx) - (double)(hIx + d.thx[Jl]), 0.0);
-            double gy = fmax(fabs(dy) - (double)(hIy + d.thy[Jl]), 0.0);
-            double gz = fmax(fabs(dz) - (double)(hIz + d.thz[Jl]), 0.0);
-            cand = gx * gx + gy * gy + gz * gz <= bb_rc2;
+    // One candidate tile J, lane = j atom: each j is tested against every i,
+    // and every periodic image code found becomes its own entry.
+    auto general_candidate = [&](int J) {
+        const int js = 32 * J + lane;
+        const int aj = d.atom_of_slot[js];
+        const double ddx = d.tcx[J] - cIx, ddy = d.tcy[J] - cIy, ddz = d.tcz[J] - cIz;
+        const double rx0 = round(ddx * invL), ry0 = round(ddy * invL), rz0 = round(ddz * invL);
+        float jx = 0.f, jy = 0.f, jz = 0.f;
+        int ex[8];
+        int nex = 0, e0 = 0, e1 = 0;
+        if (aj >= 0) {
+            jx = static_cast<float>((d.x[aj] - d.imgx[aj] * L) - cIx - rx0 * L);
+            jy = static_cast<float>((d.y[aj] - d.imgy[aj] * L) - cIy - ry0 * L);
+            jz = static_cast<float>((d.z[aj] - d.imgz[aj] * L) - cIz - rz0 * L);
+            e0 = d.ex_start[aj];
+            e1 = d.ex_start[aj + 1];
+            if (phys) nex = e1 - e0;
         }
-        uint32_t cb = __ballot_sync(FULL, cand);
-        while (cb) {
-            const int J = J0 + __ffs(cb) - 1;
-            cb &= cb - 1;
-            if ((cand_seen++ % BW) != wib) continue;
-            const int js = 32 * J + lane;
-            const int aj = d.atom_of_slot[js];
-            const double ddx = d.tcx[J] - cIx, ddy = d.tcy[J] - cIy, ddz = d.tcz[J] - cIz;
-            const double rx0 = round(ddx * invL), ry0 = round(ddy * invL), rz0 = round(ddz * invL);
-            // j atom in i-tile-local frame (centre image), exclusion partners
-            float jx = 0.f, jy = 0.f, jz = 0.f;
-            int ex[8];
-            int nex = 0, e0 = 0, e1 = 0;
-            if (aj >= 0) {
-                const double wjx = d.x[aj] - d.imgx[aj] * L, wjy = d.y[aj] - d.imgy[aj] * L,
-                             wjz = d.z[aj] - d.imgz[aj] * L;
-                jx = static_cast<float>(wjx - cIx - rx0 * L);
-                jy = static_cast<float>(wjy - cIy - ry0 * L);
-                jz = static_cast<float>(wjz - cIz - rz0 * L);
-                e0 = d.ex_start[aj];
-                e1 = d.ex_start[aj + 1];
-                if (phys) nex = e1 - e0;
-            }
 #pragma unroll
-            for (int k = 0; k < 8; ++k) ex[k] = (k < nex) ? d.ex_list[e0 + k] : -1;
-            // Pairs of one j atom normally share one periodic image; in small boxes
-            // (tile extent ~ L/4) several can occur.  Each pass emits the entry of
-            // one image code and leaves the i atoms with other codes for the next.
-            uint32_t todo = 0;
-            if (aj >= 0) todo = (J == I) ? ((1u << lane) - 1u) : 0xffffffffu;
-            while (__any_sync(FULL, todo != 0)) {
-                uint32_t bits = 0, rest = 0, code0 = 0xffffffffu;
-                for (uint32_t t = todo; t; t &= t - 1) {
-                    const int i = __ffs(t) - 1;
-                    const int ai = s_a[i];
-                    if (ai < 0) continue;
-                    float dx = jx - s_lx[i], dy = jy - s_ly[i], dz = jz - s_lz[i];
-                    int sx = 0, sy = 0, sz = 0;
-                    if (dx > hLf) { dx -= Lf; sx = 1; } else if (dx < -hLf) { dx += Lf; sx = -1; }
-                    if (dy > hLf) { dy -= Lf; sy = 1; } else if (dy < -hLf) { dy += Lf; sy = -1; }
-                    if (dz > hLf) { dz -= Lf; sz = 1; } else if (dz < -hLf) { dz += Lf; sz = -1; }
-                    const float r2 = dx * dx + dy * dy + dz * dz;
-                    if (r2 >= rc2_hi) continue;
-                    int mx, my, mz;
-                    if (r2 > rc2_lo) {
-                        // borderline: the reference's FP64 expression decides
-                        double ex_ = __dsub_rn(d.x[aj], d.x[ai]), ey = __dsub_rn(d.y[aj], d.y[ai]),
-                               ez = __dsub_rn(d.z[aj], d.z[ai]);
-                        const double qx = round(__dmul_rn(ex_, invL)), qy = round(__dmul_rn(ey, invL)),
-                                     qz = round(__dmul_rn(ez, invL));
-                        ex_ = __dsub_rn(ex_, __dmul_rn(qx, L));
-                        ey = __dsub_rn(ey, __dmul_rn(qy, L));
-                        ez = __dsub_rn(ez, __dmul_rn(qz, L));
-                        if (!(r2_ref(ex_, ey, ez) < rc2)) continue;
-                        mx = d.imgx[aj] - d.imgx[ai] - static_cast<int>(qx);
-                        my = d.imgy[aj] - d.imgy[ai] - static_cast<int>(qy);
-                        mz = d.imgz[aj] - d.imgz[ai] - static_cast<int>(qz);
-                    } else {
-                        // displacement = w_j - w_i - (r0 + s) L
-                        mx = -static_cast<int>(rx0) - sx;
-                        my = -static_cast<int>(ry0) - sy;
-                        mz = -static_cast<int>(rz0) - sz;
-                    }
-                    if (phys) {
-                        bool excluded = false;
-                        if (nex <= 8) {
-#pragma unroll
-                            for (int k = 0; k < 8; ++k) excluded |= (ex[k] == ai);
-                        } else {
-                            for (int e = e0; e < e1; ++e) excluded |= (d.ex_list[e] == ai);
-                        }
-                        if (excluded) continue;
-                    }
-                    const uint32_t code = static_cast<uint32_t>((mx + 1) | ((my + 1) << 2) | ((mz + 1) << 4));
-                    if (code0 == 0xffffffffu) code0 = code;
-                    if (code == code0) bits |= 1u << i;
-                    else rest |= 1u << i;
+        for (int k = 0; k < 8; ++k) ex[k] = (k < nex) ? d.ex_list[e0 + k] : -1;
+        uint32_t todo = 0;
+        if (aj >= 0) todo = (J == I) ? ((1u << lane) - 1u) : 0xffffffffu;
+        while (__any_sync(FULL, todo != 0)) {
+            uint32_t bits = 0, rest = 0, code0 = 0xffffffffu;
+            for (uint32_t t = todo; t; t &= t - 1) {
+                const int i = __ffs(t) - 1;
+                const int a_i = s_a[i];
+                if (a_i < 0) continue;
+                float dx = jx - s_lx[i], dy = jy - s_ly[i], dz = jz - s_lz[i];
+                int sx = 0, sy = 0, sz = 0;
+                if (dx > hLf) { dx -= Lf; sx = 1; } else if (dx < -hLf) { dx += Lf; sx = -1; }
+                if (dy > hLf) { dy -= Lf; sy = 1; } else if (dy < -hLf) { dy += Lf; sy = -1; }
+                if (dz > hLf) { dz -= Lf; sz = 1; } else if (dz < -hLf) { dz += Lf; sz = -1; }
+                const float r2 = dx * dx + dy * dy + dz * dz;
+                if (r2 >= rc2_hi) continue;
+                int mx, my, mz;
+                if (r2 > rc2_lo) {
+                    // borderline: the reference's FP64 expression decides
+                    double ex_ = __dsub_rn(d.x[aj], d.x[a_i]), ey = __dsub_rn(d.y[aj], d.y[a_i]),
+                           ez = __dsub_rn(d.z[aj], d.z[a_i]);
+                    const double qx = round(__dmul_rn(ex_, invL)), qy = round(__dmul_rn(ey, invL)),
+                                 qz = round(__dmul_rn(ez, invL));
+                    ex_ = __dsub_rn(ex_, __dmul_rn(qx, L));
+                    ey = __dsub_rn(ey, __dmul_rn(qy, L));
+                    ez = __dsub_rn(ez, __dmul_rn(qz, L));
+                    if (!(r2_ref(ex_, ey, ez) < rc2)) continue;
+                    mx = d.imgx[aj] - d.imgx[a_i] - static_cast<int>(qx);
+                    my = d.imgy[aj] - d.imgy[a_i] - static_cast<int>(qy);
+                    mz = d.imgz[aj] - d.imgz[a_i] - static_cast<int>(qz);
+                } else {
+                    // displacement = w_j - w_i - (r0 + s) L
+                    mx = -static_cast<int>(rx0) - sx;
+                    my = -static_cast<int>(ry0) - sy;
+                    mz = -static_cast<int>(rz0) - sz;
                 }
-                push(static_cast<uint32_t>(js) | ((bits ? code0 : 0u) << 26), bits);
-                todo = rest;
+                if (phys) {
+                    bool excluded = false;
+                    if (nex <= 8) {
+#pragma unroll
+                        for (int k = 0; k < 8; ++k) excluded |= (ex[k] == a_i);
+                    } else {
+                        for (int e = e0; e < e1; ++e) excluded |= (d.ex_list[e] == a_i);
+                    }
+                    if (excluded) continue;
+                }
+                const uint32_t code = static_cast<uint32_t>((mx + 1) | ((my + 1) << 2) | ((mz + 1) << 4));
+                if (code0 == 0xffffffffu) code0 = code;
+                if (code == code0) bits |= 1u << i;
+                else rest |= 1u << i;
+            }
+            push(static_cast<uint32_t>(js) | ((bits ? code0 : 0u) << 26), bits);
+            todo = rest;
+        }
+    };
+
+    int carry_n = 0;
+    int J_next = I;
+    while (J_next < t_end) {
+        // 1. candidates of this batch, in tile order
+        if (tid == 0) s_jnext = t_end;
+        int nc = 0;
+        int J0 = J_next;
+        while (J0 < t_end && nc < MAXC) {
+            const int J = J0 + tid;
+            bool cand = false;
+            int info = 0;
+            if (J < t_end) {
+                double dx = d.tcx[J] - cIx, dy = d.tcy[J] - cIy, dz = d.tcz[J] - cIz;
+                const double rx0 = round(dx * invL), ry0 = round(dy * invL), rz0 = round(dz * invL);
+                dx -= L * rx0;
+                dy -= L * ry0;
+                dz -= L * rz0;
+                const double ex = (double)(hIx + d.thx[J]), ey = (double)(hIy + d.thy[J]),
+                             ez = (double)(hIz + d.thz[J]);
+                const double gx = fmax(fabs(dx) - ex, 0.0), gy = fmax(fabs(dy) - ey, 0.0),
+                             gz = fmax(fabs(dz) - ez, 0.0);
+                cand = gx * gx + gy * gy + gz * gz <= bb_rc2;
+                // one periodic image serves every pair of the two tiles when their
+                // extents around the centre displacement stay inside half a box
+                const double hL = 0.5 * L;
+                const bool one = fabs(dx) + ex < hL && fabs(dy) + ey < hL && fabs(dz) + ez < hL;
+                info = (static_cast<int>(rx0) + 1) | ((static_cast<int>(ry0) + 1) << 2) |
+                       ((static_cast<int>(rz0) + 1) << 4) | (one ? ONE_IMAGE : 0);
+            }
+            const uint32_t b = __ballot_sync(FULL, cand);
+            if (lane == 0) s_wcnt[0][wib] = __popc(b);
+            __syncthreads();
+            int before = nc, tot = 0;
+#pragma unroll
+            for (int w = 0; w < BW; ++w) {
+                before += (w < wib) ? s_wcnt[0][w] : 0;
+                tot += s_wcnt[0][w];
+            }
+            const int rank = before + __popc(b & ((1u << lane) - 1u));
+            if (cand) {
+                if (rank < MAXC) {
+                    s_cand[rank] = J;
+                    s_cinfo[rank] = info;
+                } else if (rank == MAXC) {
+                    s_jnext = J;  // first candidate left for the next batch
+                }
+            }
+            nc += tot;
+            J0 += NT_B;
+            __syncthreads();
+        }
+        J_next = (nc > MAXC) ? s_jnext : J0;
+        if (nc > MAXC) nc = MAXC;
+        // 2. stage, in order, the j atoms of single-image candidates that lie
+        //    within the list cutoff of the i-tile's box (i-tile frame, FP32)
+        int nj = 0;
+        for (int e0 = 0; e0 < nc * 32; e0 += 4 * NT_B) {
+            float4 pj[4];
+            uint32_t ent[4];
+            bool keep[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int idx = e0 + u * NT_B + tid;
+                keep[u] = false;
+                ent[u] = 0u;
+                pj[u] = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (idx >= nc * 32) continue;
+                const int k = idx >> 5, info = s_cinfo[k];
+                if (!(info & ONE_IMAGE)) continue;
+                const int js = 32 * s_cand[k] + (idx & 31);
+                const int aj = d.atom_of_slot[js];
+                if (aj < 0) continue;
+                const double sx = static_cast<double>((info & 3) - 1) * L;
+                const double sy = static_cast<double>(((info >> 2) & 3) - 1) * L;
+                const double sz = static_cast<double>(((info >> 4) & 3) - 1) * L;
+                pj[u].x = static_cast<float>((d.x[aj] - d.imgx[aj] * L) - cIx - sx);
+                pj[u].y = static_cast<float>((d.y[aj] - d.imgy[aj] * L) - cIy - sy);
+                pj[u].z = static_cast<float>((d.z[aj] - d.imgz[aj] * L) - cIz - sz);
+                pj[u].w = __int_as_float(aj);
+                const float gx = fmaxf(fabsf(pj[u].x) - hIx, 0.f), gy = fmaxf(fabsf(pj[u].y) - hIy, 0.f),
+                            gz = fmaxf(fabsf(pj[u].z) - hIz, 0.f);
+                keep[u] = gx * gx + gy * gy + gz * gz <= rc2_hi * 1.0001f + 1e-6f;
+                const uint32_t code = static_cast<uint32_t>((2 - (info & 3)) | ((2 - ((info >> 2) & 3)) << 2) |
+                                                            ((2 - ((info >> 4) & 3)) << 4));
+                ent[u] = static_cast<uint32_t>(js) | (code << 26);
+            }
+            uint32_t bal[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                bal[u] = __ballot_sync(FULL, keep[u]);
+                if (lane == 0) s_wcnt[u][wib] = __popc(bal[u]);
+            }
+            __syncthreads();
+            int run = nj;
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                int before = run, tot = 0;
+#pragma unroll
+                for (int w = 0; w < BW; ++w) {
+                    before += (w < wib) ? s_wcnt[u][w] : 0;
+                    tot += s_wcnt[u][w];
+                }
+                if (keep[u]) {
+                    const int pos = before + __popc(bal[u] & ((1u << lane) - 1u));
+                    s_jx[pos] = pj[u];
+                    s_je[pos] = ent[u];
+                }
+                run += tot;
+            }
+            nj = run;
+            __syncthreads();
+        }
+        const int ngroups = (nj + 31) >> 5;
+        for (int idx = nj + tid; idx < 32 * ngroups; idx += NT_B) {
+            s_jx[idx] = make_float4(-FAR, -FAR, -FAR, __int_as_float(-1));
+            s_je[idx] = 0u;
+        }
+        __syncthreads();
+        // 3. masks, 32 staged j atoms per warp pass; lane = i atom, one ballot per
+        //    j.  Pairs at the cutoff band or among the i atom's exclusion partners
+        //    are settled after the pass (rare): FP64 reference test, exclusions.
+        for (int g = wib; g < ngroups; g += BW) {
+            const float4* pjs = s_jx + 32 * g;
+            uint32_t rare = 0;
+#pragma unroll
+            for (int j = 0; j < 32; ++j) {
+                const float4 pj = pjs[j];
+                const int a2 = __float_as_int(pj.w);
+                const float dx = pj.x - lix, dy = pj.y - liy, dz = pj.z - liz;
+                const float r2 = dx * dx + dy * dy + dz * dz;
+                const bool exr = static_cast<unsigned>(a2 - i_lo) <= static_cast<unsigned>(i_span);
+                const bool in = (r2 < rc2_lo) & !exr;
+                rare |= static_cast<uint32_t>((r2 < rc2_hi) & ((r2 >= rc2_lo) | exr)) << j;
+                const uint32_t m = __ballot_sync(FULL, in);
+                if (lane == 0) s_msk[32 * g + j] = m;
+            }
+            __syncwarp();
+            while (rare) {
+                const int j = __ffs(rare) - 1;
+                rare &= rare - 1;
+                const float4 pj = pjs[j];
+                const int a2 = __float_as_int(pj.w);
+                const float dx = pj.x - lix, dy = pj.y - liy, dz = pj.z - liz;
+                const float r2 = dx * dx + dy * dy + dz * dz;
+                bool in = (r2 < rc2_lo) || ref_member(d, ai, a2, L, invL, rc2);
+                if (in && static_cast<unsigned>(a2 - i_lo) <= static_cast<unsigned>(i_span)) {
+                    if (i_e1 - i_e0 <= 8) {
+#pragma unroll
+                        for (int q = 0; q < 8; ++q) in &= (iex[q] != a2);
+                    } else {
+                        for (int e = i_e0; e < i_e1; ++e) in &= (d.ex_list[e] != a2);
+                    }
+                }
+                if (in) atomicOr(&s_msk[32 * g + j], 1u << lane);
             }
         }
+        // general path for candidates that need several periodic images
+        for (int k = wib; k < nc; k += BW)
+            if (!(s_cinfo[k] & ONE_IMAGE)) general_candidate(s_cand[k]);
+        __syncthreads();
+        // 4. ordered compaction of the non-empty entries (s_jx reused), whole chunks out
+        uint32_t* s_oe = reinterpret_cast<uint32_t*>(s_jx);
+        uint32_t* s_om = s_oe + (MAXC * 32 + 32);
+        if (tid < carry_n) {
+            s_oe[tid] = s_carry_e[tid];
+            s_om[tid] = s_carry_m[tid];
+        }
+        int base = carry_n;
+        for (int e0 = 0; e0 < nj; e0 += NT_B) {
+            const int idx = e0 + tid;
+            uint32_t m = 0u, e = 0u;
+            if (idx < nj) {
+                m = s_msk[idx];
+                e = s_je[idx];
+                // within the i-tile itself only pairs i < j
+                const int js = static_cast<int>(e & 0x03FFFFFFu);
+                if ((js >> 5) == I) m &= (1u << (js & 31)) - 1u;
+            }
+            const uint32_t b = __ballot_sync(FULL, m != 0u);
+            if (lane == 0) s_wcnt[0][wib] = __popc(b);
+            __syncthreads();
+            int before = base, tot = 0;
+#pragma unroll
+            for (int w = 0; w < BW; ++w) {
+                before += (w < wib) ? s_wcnt[0][w] : 0;
+                tot += s_wcnt[0][w];
+            }
+            if (m) {
+                const int pos = before + __popc(b & ((1u << lane) - 1u));
+                s_oe[pos] = e;
+                s_om[pos] = m;
+            }
+            base += tot;
+            __syncthreads();
+        }
+        const int nfull = base >> 5;
+        if (nfull > 0) {
+            if (tid == 0) {
+                const int c0 = atomicAdd(&s->n_chunks, nfull);
+                s_c0 = c0;
+                if (c0 + nfull > R.chunk_cap) set_status(s, ST_CAPACITY);
+            }
+            __syncthreads();
+            const int c0 = s_c0;
+            for (int idx = tid; idx < nfull * 32; idx += NT_B) {
+                const int c = c0 + (idx >> 5);
+                if (c >= R.chunk_cap) continue;
+                const int g = R.chunk_begin + c;
+                if ((idx & 31) == 0) d.chunk_itile[g] = I;
+                d.chunk_j[32 * g + (idx & 31)] = s_oe[idx];
+                d.chunk_mask[32 * g + (idx & 31)] = s_om[idx];
+            }
+        }
+        carry_n = base - 32 * nfull;
+        if (tid < carry_n) {
+            s_carry_e[tid] = s_oe[32 * nfull + tid];
+            s_carry_m[tid] = s_om[32 * nfull + tid];
+        }
+        __syncthreads();
     }
-    // merge the warps' leftovers: warp 0 collects them and flushes
+    // merge the carry and the general path's leftovers: warp 0 flushes them
     if (lane == 0) s_left[wib] = nbuf;
     __syncthreads();
     if (wib == 0) {
@@ -344,6 +595,7 @@ __global__ void __launch_bounds__(32 * BW) k_build_pairs(Dev d) {
                 push(mine ? s_e[w][base + lane] : 0u, mine ? s_m[w][base + lane] : 0u);
             }
         }
+        push(lane < carry_n ? s_carry_e[lane] : 0u, lane < carry_n ? s_carry_m[lane] : 0u);
         if (nbuf > 0) flush_chunk(s_e[0], s_m[0], nbuf);
     }
 }
@@ -398,9 +650,9 @@ void launch_rebuild_body(const Dev& d, const int* bin_rep, bool in_graph, cudaSt
     k_bin_atoms<<<(d.n_atoms + T - 1) / T, T, 0, st>>>(d);
     k_bin_scan<<<d.n_rep, 1024, 0, st>>>(d);
     k_bin_scatter<<<(d.n_atoms + T - 1) / T, T, 0, st>>>(d);
-    k_bin_sort<<<(d.n_bins + T - 1) / T, T, 0, st>>>(d, bin_rep);
+    k_bin_sort<<<(d.n_bins + T / 32 - 1) / (T / 32), T, 0, st>>>(d, bin_rep);
     k_tiles<<<(d.n_tiles * 32 + T - 1) / T, T, 0, st>>>(d);
-    k_build_pairs<<<d.n_tiles, 32 * BW, 0, st>>>(d);
+    k_build_pairs<<<d.n_tiles, NT_B, 0, st>>>(d);
     k_rebuild_finish<<<1, 32, 0, st>>>(d, in_graph ? 1 : 0);
     *nlaunch += 7;
 }
