@@ -511,6 +511,7 @@ int Batch::pack() {
         d.atom_of_slot = A.alloc<int>(d.n_slots);
         if (fp64_) d.xq64 = A.alloc<double4>(d.n_slots);
         else d.xq32 = A.alloc<float4>(d.n_slots);
+        d.xl32 = fp64_ ? A.alloc<float4>(d.n_slots) : d.xq32;
         d.type_s = A.alloc<int>(d.n_slots);
         d.fnx = A.alloc<long long>(d.n_slots);
         d.fny = A.alloc<long long>(d.n_slots);

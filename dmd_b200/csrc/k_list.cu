@@ -158,11 +158,10 @@ __global__ void k_tiles(Dev d) {
         d.thy[t] = h[1];
         d.thz[t] = h[2];
     }
-    if (d.xq32) {
-        d.xq32[slot] = (a >= 0) ? make_float4(static_cast<float>(w[0] - c[0]), static_cast<float>(w[1] - c[1]),
-                                              static_cast<float>(w[2] - c[2]), static_cast<float>(qa))
-                                : make_float4(0.f, 0.f, 0.f, 0.f);
-    }
+    // build-frame FP32 coordinates (the mixed-precision mirror itself when it exists)
+    d.xl32[slot] = (a >= 0) ? make_float4(static_cast<float>(w[0] - c[0]), static_cast<float>(w[1] - c[1]),
+                                          static_cast<float>(w[2] - c[2]), static_cast<float>(qa))
+                            : make_float4(0.f, 0.f, 0.f, 0.f);
     if (d.xq64) d.xq64[slot] = make_double4(xa, ya, za, qa);
 }
 
@@ -205,6 +204,7 @@ __global__ void __launch_bounds__(NT_B, 5) k_build_pairs(Dev d) {
     __shared__ uint32_t s_e[BW][64], s_m[BW][64];   // general path: per-warp entry buffers
     __shared__ int s_left[BW];
     __shared__ int s_cand[MAXC], s_cinfo[MAXC];
+    __shared__ float4 s_coff[MAXC];                  // j-tile frame -> i-tile frame (FP32)
     __shared__ float4 s_jx[MAXC * 32];               // staged j atoms (w = atom index bits);
                                                      // reused for compaction
     __shared__ uint32_t s_je[MAXC * 32];             // staged j entry words
@@ -227,10 +227,11 @@ __global__ void __launch_bounds__(NT_B, 5) k_build_pairs(Dev d) {
     const double cIx = d.tcx[I], cIy = d.tcy[I], cIz = d.tcz[I];
     if (wib == 0) {
         const int a = d.atom_of_slot[32 * I + lane];
+        const float4 p = d.xl32[32 * I + lane];
         s_a[lane] = a;
-        s_lx[lane] = a >= 0 ? static_cast<float>((d.x[a] - d.imgx[a] * L) - cIx) : 0.f;
-        s_ly[lane] = a >= 0 ? static_cast<float>((d.y[a] - d.imgy[a] * L) - cIy) : 0.f;
-        s_lz[lane] = a >= 0 ? static_cast<float>((d.z[a] - d.imgz[a] * L) - cIz) : 0.f;
+        s_lx[lane] = p.x;
+        s_ly[lane] = p.y;
+        s_lz[lane] = p.z;
     }
     __syncthreads();
     const float hIx = d.thx[I], hIy = d.thy[I], hIz = d.thz[I];
@@ -367,15 +368,21 @@ __global__ void __launch_bounds__(NT_B, 5) k_build_pairs(Dev d) {
     int carry_n = 0;
     int J_next = I;
     while (J_next < t_end) {
-        // 1. candidates of this batch, in tile order
+        // 1. candidates of this batch, in tile order (4 tiles per thread per round)
         if (tid == 0) s_jnext = t_end;
         int nc = 0;
         int J0 = J_next;
         while (J0 < t_end && nc < MAXC) {
-            const int J = J0 + tid;
-            bool cand = false;
-            int info = 0;
-            if (J < t_end) {
+            bool cand[4];
+            int info[4];
+            float4 off[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int J = J0 + u * NT_B + tid;
+                cand[u] = false;
+                info[u] = 0;
+                off[u] = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (J >= t_end) continue;
                 double dx = d.tcx[J] - cIx, dy = d.tcy[J] - cIy, dz = d.tcz[J] - cIz;
                 const double rx0 = round(dx * invL), ry0 = round(dy * invL), rz0 = round(dz * invL);
                 dx -= L * rx0;
@@ -385,34 +392,43 @@ __global__ void __launch_bounds__(NT_B, 5) k_build_pairs(Dev d) {
                              ez = (double)(hIz + d.thz[J]);
                 const double gx = fmax(fabs(dx) - ex, 0.0), gy = fmax(fabs(dy) - ey, 0.0),
                              gz = fmax(fabs(dz) - ez, 0.0);
-                cand = gx * gx + gy * gy + gz * gz <= bb_rc2;
+                cand[u] = gx * gx + gy * gy + gz * gz <= bb_rc2;
                 // one periodic image serves every pair of the two tiles when their
                 // extents around the centre displacement stay inside half a box
                 const double hL = 0.5 * L;
                 const bool one = fabs(dx) + ex < hL && fabs(dy) + ey < hL && fabs(dz) + ez < hL;
-                info = (static_cast<int>(rx0) + 1) | ((static_cast<int>(ry0) + 1) << 2) |
-                       ((static_cast<int>(rz0) + 1) << 4) | (one ? ONE_IMAGE : 0);
+                info[u] = (static_cast<int>(rx0) + 1) | ((static_cast<int>(ry0) + 1) << 2) |
+                          ((static_cast<int>(rz0) + 1) << 4) | (one ? ONE_IMAGE : 0);
+                off[u] = make_float4(static_cast<float>(dx), static_cast<float>(dy), static_cast<float>(dz), 0.f);
             }
-            const uint32_t b = __ballot_sync(FULL, cand);
-            if (lane == 0) s_wcnt[0][wib] = __popc(b);
-            __syncthreads();
-            int before = nc, tot = 0;
+            uint32_t bal[4];
 #pragma unroll
-            for (int w = 0; w < BW; ++w) {
-                before += (w < wib) ? s_wcnt[0][w] : 0;
-                tot += s_wcnt[0][w];
+            for (int u = 0; u < 4; ++u) {
+                bal[u] = __ballot_sync(FULL, cand[u]);
+                if (lane == 0) s_wcnt[u][wib] = __popc(bal[u]);
             }
-            const int rank = before + __popc(b & ((1u << lane) - 1u));
-            if (cand) {
-                if (rank < MAXC) {
-                    s_cand[rank] = J;
-                    s_cinfo[rank] = info;
-                } else if (rank == MAXC) {
-                    s_jnext = J;  // first candidate left for the next batch
+            __syncthreads();
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                int before = nc, tot = 0;
+#pragma unroll
+                for (int w = 0; w < BW; ++w) {
+                    before += (w < wib) ? s_wcnt[u][w] : 0;
+                    tot += s_wcnt[u][w];
                 }
+                const int rank = before + __popc(bal[u] & ((1u << lane) - 1u));
+                if (cand[u]) {
+                    if (rank < MAXC) {
+                        s_cand[rank] = J0 + u * NT_B + tid;
+                        s_cinfo[rank] = info[u];
+                        s_coff[rank] = off[u];
+                    } else if (rank == MAXC) {
+                        s_jnext = J0 + u * NT_B + tid;  // first candidate left for the next batch
+                    }
+                }
+                nc += tot;
             }
-            nc += tot;
-            J0 += NT_B;
+            J0 += 4 * NT_B;
             __syncthreads();
         }
         J_next = (nc > MAXC) ? s_jnext : J0;
@@ -436,13 +452,9 @@ __global__ void __launch_bounds__(NT_B, 5) k_build_pairs(Dev d) {
                 const int js = 32 * s_cand[k] + (idx & 31);
                 const int aj = d.atom_of_slot[js];
                 if (aj < 0) continue;
-                const double sx = static_cast<double>((info & 3) - 1) * L;
-                const double sy = static_cast<double>(((info >> 2) & 3) - 1) * L;
-                const double sz = static_cast<double>(((info >> 4) & 3) - 1) * L;
-                pj[u].x = static_cast<float>((d.x[aj] - d.imgx[aj] * L) - cIx - sx);
-                pj[u].y = static_cast<float>((d.y[aj] - d.imgy[aj] * L) - cIy - sy);
-                pj[u].z = static_cast<float>((d.z[aj] - d.imgz[aj] * L) - cIz - sz);
-                pj[u].w = __int_as_float(aj);
+                const float4 p = d.xl32[js];
+                const float4 o = s_coff[k];
+                pj[u] = make_float4(p.x + o.x, p.y + o.y, p.z + o.z, __int_as_float(aj));
                 const float gx = fmaxf(fabsf(pj[u].x) - hIx, 0.f), gy = fmaxf(fabsf(pj[u].y) - hIy, 0.f),
                             gz = fmaxf(fabsf(pj[u].z) - hIz, 0.f);
                 keep[u] = gx * gx + gy * gy + gz * gz <= rc2_hi * 1.0001f + 1e-6f;

@@ -116,6 +116,7 @@ struct Dev {
     // sorted slots
     int* atom_of_slot;
     float4* xq32;                      // tile-local FP32 coordinates + charge
+    float4* xl32;                      // the same at the last list build (aliases xq32 when mixed)
     double4* xq64;                     // unwrapped FP64 coordinates + charge
     int* type_s;
     long long *fnx, *fny, *fnz;        // non-bonded forces (fixed point, slot order)

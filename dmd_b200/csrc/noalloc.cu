@@ -58,6 +58,7 @@ constexpr size_t scratch_bytes() {
     b += up256(NA * sizeof(int));                  // validated copy of the caller's types
     b += up256(NA * sizeof(int)) * 3;              // atom_of_slot, type_s, sort_buf
     b += up256(NA * sizeof(double4));              // xq (float4 or double4)
+    b += up256(NA * sizeof(float4));               // xl32 (build-frame copy, FP64 mode)
     b += 3 * up256(NA * sizeof(long long));        // fnx/fny/fnz
     b += 3 * up256(NT * sizeof(double)) + 3 * up256(NT * sizeof(float)) + up256(NT * sizeof(int));
     b += 5 * up256(NB * sizeof(int));              // bin count/start/fill, vox_rank, bin_rep
@@ -191,6 +192,8 @@ extern "C" int dmdgpu_nonbonded_noalloc(const dmdgpu_nb_params* p, const double*
     unsigned char* xq = at(NA * sizeof(double4));
     if (fp64) d.xq64 = reinterpret_cast<double4*>(xq);
     else d.xq32 = reinterpret_cast<float4*>(xq);
+    unsigned char* xl = at(NA * sizeof(float4));
+    d.xl32 = fp64 ? reinterpret_cast<float4*>(xl) : d.xq32;
     d.fnx = reinterpret_cast<long long*>(at(NA * sizeof(long long)));
     d.fny = reinterpret_cast<long long*>(at(NA * sizeof(long long)));
     d.fnz = reinterpret_cast<long long*>(at(NA * sizeof(long long)));
