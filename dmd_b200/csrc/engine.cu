@@ -66,8 +66,14 @@ Batch::Batch(const dmdgpu_options& opt, long long budget) : opt_(opt), budget_(b
     device_ = opt.device;
     if (cudaSetDevice(device_) != cudaSuccess) throw std::runtime_error("cudaSetDevice failed");
     cudaDeviceGetAttribute(&n_sm_, cudaDevAttrMultiProcessorCount, device_);
-    if (cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaStreamCreateWithFlags(&body_stream_, cudaStreamNonBlocking) != cudaSuccess)
+    // The main stream (list rebuild, pair kernel: the critical path) has the
+    // higher priority; the bonded / PME chain on aux_stream_ fills what is left.
+    int prio_lo = 0, prio_hi = 0;
+    if (cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi) != cudaSuccess ||
+        cudaStreamCreateWithPriority(&stream_, cudaStreamNonBlocking, prio_hi) != cudaSuccess ||
+        cudaStreamCreateWithPriority(&aux_stream_, cudaStreamNonBlocking, prio_lo) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ev_fork_, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ev_join_, cudaEventDisableTiming) != cudaSuccess)
         throw std::runtime_error("cudaStreamCreate failed");
 }
 
@@ -76,7 +82,9 @@ Batch::~Batch() {
     free_device();
     if (flush_buf_) cudaFree(flush_buf_);
     for (cudaEvent_t e : ev_pool_) cudaEventDestroy(e);
-    if (body_stream_) cudaStreamDestroy(body_stream_);
+    if (ev_fork_) cudaEventDestroy(ev_fork_);
+    if (ev_join_) cudaEventDestroy(ev_join_);
+    if (aux_stream_) cudaStreamDestroy(aux_stream_);
     if (stream_) cudaStreamDestroy(stream_);
 }
 
@@ -536,7 +544,10 @@ int Batch::pack() {
         d.chunk_itile = A.alloc<int>(n_chunks);
         d.chunk_j = A.alloc<uint32_t>(n_chunks * 32);
         d.chunk_mask = A.alloc<uint32_t>(n_chunks * 32);
-        d.chunk_prefix = A.alloc<int>(R + 1);
+        d.chunk_prefix = A.alloc<int>(R + 3);
+        d.nb_work = d.chunk_prefix + R + 1;
+        d.build_work = d.chunk_prefix + R + 2;
+        d.grid_bar = A.alloc<unsigned>(2);
         // host-side staging
         std::vector<double> hm(n_atoms), hq(n_atoms), hx(n_atoms), hy(n_atoms), hz(n_atoms), hvx(n_atoms),
             hvy(n_atoms), hvz(n_atoms);
@@ -712,9 +723,11 @@ int Batch::pack() {
             if (fp64_) {
                 d.mesh_real = A.alloc<double>(mesh_real);
                 d.mesh_cplx = A.alloc<double2>(mesh_cplx);
+                d.pme_green = A.alloc<double>(mesh_cplx);
             } else {
                 d.mesh_real = A.alloc<float>(mesh_real);
                 d.mesh_cplx = A.alloc<float2>(mesh_cplx);
+                d.pme_green = A.alloc<float>(mesh_cplx);
             }
             double* dbsp = A.alloc<double>(bsp.size());
             up(dbsp, bsp.data(), 8 * bsp.size());
@@ -756,8 +769,8 @@ int Batch::pack() {
         if (cufftPlan3d(&f, K, K, K, fp64_ ? CUFFT_D2Z : CUFFT_R2C) != CUFFT_SUCCESS ||
             cufftPlan3d(&b, K, K, K, fp64_ ? CUFFT_Z2D : CUFFT_C2R) != CUFFT_SUCCESS)
             return fail(DMDGPU_ERR_GPU, "cufftPlan3d failed");
-        cufftSetStream(f, stream_);
-        cufftSetStream(b, stream_);
+        cufftSetStream(f, aux_stream_);
+        cufftSetStream(b, aux_stream_);
         plans_[K] = {f, b};
     }
     packed_ = true;
@@ -772,26 +785,23 @@ void Batch::enqueue_eval(int pass) {
     Dev& d = dev_;
     launch_eval_begin(d, pass, stream_, &launches_);
     if (pass != PASS_SECOND) launch_clear_forces(d, stream_, &launches_);
+    // The list rebuild (a cooperative launch: it needs the whole GPU) goes first;
+    // it returns at once on steps without a rebuild.
     enqueue_rebuild();
+    // Bonded terms and PME depend on atom positions only (not on the sorted slots),
+    // so they run on aux_stream_ concurrently with the pair kernel; all force and
+    // energy sums are fixed-point atomics (order-free).
+    cudaEventRecord(ev_fork_, stream_);
+    cudaStreamWaitEvent(aux_stream_, ev_fork_, 0);
     cudaEvent_t e0 = nullptr, e1 = nullptr;
-    if (prof_nb_) {
-        e0 = next_event();
-        record(e0);
-    }
-    launch_nonbonded(d, fp64_, phys_, n_sm_, stream_, &launches_);
-    if (prof_nb_) {
-        e1 = next_event();
-        record(e1);
-        prof_nb_->emplace_back(e0, e1);
-    }
-    launch_bonded(d, fp64_, phys_, stream_, &launches_);
+    launch_bonded(d, fp64_, phys_, aux_stream_, &launches_);
     if (any_pme_) {
         if (prof_pme_) {
             e0 = next_event();
-            record(e0);
+            record(e0, aux_stream_);
         }
-        launch_pme_spread(d, fp64_, stream_, &launches_);
-        launch_pme_convert(d, fp64_, n_fix_total_, stream_, &launches_);
+        launch_pme_spread(d, fp64_, aux_stream_, &launches_);
+        launch_pme_convert(d, fp64_, n_fix_total_, aux_stream_, &launches_);
         for (int k : order_) {
             const Rep& P = reps_[k]->rep;
             if (!(P.flags & F_PME)) continue;
@@ -804,7 +814,7 @@ void Batch::enqueue_eval(int pass) {
                              static_cast<cufftComplex*>(d.mesh_cplx) + P.mesh_cplx_off);
             }
         }
-        launch_pme_influence(d, fp64_, n_pme_blocks_, stream_, &launches_);
+        launch_pme_influence(d, fp64_, n_pme_blocks_, aux_stream_, &launches_);
         for (int k : order_) {
             const Rep& P = reps_[k]->rep;
             if (!(P.flags & F_PME)) continue;
@@ -817,62 +827,31 @@ void Batch::enqueue_eval(int pass) {
                              static_cast<float*>(d.mesh_real) + P.mesh_real_off);
             }
         }
-        launch_pme_gather(d, fp64_, stream_, &launches_);
+        launch_pme_gather(d, fp64_, aux_stream_, &launches_);
         if (prof_pme_) {
             e1 = next_event();
-            record(e1);
+            record(e1, aux_stream_);
             prof_pme_->emplace_back(e0, e1);
         }
     }
+    cudaEventRecord(ev_join_, aux_stream_);
+    if (prof_nb_) {
+        e0 = next_event();
+        record(e0, stream_);
+    }
+    launch_nonbonded(d, fp64_, phys_, n_sm_, stream_, &launches_);
+    if (prof_nb_) {
+        e1 = next_event();
+        record(e1, stream_);
+        prof_nb_->emplace_back(e0, e1);
+    }
+    cudaStreamWaitEvent(stream_, ev_join_, 0);
     launch_eval_end(d, stream_, &launches_);
 }
 
-// Neighbour-list rebuild.  Eagerly every kernel is launched and the ones of
-// replicas without a pending rebuild return at once; inside a captured graph
-// the body sits in an IF conditional node that the flag kernel switches on only
-// when some replica rebuilds, so a step without a rebuild costs one launch.
-void Batch::enqueue_rebuild() {
-    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
-    cudaStreamIsCapturing(stream_, &cs);
-    if (cs != cudaStreamCaptureStatusActive) {
-        launch_rebuild_flag(dev_, cudaGraphConditionalHandle{}, false, stream_, &launches_);
-        launch_rebuild_body(dev_, d_bin_rep_, false, stream_, &launches_);
-        return;
-    }
-    cudaGraph_t g = nullptr;
-    const cudaGraphNode_t* deps = nullptr;
-    size_t ndeps = 0;
-    cudaStreamGetCaptureInfo(stream_, &cs, nullptr, &g, nullptr, nullptr);
-    cudaGraphConditionalHandle h;
-    if (cudaGraphConditionalHandleCreate(&h, g, 0, 0) != cudaSuccess) {
-        capture_error_ = true;
-        return;
-    }
-    launch_rebuild_flag(dev_, h, true, stream_, &launches_);
-    cudaStreamGetCaptureInfo(stream_, &cs, nullptr, &g, &deps, &ndeps);
-    cudaGraphNodeParams cp = {};
-    cp.type = cudaGraphNodeTypeConditional;
-    cp.conditional.handle = h;
-    cp.conditional.type = cudaGraphCondTypeIf;
-    cp.conditional.size = 1;
-    cudaGraphNode_t node;
-    if (cudaGraphAddNode(&node, g, deps, ndeps, &cp) != cudaSuccess) {
-        capture_error_ = true;
-        return;
-    }
-    cudaGraph_t body = cp.conditional.phGraph_out[0];
-    if (cudaStreamBeginCaptureToGraph(body_stream_, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed) !=
-        cudaSuccess) {
-        capture_error_ = true;
-        return;
-    }
-    // counted when they actually run (from the device's list-build counter)
-    long long body_count = 0;
-    launch_rebuild_body(dev_, d_bin_rep_, true, body_stream_, &body_count);
-    cudaGraph_t out = nullptr;
-    if (cudaStreamEndCapture(body_stream_, &out) != cudaSuccess) capture_error_ = true;
-    cudaStreamUpdateCaptureDependencies(stream_, &node, 1, cudaStreamSetCaptureDependencies);
-}
+// Neighbour-list rebuild: one cooperative launch that returns at once unless
+// some replica's rebuild flag is set.
+void Batch::enqueue_rebuild() { launch_rebuild(dev_, d_bin_rep_, n_sm_, stream_, &launches_); }
 
 void Batch::enqueue_step() {
     launch_step_begin(dev_, stream_, &launches_);
@@ -980,14 +959,11 @@ int Batch::sync_status() {
     CK(cudaMemcpyAsync(h_st_, d_st_, sizeof(RepState) * order_.size(), cudaMemcpyDeviceToHost, stream_));
     CK(cudaStreamSynchronize(stream_));
     int rc = DMDGPU_OK;
-    // rebuild bodies inside graph conditional nodes: 7 kernels per executed body
-    const long long runs = h_st_[0].body_runs;
-    if (runs > body_runs_seen_) launches_ += 7 * (runs - body_runs_seen_);
-    body_runs_seen_ = runs;
     for (size_t k = 0; k < order_.size(); ++k) {
         HostRep& h = *reps_[order_[k]];
         const int st = h_st_[k].status;
-        if (st & ST_NAN) rc = fail(DMDGPU_ERR_NAN, "non-finite force or energy on device");
+        if (st & ST_TIMEOUT) rc = fail(DMDGPU_ERR_GPU, "list-build grid barrier timed out");
+        else if (st & ST_NAN) rc = fail(DMDGPU_ERR_NAN, "non-finite force or energy on device");
         else if (st & ST_RANGE) rc = fail(DMDGPU_ERR_BOND_EXPLOSION, "force outside the fixed-point range");
         else if (st & ST_CAPACITY) rc = fail(DMDGPU_ERR_CAPACITY, "pair list capacity exceeded");
         if (!h.done && h.target > 0 && h_st_[k].step >= h.target) {
@@ -1039,11 +1015,11 @@ int Batch::extend_targets(long long n) {
 
 // Event record usable for timing inside a captured graph: an external event
 // node (a plain record during capture only becomes a graph dependency).
-void Batch::record(cudaEvent_t e) {
+void Batch::record(cudaEvent_t e, cudaStream_t st) {
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
-    cudaStreamIsCapturing(stream_, &cs);
-    if (cs == cudaStreamCaptureStatusActive) cudaEventRecordWithFlags(e, stream_, cudaEventRecordExternal);
-    else cudaEventRecord(e, stream_);
+    cudaStreamIsCapturing(st, &cs);
+    if (cs == cudaStreamCaptureStatusActive) cudaEventRecordWithFlags(e, st, cudaEventRecordExternal);
+    else cudaEventRecord(e, st);
 }
 
 // n steps as one captured graph with timing events around every step and every
@@ -1088,9 +1064,9 @@ int Batch::step_timed(int n, long long flush_bytes, dmdgpu_timing* out) {
         for (int i = 0; i < n; ++i) {
             if (flush_buf_) cudaMemsetAsync(flush_buf_, i & 0xff, flush_bytes_, stream_);
             cudaEvent_t a = next_event(), b = next_event();
-            record(a);
+            record(a, stream_);
             enqueue_step();
-            record(b);
+            record(b, stream_);
             steps.emplace_back(a, b);
         }
         e = cudaStreamEndCapture(stream_, &g);
@@ -1104,7 +1080,6 @@ int Batch::step_timed(int n, long long flush_bytes, dmdgpu_timing* out) {
     const long long captured = launches_ - before;
     CK(cudaGraphInstantiate(&ge, g, 0));
     cudaGraphDestroy(g);
-    const long long runs0 = body_runs_seen_;
     CK(cudaGraphLaunch(ge, stream_));
     CK(cudaStreamSynchronize(stream_));
     cudaGraphExecDestroy(ge);
@@ -1122,8 +1097,8 @@ int Batch::step_timed(int n, long long flush_bytes, dmdgpu_timing* out) {
         out->pme_ms += ms;
     }
     out->nonbonded_launches = static_cast<long long>(nb.size());
-    int rc = sync_status();  // adds the rebuild bodies that executed
-    out->kernel_launches = captured + 7 * (body_runs_seen_ - runs0);
+    int rc = sync_status();
+    out->kernel_launches = captured;
     return rc;
 }
 

@@ -115,7 +115,10 @@ class Batch {
     long long budget_;
     bool fp64_, phys_;
     int device_ = 0, n_sm_ = 148;
-    cudaStream_t stream_ = nullptr, body_stream_ = nullptr;
+    cudaStream_t stream_ = nullptr;
+    // bonded + PME run on aux_stream_, forked from and joined back to stream_
+    cudaStream_t aux_stream_ = nullptr;
+    cudaEvent_t ev_fork_ = nullptr, ev_join_ = nullptr;
     bool capture_error_ = false;
     std::vector<std::unique_ptr<HostRep>> reps_;   // indexed by slot (nullptr = free)
     std::vector<int> order_;                        // packed replica index -> slot
@@ -136,7 +139,6 @@ class Batch {
     bool need_eval1_ = true;
     long long launches_ = 0;
     long long per_step_launches_ = 0;
-    long long body_runs_seen_ = 0;
     long long used_bytes_ = 0;
     // per-kernel timing (step_profiled): event pairs recorded around launches
     std::vector<cudaEvent_t> ev_pool_;
@@ -145,7 +147,7 @@ class Batch {
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>>* prof_pme_ = nullptr;
     void* flush_buf_ = nullptr;
     long long flush_bytes_ = 0;
-    void record(cudaEvent_t e);
+    void record(cudaEvent_t e, cudaStream_t st);
     cudaEvent_t next_event();
     std::string err_;
     std::vector<int> finished_;

@@ -249,16 +249,24 @@ __device__ __forceinline__ void do_exclusion(const Dev& d, int n) {
 
 // Fractional mesh coordinate as in spread_charges (coulomb_pme.cpp:93-112): the
 // position is divided by L, wrapped with floor, scaled by K; FP64.
-__device__ __forceinline__ void mesh_coord(double x, double L, int K, int& m0, double& u) {
-    double f = x / L;
+__device__ __forceinline__ int wrap_mesh(int g, int K) {
+    g += (g < 0) ? K : 0;
+    return g - ((g >= K) ? K : 0);
+}
+
+__device__ __forceinline__ void mesh_coord(double x, double invL, int K, int& m0, double& u) {
+    double f = x * invL;
     f -= floor(f);
     u = f * K;
     m0 = static_cast<int>(floor(u)) - 1;
 }
 
+// 16 threads per atom: thread (iz, iy) = (sub >> 2, sub & 3) adds the atom's
+// 4 mesh points along x of one (y, z) row of its 4x4x4 stencil.
 template <typename T>
 __global__ void k_pme_spread(Dev d) {
-    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    const long long t = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const int a = static_cast<int>(t >> 4);
     if (a >= d.n_atoms) return;
     const int r = d.atom_rep[a];
     RepState* s = d.st + r;
@@ -267,33 +275,29 @@ __global__ void k_pme_spread(Dev d) {
     const double q = d.q[a];
     if (q == 0.0) return;
     const int K = R.pme_K;
-    const double L = s->L;
+    const int iz = (threadIdx.x >> 2) & 3, iy = threadIdx.x & 3;
     int m0[3];
     double u[3];
-    mesh_coord(d.x[a], L, K, m0[0], u[0]);
-    mesh_coord(d.y[a], L, K, m0[1], u[1]);
-    mesh_coord(d.z[a], L, K, m0[2], u[2]);
-    T w[3][4];
-    for (int k = 0; k < 3; ++k)
-        for (int j = 0; j < 4; ++j) w[k][j] = theta4<T>((T)(u[k] - (m0[k] + j)));
+    mesh_coord(d.x[a], s->invL, K, m0[0], u[0]);
+    mesh_coord(d.y[a], s->invL, K, m0[1], u[1]);
+    mesh_coord(d.z[a], s->invL, K, m0[2], u[2]);
+    T wx[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) wx[j] = theta4<T>((T)(u[0] - (m0[0] + j)));
+    const T wy = theta4<T>((T)(u[1] - (m0[1] + iy)));
+    const T wz = theta4<T>((T)(u[2] - (m0[2] + iz)));
     long long* mesh = d.mesh_fix + R.mesh_fix_off;
     const T qt = (T)q;
-    for (int iz = 0; iz < 4; ++iz) {
-        int gz = (m0[2] + iz) % K;
-        if (gz < 0) gz += K;
-        for (int iy = 0; iy < 4; ++iy) {
-            int gy = (m0[1] + iy) % K;
-            if (gy < 0) gy += K;
-            const T wyz = w[1][iy] * w[2][iz];
-            for (int ix = 0; ix < 4; ++ix) {
-                int gx = (m0[0] + ix) % K;
-                if (gx < 0) gx += K;
-                // grid_[gz*ny*nx + gy*nx + gx] (coulomb_pme.cpp:131); the REF buffer is
-                // K*K*2(K/2+1) long, the PHYS one K^3: the index is the same.
-                const long long idx = (static_cast<long long>(gz) * K + gy) * K + gx;
-                fix_add(mesh + idx, __double2ll_rn(static_cast<double>(qt * w[0][ix] * wyz) * MSCALE));
-            }
-        }
+    // m0 + j lies in [-1, K + 2]: one conditional wrap per index
+    const int gz = wrap_mesh(m0[2] + iz, K), gy = wrap_mesh(m0[1] + iy, K);
+    const T wyz = wy * wz;
+    // grid_[gz*ny*nx + gy*nx + gx] (coulomb_pme.cpp:131); the REF buffer is
+    // K*K*2(K/2+1) long, the PHYS one K^3: the index is the same.
+    const long long row = (static_cast<long long>(gz) * K + gy) * K;
+#pragma unroll
+    for (int ix = 0; ix < 4; ++ix) {
+        const int gx = wrap_mesh(m0[0] + ix, K);
+        fix_add(mesh + row + gx, __double2ll_rn(static_cast<double>(qt * wx[ix] * wyz) * MSCALE));
     }
 }
 
@@ -317,32 +321,42 @@ __global__ void k_pme_convert(Dev d, long long n_fix) {
     if (!d.st[r].eval) return;
     const int loc = static_cast<int>(e - R.mesh_fix_off);  // meshes are < 2^31 points
     const int K = R.pme_K;
-    const int pitch = (R.flags & F_PHYS) ? K : 2 * (K / 2 + 1);
-    const int row = loc / pitch;
-    const int col = loc - row * pitch;
     const long long v = d.mesh_fix[e];
     d.mesh_fix[e] = 0;
-    if (col < K) {
-        T* real = reinterpret_cast<T*>(d.mesh_real) + R.mesh_real_off;
-        real[static_cast<long long>(row) * K + col] = static_cast<T>(static_cast<double>(v) * (1.0 / MSCALE));
+    T* real = reinterpret_cast<T*>(d.mesh_real) + R.mesh_real_off;
+    const T val = static_cast<T>(static_cast<double>(v) * (1.0 / MSCALE));
+    if (R.flags & F_PHYS) {
+        real[loc] = val;  // natural layout, same index
+    } else {
+        const int pitch = 2 * (K / 2 + 1);
+        const int row = loc / pitch;
+        const int col = loc - row * pitch;
+        if (col < K) real[static_cast<long long>(row) * K + col] = val;
     }
 }
 
 // Green's function multiply and reciprocal energy/virial
 // (compute_reciprocal_energy_and_potential, coulomb_pme.cpp:143-201).
+// The influence function G depends only on the box, alpha and K: it is cached
+// (rounded to T) and recomputed only when the box edge changed (barostat, state
+// load).  Energy and virial sums are formed only when this evaluation's
+// energies are read.
 template <typename T>
 __global__ void k_pme_influence(Dev d) {
     const int r = d.pme_block_rep[blockIdx.x];
     const Rep& R = d.rep[r];
     RepState* s = d.st + r;
+    if (!s->eval) return;  // uniform over the block
     const int lb = blockIdx.x - R.pme_block_begin;
     const int K = R.pme_K, H = K / 2 + 1;
     const int nc = K * K * H;
     const int e = lb * static_cast<int>(blockDim.x) + static_cast<int>(threadIdx.x);
+    const bool want_e = s->want_e != 0;
     double en = 0.0, vr = 0.0;
-    if (s->eval && e < nc) {
+    if (e < nc) {
         using C2 = typename std::conditional<sizeof(T) == 8, double2, float2>::type;
         C2* cm = reinterpret_cast<C2*>(d.mesh_cplx) + R.mesh_cplx_off;
+        T* gc = reinterpret_cast<T*>(d.pme_green) + R.mesh_cplx_off;
         const int kx = e % H;
         const int ky = (e / H) % K;
         const int kz = e / (H * K);
@@ -351,22 +365,35 @@ __global__ void k_pme_influence(Dev d) {
             if (R.flags & F_PHYS) cm[e] = C2{0, 0};
         } else {
             const double L = s->L;
-            const double w = (kx == 0 || (K % 2 == 0 && kx == K / 2)) ? 1.0 : 2.0;
-            const double msq = (static_cast<double>(mx) * mx) / (L * L) + (static_cast<double>(my) * my) / (L * L) +
-                               (static_cast<double>(mz) * mz) / (L * L);
-            const double k2 = 4.0 * PI * PI * msq;
-            const double V = L * (L * L);
-            const double* b = d.bsp + R.bsp_off;
-            const double B = b[kx] * b[ky] * b[kz];
-            const double green = 4.0 * PI * KE / V * exp(-k2 / (4.0 * R.alpha * R.alpha)) * B / k2;
+            double k2 = 0.0;
+            if (!s->green_ok || want_e) {
+                const double msq = (static_cast<double>(mx) * mx) / (L * L) +
+                                   (static_cast<double>(my) * my) / (L * L) +
+                                   (static_cast<double>(mz) * mz) / (L * L);
+                k2 = 4.0 * PI * PI * msq;
+            }
+            T green;
+            if (s->green_ok) {
+                green = gc[e];
+            } else {
+                const double V = L * (L * L);
+                const double* b = d.bsp + R.bsp_off;
+                const double B = b[kx] * b[ky] * b[kz];
+                green = static_cast<T>(4.0 * PI * KE / V * exp(-k2 / (4.0 * R.alpha * R.alpha)) * B / k2);
+                gc[e] = green;
+            }
             const C2 z = cm[e];
-            const double re = z.x, im = z.y;
-            const double ek = 0.5 * w * green * (re * re + im * im);
-            en = ek;
-            vr = ek * (1.0 - k2 / (2.0 * R.alpha * R.alpha));
-            cm[e] = C2{static_cast<T>(re * green), static_cast<T>(im * green)};
+            if (want_e) {
+                const double w = (kx == 0 || (K % 2 == 0 && kx == K / 2)) ? 1.0 : 2.0;
+                const double re = z.x, im = z.y;
+                const double ek = 0.5 * w * static_cast<double>(green) * (re * re + im * im);
+                en = ek;
+                vr = ek * (1.0 - k2 / (2.0 * R.alpha * R.alpha));
+            }
+            cm[e] = C2{z.x * green, z.y * green};
         }
     }
+    if (!want_e) return;  // uniform over the block
     // deterministic block reduction (fixed tree)
     __shared__ double se[256], sv[256];
     se[threadIdx.x] = en;
@@ -388,9 +415,13 @@ __global__ void k_pme_influence(Dev d) {
 // interpolate_forces (coulomb_pme.cpp:205-283).  REF reads the potential with
 // the unpadded index from FFTW's padded buffer (padding reads as zero) and
 // scales it by 1/N (:303-306); PHYS reads the natural layout, unscaled.
+// 16 threads per atom as in the spread: each sums its row of 4 points, then the
+// group of 16 lanes reduces in a fixed butterfly order.
 template <typename T>
 __global__ void k_pme_gather(Dev d) {
-    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    const long long t = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const int a = static_cast<int>(t >> 4);
+    // every condition below is uniform over the atom's 16 lanes
     if (a >= d.n_atoms) return;
     const int r = d.atom_rep[a];
     RepState* s = d.st + r;
@@ -402,48 +433,53 @@ __global__ void k_pme_gather(Dev d) {
     const bool phys = (R.flags & F_PHYS) != 0;
     const int P = 2 * (K / 2 + 1);
     const double norm = 1.0 / (static_cast<double>(K) * K * K);
-    const double L = s->L;
+    const int iz = (threadIdx.x >> 2) & 3, iy = threadIdx.x & 3;
     int m0[3];
     double u[3];
-    mesh_coord(d.x[a], L, K, m0[0], u[0]);
-    mesh_coord(d.y[a], L, K, m0[1], u[1]);
-    mesh_coord(d.z[a], L, K, m0[2], u[2]);
-    T w[3][4], dw[3][4];
-    for (int k = 0; k < 3; ++k)
-        for (int j = 0; j < 4; ++j) {
-            const T t = (T)(u[k] - (m0[k] + j));
-            w[k][j] = theta4<T>(t);
-            dw[k][j] = dtheta4<T>(t);
-        }
-    const T* real = reinterpret_cast<const T*>(d.mesh_real) + R.mesh_real_off;
-    T gx = 0, gy = 0, gz = 0;
-    for (int iz = 0; iz < 4; ++iz) {
-        int z = (m0[2] + iz) % K;
-        if (z < 0) z += K;
-        for (int iy = 0; iy < 4; ++iy) {
-            int y = (m0[1] + iy) % K;
-            if (y < 0) y += K;
-            for (int ix = 0; ix < 4; ++ix) {
-                int x = (m0[0] + ix) % K;
-                if (x < 0) x += K;
-                const int lin = (z * K + y) * K + x;
-                T phi;
-                if (phys) {
-                    phi = real[lin];
-                } else {
-                    const int row = lin / P;
-                    const int col = lin - row * P;
-                    phi = (col < K) ? (T)(static_cast<double>(real[row * K + col]) * norm) : T(0);
-                }
-                gx += phi * dw[0][ix] * w[1][iy] * w[2][iz];
-                gy += phi * w[0][ix] * dw[1][iy] * w[2][iz];
-                gz += phi * w[0][ix] * w[1][iy] * dw[2][iz];
-            }
-        }
+    mesh_coord(d.x[a], s->invL, K, m0[0], u[0]);
+    mesh_coord(d.y[a], s->invL, K, m0[1], u[1]);
+    mesh_coord(d.z[a], s->invL, K, m0[2], u[2]);
+    T wx[4], dwx[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const T tx = (T)(u[0] - (m0[0] + j));
+        wx[j] = theta4<T>(tx);
+        dwx[j] = dtheta4<T>(tx);
     }
-    const T fac = (T)(static_cast<double>(K) / L);
-    const T qt = (T)q;
-    add_force(d, a, -qt * fac * gx, -qt * fac * gy, -qt * fac * gz, s);
+    const T ty = (T)(u[1] - (m0[1] + iy)), tz = (T)(u[2] - (m0[2] + iz));
+    const T wy = theta4<T>(ty), dwy = dtheta4<T>(ty);
+    const T wz = theta4<T>(tz), dwz = dtheta4<T>(tz);
+    const T* real = reinterpret_cast<const T*>(d.mesh_real) + R.mesh_real_off;
+    const int z = wrap_mesh(m0[2] + iz, K), y = wrap_mesh(m0[1] + iy, K);
+    T sd = 0, sw = 0;  // the row's sums of phi * dtheta_x and phi * theta_x
+#pragma unroll
+    for (int ix = 0; ix < 4; ++ix) {
+        const int x = wrap_mesh(m0[0] + ix, K);
+        const int lin = (z * K + y) * K + x;
+        T phi;
+        if (phys) {
+            phi = real[lin];
+        } else {
+            const int row = lin / P;
+            const int col = lin - row * P;
+            phi = (col < K) ? (T)(static_cast<double>(real[row * K + col]) * norm) : T(0);
+        }
+        sd += phi * dwx[ix];
+        sw += phi * wx[ix];
+    }
+    T gx = sd * wy * wz, gy = sw * dwy * wz, gz = sw * wy * dwz;
+    const unsigned grp = 0xFFFFu << (threadIdx.x & 16);
+#pragma unroll
+    for (int o = 8; o > 0; o >>= 1) {
+        gx += __shfl_xor_sync(grp, gx, o);
+        gy += __shfl_xor_sync(grp, gy, o);
+        gz += __shfl_xor_sync(grp, gz, o);
+    }
+    if ((threadIdx.x & 15) == 0) {
+        const T fac = (T)(static_cast<double>(K) * s->invL);
+        const T qt = (T)q;
+        add_force(d, a, -qt * fac * gx, -qt * fac * gy, -qt * fac * gz, s);
+    }
 }
 
 // One launch for every bonded-type term: blocks [0, nb) bonds, then angles,
@@ -479,7 +515,7 @@ void launch_bonded(const Dev& d, bool fp64, bool phys, cudaStream_t st, long lon
 }
 
 void launch_pme_spread(const Dev& d, bool fp64, cudaStream_t st, long long* nlaunch) {
-    const int T = 128, g = (d.n_atoms + T - 1) / T;
+    const int T = 256, g = static_cast<int>((16LL * d.n_atoms + T - 1) / T);
     if (fp64) k_pme_spread<double><<<g, T, 0, st>>>(d);
     else k_pme_spread<float><<<g, T, 0, st>>>(d);
     ++*nlaunch;
@@ -501,7 +537,7 @@ void launch_pme_influence(const Dev& d, bool fp64, int n_blocks, cudaStream_t st
 }
 
 void launch_pme_gather(const Dev& d, bool fp64, cudaStream_t st, long long* nlaunch) {
-    const int T = 128, g = (d.n_atoms + T - 1) / T;
+    const int T = 256, g = static_cast<int>((16LL * d.n_atoms + T - 1) / T);
     if (fp64) k_pme_gather<double><<<g, T, 0, st>>>(d);
     else k_pme_gather<float><<<g, T, 0, st>>>(d);
     ++*nlaunch;

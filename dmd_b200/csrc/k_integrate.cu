@@ -33,6 +33,10 @@ __global__ void k_step_begin(Dev d) {
 
 __global__ void k_eval_begin(Dev d, int pass) {
     int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r == 0) {
+        *d.nb_work = 0;
+        d.grid_bar[0] = 0;  // arrivals (the generation word keeps counting)
+    }
     if (r >= d.n_rep) return;
     RepState* s = d.st + r;
     const Rep& R = d.rep[r];
@@ -49,6 +53,7 @@ __global__ void k_eval_begin(Dev d, int pass) {
         ev = 1;
     }
     s->eval = ev;
+    s->green_ok = (s->green_L == s->L) ? 1 : 0;
     // Pair energies and the pair virial are needed by single-point evaluations,
     // by the evaluation that ends a run (its energies are what the host reads) and,
     // with the PHYS barostat, every step (its pressure uses the atomic virial).
@@ -71,6 +76,7 @@ __global__ void k_eval_end(Dev d) {
     if (!s->eval) return;
     if (!(R.flags & F_PHYS) && (R.flags & F_LJ)) s->lj_counter += 1;
     s->have_forces = 1;
+    if (R.flags & F_PME) s->green_L = s->L;  // the influence kernel has filled the cache
 }
 
 __global__ void k_clear_forces(Dev d) {

@@ -17,9 +17,7 @@
 namespace dmd {
 
 // R1: voxel of every atom (wrapped coordinates), frozen periodic image.
-__global__ void k_bin_atoms(Dev d) {
-    int a = blockIdx.x * blockDim.x + threadIdx.x;
-    if (a >= d.n_atoms) return;
+__device__ __forceinline__ void bin_atom(const Dev& d, int a) {
     int r = d.atom_rep[a];
     RepState* s = d.st + r;
     if (!s->rebuild) return;
@@ -44,37 +42,39 @@ __global__ void k_bin_atoms(Dev d) {
     atomicAdd(d.bin_count + bin, 1);
 }
 
-// R2: exclusive scan of bin counts per replica (one block per replica).
-__global__ void k_bin_scan(Dev d) {
-    int r = blockIdx.x;
-    if (!d.st[r].rebuild) return;
+// R2: exclusive scan of one replica's bin counts by one block (NT_B threads):
+// contiguous bin ranges per thread, warp-shuffle scan of the thread sums.
+constexpr int NT_R = 128;
+__device__ __forceinline__ void bin_scan_replica(const Dev& d, int r) {
+    __shared__ int s_warp[NT_R / 32];
     const Rep& R = d.rep[r];
     const int nb = R.nvx * R.nvx * R.nvz;
-    const int per = (nb + blockDim.x - 1) / blockDim.x;
-    const int b0 = R.bin_begin + threadIdx.x * per;
+    const int per = (nb + NT_R - 1) / NT_R;
+    const int b0 = R.bin_begin + min(static_cast<int>(threadIdx.x) * per, nb);
     const int b1 = min(b0 + per, R.bin_begin + nb);
     int local = 0;
     for (int b = b0; b < b1; ++b) local += d.bin_count[b];
-    __shared__ int sh[1024];
-    sh[threadIdx.x] = local;
-    __syncthreads();
-    for (int o = 1; o < blockDim.x; o <<= 1) {
-        int v = (threadIdx.x >= o) ? sh[threadIdx.x - o] : 0;
-        __syncthreads();
-        sh[threadIdx.x] += v;
-        __syncthreads();
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int incl = local;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(FULL, incl, o);
+        if (lane >= o) incl += v;
     }
-    int run = sh[threadIdx.x] - local + 32 * R.tile_begin;
+    if (lane == 31) s_warp[w] = incl;
+    __syncthreads();
+    int off = 0;
+    for (int k = 0; k < w; ++k) off += s_warp[k];
+    int run = off + incl - local + 32 * R.tile_begin;
     for (int b = b0; b < b1; ++b) {
         d.bin_start[b] = run;
         run += d.bin_count[b];
     }
+    __syncthreads();
 }
 
 // R3: scatter atoms to their bin ranges (order within a bin fixed by R4).
-__global__ void k_bin_scatter(Dev d) {
-    int a = blockIdx.x * blockDim.x + threadIdx.x;
-    if (a >= d.n_atoms) return;
+__device__ __forceinline__ void bin_scatter_atom(const Dev& d, int a) {
     if (!d.st[d.atom_rep[a]].rebuild) return;
     int b = d.atom_bin[a];
     int pos = d.bin_start[b] + atomicAdd(d.bin_fill + b, 1);
@@ -85,10 +85,7 @@ __global__ void k_bin_scatter(Dev d) {
 // counters.  One warp per bin: every member's rank is the number of smaller
 // atom indices in the bin (indices are distinct), and it is written straight
 // to its slot in atom_of_slot.
-__global__ void k_bin_sort(Dev d, const int* bin_rep) {
-    const int lane = threadIdx.x & 31;
-    const int b = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    if (b >= d.n_bins) return;
+__device__ __forceinline__ void bin_sort_warp(const Dev& d, const int* bin_rep, int b, int lane) {
     if (!d.st[bin_rep[b]].rebuild) return;
     const int n = d.bin_count[b];
     const int* p = d.sort_buf + d.bin_start[b];
@@ -111,10 +108,7 @@ __global__ void k_bin_sort(Dev d, const int* bin_rep) {
 }
 
 // R5: tiles -- slot<->atom maps, reference positions, bounding boxes, mirror.
-__global__ void k_tiles(Dev d) {
-    const int lane = threadIdx.x & 31;
-    const int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    if (t >= d.n_tiles) return;
+__device__ __forceinline__ void tile_warp(const Dev& d, int t, int lane) {
     const int r = d.tile_rep[t];
     RepState* s = d.st + r;
     if (!s->rebuild) return;
@@ -194,11 +188,10 @@ __device__ __forceinline__ bool ref_member(const Dev& d, int ai, int aj, double 
     return r2_ref(ex, ey, ez) < rc2;
 }
 
-__global__ void __launch_bounds__(NT_B, 5) k_build_pairs(Dev d) {
+__device__ __forceinline__ void build_tile(const Dev& d, int I) {
     const int tid = threadIdx.x;
     const int lane = tid & 31;
     const int wib = tid >> 5;
-    const int I = blockIdx.x;
     __shared__ float s_lx[32], s_ly[32], s_lz[32];
     __shared__ int s_a[32];
     __shared__ uint32_t s_e[BW][64], s_m[BW][64];   // general path: per-warp entry buffers
@@ -212,7 +205,6 @@ __global__ void __launch_bounds__(NT_B, 5) k_build_pairs(Dev d) {
     __shared__ uint32_t s_carry_e[32], s_carry_m[32];
     __shared__ int s_wcnt[4][BW];
     __shared__ int s_jnext, s_c0;
-    if (I >= d.n_tiles) return;
     const int r = d.tile_rep[I];
     RepState* s = d.st + r;
     if (!s->rebuild) return;
@@ -613,9 +605,7 @@ __global__ void __launch_bounds__(NT_B, 5) k_build_pairs(Dev d) {
 }
 
 // R7: close the rebuild -- capacity check, counters, flat chunk numbering.
-__global__ void k_rebuild_finish(Dev d, int in_graph) {
-    if (threadIdx.x != 0) return;
-    if (in_graph) d.st[0].body_runs += 1;
+__device__ __forceinline__ void rebuild_finish(const Dev& d) {
     int run = 0;
     for (int r = 0; r < d.n_rep; ++r) {
         RepState* s = d.st + r;
@@ -634,39 +624,111 @@ __global__ void k_rebuild_finish(Dev d, int in_graph) {
     d.chunk_prefix[d.n_rep] = run;
 }
 
-// R0: reset chunk counters of replicas about to rebuild; when the step runs as
-// a CUDA graph, also set the IF-node condition that gates R1..R7.
-__global__ void k_rebuild_begin(Dev d, cudaGraphConditionalHandle cond, int use_cond) {
-    __shared__ int any;
-    if (threadIdx.x == 0) any = 0;
+__device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release(unsigned* p, unsigned v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Grid-wide barrier over the co-resident blocks of the cooperative launch:
+// bar[0] counts arrivals, bar[1] is the generation.  A wait gives up after one
+// second, records ST_TIMEOUT and returns false (the caller leaves the kernel).
+__device__ bool grid_barrier(const Dev& d) {
+    __shared__ int ok;
+    unsigned* bar = d.grid_bar;
     __syncthreads();
-    for (int r = threadIdx.x; r < d.n_rep; r += blockDim.x) {
-        if (d.st[r].rebuild) {
-            d.st[r].n_chunks = 0;
-            any = 1;
+    if (threadIdx.x == 0) {
+        ok = 1;
+        const unsigned gen = ld_acquire(bar + 1);
+        __threadfence();
+        if (atomicAdd(bar, 1u) == gridDim.x - 1) {
+            bar[0] = 0;
+            __threadfence();
+            st_release(bar + 1, gen + 1);
+        } else {
+            const unsigned long long t0 = global_ns();
+            while (ld_acquire(bar + 1) == gen) {
+                if (global_ns() - t0 > 1000000000ull) {
+                    atomicOr(&d.st[0].status, ST_TIMEOUT);
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(100);
+            }
         }
     }
     __syncthreads();
-    if (use_cond && threadIdx.x == 0) cudaGraphSetConditional(cond, any ? 1u : 0u);
+    return ok != 0;
 }
 
-void launch_rebuild_flag(const Dev& d, cudaGraphConditionalHandle cond, bool use_cond, cudaStream_t st,
-                         long long* nlaunch) {
-    k_rebuild_begin<<<1, 256, 0, st>>>(d, cond, use_cond ? 1 : 0);
+// The whole rebuild as one cooperative launch: R0 decides (all blocks read the
+// same flags, so a step without a rebuild leaves at once), then R1..R7 with a
+// grid barrier between phases.  Only replicas whose `rebuild` flag is set are
+// touched.
+__global__ void __launch_bounds__(NT_B, 4) k_rebuild(Dev d, const int* bin_rep) {
+    int any = 0;
+    for (int r = 0; r < d.n_rep; ++r) any |= d.st[r].rebuild;
+    if (!any) return;
+    const int tid = threadIdx.x, lane = tid & 31;
+    const int gthreads = gridDim.x * NT_B;
+    const int gtid = blockIdx.x * NT_B + tid;
+    const int gwarp = gtid >> 5, nwarps = gthreads >> 5;
+    // R0: chunk counters of the replicas that rebuild, work counter of R6
+    if (gtid == 0) *d.build_work = 0;
+    for (int r = gtid; r < d.n_rep; r += gthreads)
+        if (d.st[r].rebuild) d.st[r].n_chunks = 0;
+    for (int a = gtid; a < d.n_atoms; a += gthreads) bin_atom(d, a);
+    if (!grid_barrier(d)) return;
+    for (int r = blockIdx.x; r < d.n_rep; r += gridDim.x)
+        if (d.st[r].rebuild) bin_scan_replica(d, r);
+    if (!grid_barrier(d)) return;
+    for (int a = gtid; a < d.n_atoms; a += gthreads) bin_scatter_atom(d, a);
+    if (!grid_barrier(d)) return;
+    for (int b = gwarp; b < d.n_bins; b += nwarps) bin_sort_warp(d, bin_rep, b, lane);
+    if (!grid_barrier(d)) return;
+    for (int t = gwarp; t < d.n_tiles; t += nwarps) tile_warp(d, t, lane);
+    if (!grid_barrier(d)) return;
+    // R6: i-tiles taken one at a time from a counter (their costs differ)
+    __shared__ int s_tile;
+    for (;;) {
+        if (tid == 0) s_tile = atomicAdd(d.build_work, 1);
+        __syncthreads();
+        const int I = s_tile;
+        __syncthreads();
+        if (I >= d.n_tiles) break;
+        build_tile(d, I);
+    }
+    if (!grid_barrier(d)) return;
+    if (gtid == 0) rebuild_finish(d);
+}
+
+void launch_rebuild(const Dev& d, const int* bin_rep, int n_sm, cudaStream_t st, long long* nlaunch) {
+    static int per_sm = 0;  // co-resident blocks per SM (same on every device of one kind)
+    if (per_sm == 0) {
+        int n = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_rebuild, NT_B, 0);
+        per_sm = n < 1 ? 1 : (n > 4 ? 4 : n);
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(static_cast<unsigned>(n_sm * per_sm));
+    cfg.blockDim = dim3(NT_B);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, k_rebuild, d, bin_rep);
     *nlaunch += 1;
-}
-
-void launch_rebuild_body(const Dev& d, const int* bin_rep, bool in_graph, cudaStream_t st,
-                         long long* nlaunch) {
-    const int T = 256;
-    k_bin_atoms<<<(d.n_atoms + T - 1) / T, T, 0, st>>>(d);
-    k_bin_scan<<<d.n_rep, 1024, 0, st>>>(d);
-    k_bin_scatter<<<(d.n_atoms + T - 1) / T, T, 0, st>>>(d);
-    k_bin_sort<<<(d.n_bins + T / 32 - 1) / (T / 32), T, 0, st>>>(d, bin_rep);
-    k_tiles<<<(d.n_tiles * 32 + T - 1) / T, T, 0, st>>>(d);
-    k_build_pairs<<<d.n_tiles, NT_B, 0, st>>>(d);
-    k_rebuild_finish<<<1, 32, 0, st>>>(d, in_graph ? 1 : 0);
-    *nlaunch += 7;
 }
 
 }  // namespace dmd

@@ -279,11 +279,16 @@ __global__ void __launch_bounds__(256, 3) k_nb_f32(Dev d) {
         for (int k = threadIdx.x; k < d.n_lj; k += blockDim.x) s_lj[k] = d.lj32[k];
     __syncthreads();
     const float4* lj_tab = lj_shared ? s_lj : d.lj32;
-    const int nw = (gridDim.x * blockDim.x) >> 5;
     const int total = d.chunk_prefix[d.n_rep];
     Acc acc{0, 0, 0};
     int cur = -1;
-    for (int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < total; w += nw) {
+    // chunks are taken one per warp from a counter, so warps on SMs shared with
+    // the concurrent PME kernels simply take fewer
+    for (;;) {
+        int w = 0;
+        if (lane == 0) w = atomicAdd(d.nb_work, 1);
+        w = __shfl_sync(FULL, w, 0);
+        if (w >= total) break;
         const int r = chunk_replica(d.chunk_prefix, d.n_rep, w);
         if (r != cur) {
             flush_acc(d, cur, acc);
@@ -408,9 +413,10 @@ void launch_nonbonded(const Dev& d, bool fp64, bool phys, int n_sm, cudaStream_t
         if (phys) k_nb_f64<true><<<n_sm * 8, 256, 0, st>>>(d);
         else k_nb_f64<false><<<n_sm * 8, 256, 0, st>>>(d);
     } else {
-        // persistent: exactly the 4 resident blocks per SM its 64 registers allow
-        if (phys) k_nb_f32<true><<<n_sm * 3, 256, 0, st>>>(d);
-        else k_nb_f32<false><<<n_sm * 3, 256, 0, st>>>(d);
+        // persistent, 2 of the 3 blocks per SM its registers allow: the rest of
+        // the SM stays free for the bonded / PME kernels running alongside
+        if (phys) k_nb_f32<true><<<n_sm * 2, 256, 0, st>>>(d);
+        else k_nb_f32<false><<<n_sm * 2, 256, 0, st>>>(d);
     }
     *nlaunch += 1;
 }

@@ -7,13 +7,9 @@
 
 namespace dmd {
 
-// k_list.cu: rebuild pipeline for replicas whose `rebuild` flag is set.  The
-// flag kernel resets their list counters and (in a graph) sets `cond` to
-// whether any replica rebuilds; the body kernels are no-ops for the others.
-void launch_rebuild_flag(const Dev& d, cudaGraphConditionalHandle cond, bool use_cond, cudaStream_t st,
-                         long long* nlaunch);
-void launch_rebuild_body(const Dev& d, const int* bin_rep, bool in_graph, cudaStream_t st,
-                         long long* nlaunch);
+// k_list.cu: spatial sort + pair-list build for replicas whose `rebuild` flag
+// is set, as one cooperative launch (returns at once when no replica rebuilds).
+void launch_rebuild(const Dev& d, const int* bin_rep, int n_sm, cudaStream_t st, long long* nlaunch);
 
 // k_nonbonded.cu: LJ + real-space Ewald over the chunk list (replicas with `eval`).
 // Pair energies and virial are summed only for replicas whose `want_e` is set.

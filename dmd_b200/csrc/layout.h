@@ -37,7 +37,7 @@ enum RepFlags : int {
 };
 
 enum Status : int {
-    ST_NAN = 1, ST_RANGE = 2, ST_CAPACITY = 4, ST_LIST = 8,
+    ST_NAN = 1, ST_RANGE = 2, ST_CAPACITY = 4, ST_LIST = 8, ST_TIMEOUT = 16,
 };
 
 enum ETerm : int { E_LJ = 0, E_CREAL = 1, E_CRECIP = 2, E_CSELF = 3, E_CEXCL = 4, E_BOND = 5,
@@ -88,7 +88,6 @@ struct RepState {
     long long step, target_step;
     long long andersen_calls;
     long long list_builds;
-    long long body_runs;  // replica 0 only: graph-executed rebuild bodies
     int active;           // advances this step
     int eval;             // forces evaluated in the current evaluation pass
     int rebuild;          // neighbour list rebuild requested
@@ -97,6 +96,8 @@ struct RepState {
     int status;
     int n_chunks;
     int want_e;           // the current evaluation's pair energies / virial are read
+    int green_ok;         // the cached PME influence function matches the box
+    double green_L;       // box edge the cached influence function was made for
 };
 
 // Kernel view of the whole batch (passed by value).
@@ -137,6 +138,10 @@ struct Dev {
     int* chunk_itile;
     uint32_t *chunk_j, *chunk_mask;
     int* chunk_prefix;                 // [n_rep + 1] flat chunk numbering
+    void* pme_green;                   // cached PME influence function (mesh_cplx layout, T)
+    int* nb_work;                      // pair-kernel chunk counter (reset per evaluation)
+    int* build_work;                   // list-build i-tile counter (reset per rebuild)
+    unsigned* grid_bar;                // [2] rebuild grid barrier: arrivals, generation
     // bonded terms (global atom indices)
     int n_bonds, n_angles, n_dih;
     const int2* bond_ij;

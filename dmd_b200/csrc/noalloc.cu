@@ -168,6 +168,9 @@ extern "C" int dmdgpu_nonbonded_noalloc(const dmdgpu_nb_params* p, const double*
     Rep* d_rep = reinterpret_cast<Rep*>(at(sizeof(Rep)));
     RepState* d_st = reinterpret_cast<RepState*>(at(sizeof(RepState)));
     d.chunk_prefix = reinterpret_cast<int*>(at(8 * sizeof(int)));
+    d.nb_work = d.chunk_prefix + 4;  // zeroed with the prefix below
+    d.build_work = d.chunk_prefix + 5;
+    d.grid_bar = reinterpret_cast<unsigned*>(d.chunk_prefix + 6);  // [2]: words 6, 7
     d.rep = d_rep;
     d.st = d_st;
     d.x = const_cast<double*>(d_x);
@@ -310,10 +313,9 @@ extern "C" int dmdgpu_nonbonded_noalloc(const dmdgpu_nb_params* p, const double*
     if (!good) return DMDGPU_ERR_GPU;
     long long nl = 0;
     k_noalloc_types<<<(n + 255) / 256, 256, 0, st>>>(d_type, types, n, nt, d_st);
-    launch_rebuild_flag(d, cudaGraphConditionalHandle{}, false, st, &nl);
-    launch_rebuild_body(d, bin_rep, false, st, &nl);
     int n_sm = 148;
     cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+    launch_rebuild(d, bin_rep, n_sm, st, &nl);
     launch_nonbonded(d, fp64, phys, n_sm, st, &nl);
     k_noalloc_out<<<(n + 255) / 256, 256, 0, st>>>(d, d_fx, d_fy, d_fz, d_energies);
     if (cudaGetLastError() != cudaSuccess) return DMDGPU_ERR_GPU;
