@@ -34,6 +34,8 @@
 #include <unordered_set>
 #include <vector>
 
+#include "fft.h"
+
 namespace {
 
 constexpr double KB = 0.008314462618;   // src/core/constants.h:6
@@ -118,161 +120,17 @@ void pairs_within(int n, const double* x, const double* y, const double* z, doub
     }
 }
 
-// ---- FFT (self-written mixed radix, any length) ----------------------------
-using cd = std::complex<double>;
-
-void factorize(int n, std::vector<int>& f) {
-    f.clear();
-    for (int p : {4, 2, 3, 5}) {
-        while (n % p == 0) {
-            f.push_back(p);
-            n /= p;
-        }
-    }
-    for (int p = 7; n > 1; p += 2) {
-        while (n % p == 0) {
-            f.push_back(p);
-            n /= p;
-        }
-    }
-}
-
-// Decimation in time: X[k + q m] = sum_r W_n^{r(k+qm)} Y_r[k], Y_r = DFT_m(x[r::p]).
-// One plan per length: factors and a table of the N-th roots of unity (twiddles
-// of every sub-length n | N are W_n^e = W_N^{e N/n}); one scratch buffer.
-struct FFTPlan {
-    int n = 0;
-    std::vector<int> f;
-    std::vector<cd> w;        // exp(-2 pi i k / n)
-    std::vector<cd> scratch, tmp;
-};
-
-FFTPlan& plan_for(int n) {
-    static thread_local std::vector<FFTPlan> plans;
-    for (auto& p : plans)
-        if (p.n == n) return p;
-    FFTPlan p;
-    p.n = n;
-    factorize(n, p.f);
-    p.w.resize(n);
-    for (int k = 0; k < n; ++k) {
-        double a = -2.0 * PI * static_cast<double>(k) / n;
-        p.w[k] = cd(std::cos(a), std::sin(a));
-    }
-    p.scratch.resize(n);
-    p.tmp.resize(n);
-    plans.push_back(std::move(p));
-    return plans.back();
-}
-
-void fft_rec(const cd* in, int is, cd* out, int n, int level, FFTPlan& P, bool inv) {
-    if (n == 1) {
-        out[0] = in[0];
-        return;
-    }
-    const int p = P.f[level], m = n / p;
-    for (int r = 0; r < p; ++r) fft_rec(in + r * is, is * p, out + r * m, m, level + 1, P, inv);
-    const int N = P.n, step = N / n;
-    cd* res = P.scratch.data();
-    cd t[64];
-    std::vector<cd> big;
-    cd* tt = t;
-    if (p > 64) {
-        big.resize(p);
-        tt = big.data();
-    }
-    for (int k = 0; k < m; ++k) {
-        for (int r = 0; r < p; ++r) {
-            cd wv = P.w[(static_cast<long>(r) * k % n) * step];
-            if (inv) wv = std::conj(wv);
-            tt[r] = out[r * m + k] * wv;
-        }
-        for (int q = 0; q < p; ++q) {
-            cd acc = 0;
-            for (int r = 0; r < p; ++r) {
-                cd wv = P.w[(static_cast<long>(r) * q % p) * (N / p)];
-                if (inv) wv = std::conj(wv);
-                acc += tt[r] * wv;
-            }
-            res[k + q * m] = acc;
-        }
-    }
-    std::copy(res, res + n, out);
-}
-
-void fft1d(cd* a, int n, int sign) {
-    FFTPlan& P = plan_for(n);
-    std::copy(a, a + n, P.tmp.begin());
-    fft_rec(P.tmp.data(), 1, a, n, 0, P, sign > 0);
-}
-
-// 3-D complex transform in place over a K*K*K array, index (z*K + y)*K + x.
-void fft3d(std::vector<cd>& a, int K, int sign) {
-    std::vector<cd> line(K);
-    for (int z = 0; z < K; ++z)
-        for (int y = 0; y < K; ++y) fft1d(&a[(static_cast<size_t>(z) * K + y) * K], K, sign);
-    for (int z = 0; z < K; ++z)
-        for (int x = 0; x < K; ++x) {
-            for (int y = 0; y < K; ++y) line[y] = a[(static_cast<size_t>(z) * K + y) * K + x];
-            fft1d(line.data(), K, sign);
-            for (int y = 0; y < K; ++y) a[(static_cast<size_t>(z) * K + y) * K + x] = line[y];
-        }
-    for (int y = 0; y < K; ++y)
-        for (int x = 0; x < K; ++x) {
-            for (int z = 0; z < K; ++z) line[z] = a[(static_cast<size_t>(z) * K + y) * K + x];
-            fft1d(line.data(), K, sign);
-            for (int z = 0; z < K; ++z) a[(static_cast<size_t>(z) * K + y) * K + x] = line[z];
-        }
-}
-
-// FFTW-style in-place r2c on a padded buffer: real row (z,y) at buf[(z*K+y)*P + x],
-// x < K, P = 2(K/2+1); complex output (K/2+1 per row) written over the buffer.
+// ---- FFT (fft.h: the same transform the FFTW-API shim gives the reference) --
+// FFTW-style in-place r2c on a padded K^3 buffer: real row (z,y) at
+// buf[(z*K+y)*P + x], x < K, P = 2(K/2+1); the half spectrum overwrites it.
 void r2c_inplace(std::vector<double>& buf, int K) {
-    const int P = 2 * (K / 2 + 1), H = K / 2 + 1;
-    std::vector<cd> a(static_cast<size_t>(K) * K * K);
-    for (int z = 0; z < K; ++z)
-        for (int y = 0; y < K; ++y)
-            for (int x = 0; x < K; ++x)
-                a[(static_cast<size_t>(z) * K + y) * K + x] =
-                    buf[(static_cast<size_t>(z) * K + y) * P + x];
-    fft3d(a, K, -1);
-    for (int z = 0; z < K; ++z)
-        for (int y = 0; y < K; ++y)
-            for (int kx = 0; kx < H; ++kx) {
-                size_t o = ((static_cast<size_t>(z) * K + y) * H + kx) * 2;
-                cd v = a[(static_cast<size_t>(z) * K + y) * K + kx];
-                buf[o] = v.real();
-                buf[o + 1] = v.imag();
-            }
+    dmd_fft::r2c3d(buf.data(), 2 * (K / 2 + 1), buf.data(), K, K, K);
 }
 
-// Unnormalised c2r; the half spectrum is completed by Hermitian symmetry.
-// Padding doubles of each output row are set to zero (FFTW leaves them
-// unspecified; this build defines them as zero).
+// Unnormalised c2r in place; padding doubles of each output row are set to
+// zero (FFTW leaves them unspecified; this build defines them as zero).
 void c2r_inplace(std::vector<double>& buf, int K) {
-    const int P = 2 * (K / 2 + 1), H = K / 2 + 1;
-    std::vector<cd> a(static_cast<size_t>(K) * K * K);
-    for (int z = 0; z < K; ++z)
-        for (int y = 0; y < K; ++y)
-            for (int kx = 0; kx < K; ++kx) {
-                cd v;
-                if (kx < H) {
-                    size_t o = ((static_cast<size_t>(z) * K + y) * H + kx) * 2;
-                    v = cd(buf[o], buf[o + 1]);
-                } else {
-                    int zz = (K - z) % K, yy = (K - y) % K, xx = K - kx;
-                    size_t o = ((static_cast<size_t>(zz) * K + yy) * H + xx) * 2;
-                    v = std::conj(cd(buf[o], buf[o + 1]));
-                }
-                a[(static_cast<size_t>(z) * K + y) * K + kx] = v;
-            }
-    fft3d(a, K, +1);
-    std::fill(buf.begin(), buf.end(), 0.0);
-    for (int z = 0; z < K; ++z)
-        for (int y = 0; y < K; ++y)
-            for (int x = 0; x < K; ++x)
-                buf[(static_cast<size_t>(z) * K + y) * P + x] =
-                    a[(static_cast<size_t>(z) * K + y) * K + x].real();
+    dmd_fft::c2r3d(buf.data(), buf.data(), 2 * (K / 2 + 1), K, K, K);
 }
 
 // CoulombPME::theta4 / dtheta4 (src/force/coulomb_pme.cpp:50-69)

@@ -324,6 +324,7 @@ class ref_run_desc(C.Structure):
         ("dih_n", _ip), ("dih_kphi", _dp), ("dih_phi0", _dp),
         ("n_excl", C.c_int), ("excl_i", _ip), ("excl_j", _ip),
         ("coulomb_type", C.c_int), ("coul_cutoff", C.c_double), ("ewald", C.c_double),
+        ("pme_spacing", C.c_double), ("pme_order", C.c_int),
         ("dt", C.c_double), ("thermostat", C.c_int), ("t_temp", C.c_double), ("t_tau", C.c_double),
         ("t_freq", C.c_double), ("barostat", C.c_int), ("b_pressure", C.c_double),
         ("b_tau", C.c_double), ("b_compress", C.c_double), ("gen_vel", C.c_int), ("seed", C.c_int),
@@ -351,6 +352,7 @@ class Ref:
                                   _dp, _dp, _ip, _ip, C.c_long]),
             "ref_coulomb_direct": (None, [C.c_int, _dp, _dp, _dp, D, _dp, D, D, _dp, _dp, _dp, _dp]),
             "ref_exclusion": (None, [C.c_int, _dp, _dp, _dp, D, _dp, C.c_int, _ip, _ip, _dp, _dp, _dp, _dp]),
+            "ref_pme": (None, [C.c_int, _dp, _dp, _dp, D, _dp, C.c_int, D, D, C.c_int, _dp, _dp, _dp, _dp]),
             "ref_bond": (None, [C.c_int, _dp, _dp, _dp, D, C.c_int, _ip, _ip, _dp, _dp, _dp, _dp, _dp, _dp]),
             "ref_angle": (None, [C.c_int, _dp, _dp, _dp, D, C.c_int, _ip, _ip, _ip, _dp, _dp, _dp,
                                  _dp, _dp, _dp]),
@@ -439,6 +441,16 @@ class Ref:
         return self._bonded(self.L.ref_coulomb_direct, pos, box or cfg.box_size, len(pos), q[1],
                             cfg.coulomb_cutoff, cfg.ewald_coeff)
 
+    def pme(self, cfg, pos=None, box=None):
+        """CoulombPME::compute (reciprocal forces, reciprocal + self energy) on the
+        mesh build_force_engine picks (K = max(8, int(L/spacing + 0.5)))."""
+        pos = np.stack([cfg.pos_x, cfg.pos_y, cfg.pos_z], 1) if pos is None else pos
+        q = _d(cfg.charges)
+        box = box or cfg.box_size
+        K = max(8, int(cfg.box_size / cfg.pme_grid_spacing + 0.5))
+        return self._bonded(self.L.ref_pme, pos, box, len(pos), q[1], K, cfg.coulomb_cutoff,
+                            cfg.ewald_coeff, int(cfg.pme_order))
+
     def engine(self, cfg):
         return RefEngine(self, cfg)
 
@@ -447,8 +459,6 @@ class RefEngine:
     """The reference's components stepped in SimulationEngine::step order."""
 
     def __init__(self, r: Ref, cfg):
-        if cfg.coulomb_type == "pme":
-            raise ValueError("CoulombPME needs FFTW3 and is not built from the reference")
         self.r = r
         k = []
 
@@ -491,7 +501,9 @@ class RefEngine:
         s.n_excl = len(cfg.excl_i)
         if s.n_excl:
             s.excl_i, s.excl_j = i(cfg.excl_i), i(cfg.excl_j)
-        s.coulomb_type, s.coul_cutoff, s.ewald = 0, cfg.coulomb_cutoff, cfg.ewald_coeff
+        s.coulomb_type = 1 if cfg.coulomb_type == "pme" else 0
+        s.coul_cutoff, s.ewald = cfg.coulomb_cutoff, cfg.ewald_coeff
+        s.pme_spacing, s.pme_order = cfg.pme_grid_spacing, int(cfg.pme_order)
         s.dt = cfg.dt
         s.thermostat = THERMO[cfg.thermostat.type]
         s.t_temp, s.t_tau, s.t_freq = cfg.thermostat.temperature, cfg.thermostat.tau, cfg.thermostat.frequency

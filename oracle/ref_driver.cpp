@@ -7,10 +7,11 @@
 //
 // Buildable reference translation units (g++ 13, -std=c++20, no FMA
 // contraction, which is what the reference's own CMake build produces on
-// x86-64): src/core/*, src/force/* except coulomb_pme.cpp, src/integrate/*,
-// src/thermostat/*, src/barostat/*, src/sim/checkpoint.cpp.
-// Unbuildable here: src/force/coulomb_pme.cpp (needs FFTW3),
-// src/sim/simulation_engine.cpp (includes trajectory/h5md_writer.h -> HDF5),
+// x86-64): src/core/*, src/force/*, src/integrate/*, src/thermostat/*,
+// src/barostat/*, src/sim/checkpoint.cpp.  src/force/coulomb_pme.cpp includes
+// <fftw3.h>; FFTW3 is not installed, so it is compiled against shims/fftw3.h
+// (the same API over this repo's FFT, FFTW's in-place layout kept).
+// Unbuildable here: src/sim/simulation_engine.cpp (includes trajectory/h5md_writer.h -> HDF5),
 // src/trajectory/* (HDF5).  The engine step sequence of
 // src/sim/simulation_engine.cpp:53-86 and the factory of :147-203 are
 // therefore restated below (a dozen lines) on top of the reference's own
@@ -20,6 +21,7 @@
 // it is read here (for pair-set parity) by compiling the headers with
 // `private` mapped to `public`.  That changes no layout or code.
 
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -38,6 +40,7 @@
 #include "force/lennard_jones.h"
 #include "force/coulomb_direct.h"
 #include "force/coulomb_exclusion.h"
+#include "force/coulomb_pme.h"
 #include "force/harmonic_bond.h"
 #include "force/harmonic_angle.h"
 #include "force/periodic_dihedral.h"
@@ -110,6 +113,23 @@ void ref_coulomb_direct(int n, const double* x, const double* y, const double* z
     c.rebuild_pair_list(sx, sy, sz, cell);
     c.compute(sx, sy, sz, cell, std::span<double>(fx, n), std::span<double>(fy, n),
               std::span<double>(fz, n), *energy);
+}
+
+// ---- CoulombPME (reciprocal part + self energy) on a cubic K^3 mesh ------
+void ref_pme(int n, const double* x, const double* y, const double* z, double L, const double* q,
+             int K, double rc, double alpha, int order, double* fx, double* fy, double* fz,
+             double* energy) {
+    PMEParams p;
+    p.cutoff = rc;
+    p.ewald_coefficient = alpha;
+    p.spline_order = order;
+    p.nx = p.ny = p.nz = K;
+    CoulombPME c(p);
+    c.set_charges(std::span<const double>(q, n));
+    Cell cell(L, L, L);
+    c.compute(std::span<const double>(x, n), std::span<const double>(y, n),
+              std::span<const double>(z, n), cell, std::span<double>(fx, n),
+              std::span<double>(fy, n), std::span<double>(fz, n), *energy);
 }
 
 void ref_exclusion(int n, const double* x, const double* y, const double* z, double L,
@@ -222,8 +242,10 @@ struct ref_run_desc {
     const double *dih_kphi, *dih_phi0;
     int n_excl;
     const int *excl_i, *excl_j;
-    int coulomb_type;  // 0 = cutoff/direct (pme is unbuildable here)
+    int coulomb_type;  // 0 = cutoff/direct, 1 = pme
     double coul_cutoff, ewald;
+    double pme_spacing;
+    int pme_order;
     double dt;
     int thermostat;  // 0 none 1 berendsen 2 nose-hoover 3 andersen
     double t_temp, t_tau, t_freq;
@@ -280,6 +302,7 @@ void* ref_engine_create(const ref_run_desc* d) {
     }
     CoulombDirect* cd = nullptr;
     CoulombExclusion* ce = nullptr;
+    CoulombPME* cp = nullptr;
     {
         CoulombDirectParams p;
         p.cutoff = d->coul_cutoff;
@@ -288,7 +311,21 @@ void* ref_engine_create(const ref_run_desc* d) {
         cd = c.get();
         e->fe->add_component(std::move(c));
     }
-    if (d->n_excl > 0) {
+    if (d->coulomb_type == 1) {
+        // pme branch of build_force_engine (simulation_engine.cpp:173-190):
+        // direct, PME, then the exclusion correction (always added)
+        PMEParams p;
+        p.cutoff = d->coul_cutoff;
+        p.ewald_coefficient = d->ewald;
+        p.spline_order = d->pme_order;
+        p.nx = std::max(8, static_cast<int>(d->box / d->pme_spacing + 0.5));
+        p.ny = p.nx;
+        p.nz = p.nx;
+        auto c = std::make_unique<CoulombPME>(p);
+        cp = c.get();
+        e->fe->add_component(std::move(c));
+    }
+    if (d->coulomb_type == 1 || d->n_excl > 0) {
         auto c = std::make_unique<CoulombExclusion>();
         c->set_exclusions(std::span<const int>(d->excl_i, d->n_excl),
                           std::span<const int>(d->excl_j, d->n_excl));
@@ -335,6 +372,7 @@ void* ref_engine_create(const ref_run_desc* d) {
     s.atom_types = d->types ? veci(d->types, n) : std::vector<int>(n, 0);
     if (e->lj) e->lj->set_atom_types(s.atom_types);
     if (cd) cd->set_charges(s.charges);
+    if (cp) cp->set_charges(s.charges);
     if (ce) ce->set_charges(s.charges);
     if (d->gen_vel && n > 0) {
         // Maxwell-Boltzmann generation as in build_simulation (simulation_engine.cpp:339-383)
