@@ -13,6 +13,10 @@ FP64 CPU oracle at the starting configuration.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
+Defaults: K = 2000 timed steps (long enough for ~30 clock samples), W = 20.
+The CPU baseline (and the whole reference arm) is the reference's own C++ path
+compiled by oracle/Makefile, one core, a bounded 10-step sample.
+
 N > 1 runs one independent replica per GPU (one process per GPU, weak
 scaling, no collective on the data path); the step time is the max over ranks.
 One JSON line is printed by rank 0.
@@ -39,8 +43,9 @@ SM_COUNT, FP32_LANES = 148, 128
 PAIR_BYTES_PER_ATOM = 650.0
 PAIR_FLOP_PER_ATOM = 14690.0
 # DRAM bytes (read + write) of one pair-kernel launch on this workload, from the
-# ncu capture summarised in profiles/k_nb_f32_water30k.md.
-PAIR_DRAM_BYTES = None
+# ncu capture summarised in profiles/k_nb_f32_water30k.md (7.05 MB read, 0 written:
+# the 30k-atom working set stays in the 126 MB L2 apart from the first touch).
+PAIR_DRAM_BYTES = 7.05e6
 
 
 def _dist():
@@ -66,7 +71,7 @@ class ClockSampler:
         try:
             self.p = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=self.f, stderr=subprocess.DEVNULL)
         except OSError:
             self.p = None
@@ -213,6 +218,8 @@ def run_ours(args):
             "traffic": PAIR_DRAM_BYTES,
             "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
             "launch_ms": round(nb_ms, 5),
+            "launch_note": "average over the timed steps, measured while the bonded + PME chain "
+                           "runs beside it on a second stream",
             "algorithmic_bytes_per_launch": b_alg, "algorithmic_flop_per_launch": f_alg,
             "fp32": {"achieved_tflops": round(tflops, 3), "peak_tflops": round(p32, 2),
                      "frac": round(tflops / p32, 4),
@@ -254,19 +261,28 @@ def run_ours(args):
 
 
 def cpu_reference(cfg, n_atoms, steps):
-    """The reference's algorithm on one host core: REF profile (the reference's
-    formulas), its O(N^2) LennardJones list rebuilt every 10 force evaluations,
-    two force evaluations per step, FP64; PME with this repo's FFT (FFTW is not
-    available here)."""
-    from oracle.oracle import Oracle
-    eng = Oracle().engine(cfg, "ref", brute_list=True)
+    """The reference's CPU path on one host core (the reference has no threading
+    on this path), timed on a bounded sample from the start of the run.
+
+    Preferred: the reference's own C++ (src/ compiled unmodified by oracle/Makefile;
+    CoulombPME against the FFTW-API shim, since FFTW3 is not installed), stepped
+    in SimulationEngine::step order: its O(N^2) LennardJones list rebuilt every
+    10 force evaluations, two evaluations per step, FP64.  If that build is not
+    present, the oracle's restatement of the same algorithm (REF profile)."""
+    from oracle.oracle import Oracle, Ref, ref_available
+    if ref_available():
+        eng, kind = Ref().engine(cfg), "reference"
+        what = "reference C++ (src/, unmodified; PME via the FFTW-API shim)"
+    else:
+        eng, kind = Oracle().engine(cfg, "ref", brute_list=True), "port"
+        what = "oracle restatement of the reference algorithm (REF profile)"
     t0 = time.perf_counter()
     eng.step(steps)
     dt = time.perf_counter() - t0
     return {"value": round(n_atoms * steps / dt, 1), "unit": "atom-steps/s", "cores": 1,
-            "kind": "port",
+            "kind": kind,
             "sample": f"{steps} MD steps of the same 30,000-atom water box from the start "
-                      f"(includes {(steps + 4) // 5} O(N^2) list rebuilds), {dt:.1f} s"}
+                      f"({what}; includes {(steps + 4) // 5} O(N^2) list rebuilds), {dt:.1f} s"}
 
 
 def run_reference(args):
@@ -282,7 +298,8 @@ def run_reference(args):
             "n_gpus": ws, "steps": steps, "warmup": 0, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": "water_30k_nvt_pme64", "n_atoms": w.n_atoms, "profile": "ref",
-                       "implementation": "CPU restatement of the reference path (oracle port)"},
+                       "implementation": cpu["sample"].split("(")[1].split(";")[0],
+                       "sample_steps": steps},
             "cpu_baseline": cpu,
             "e2e": {"value": v, "unit": "atom-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
@@ -290,7 +307,7 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cpu-steps", type=int, default=10)

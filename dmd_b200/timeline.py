@@ -1,0 +1,69 @@
+"""Per-kernel device timeline of a few MD steps (CUPTI through torch.profiler).
+
+Shows what runs where inside the step graph: start and end of every kernel of
+a step relative to the step's first kernel, so overlap between the main stream
+(list rebuild, pair kernel) and the bonded/PME stream is visible, plus the
+mean step period and per-kernel totals.
+
+    python -m dmd_b200.timeline [--steps 30] [--precision mixed] [--show 3]
+
+Runs on the headline workload (water 30k NVT, PHYS profile).  A diagnostic:
+numbers printed under a profiler are not benchmark values.
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import sys
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--show", type=int, default=3, help="steps printed kernel by kernel")
+    args = ap.parse_args()
+    import torch
+    from torch.profiler import ProfilerActivity, profile
+
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    from dmd_b200.core import Engine
+    from dmd_b200 import workloads as W
+
+    cfg = W.water_box(n_mol=10_000, box=6.69, seed=7, spacing=0.1045, thermostat="nose-hoover",
+                      dt=0.0005).config()
+    eng = Engine(cfg, precision=args.precision, profile="phys")
+    eng.run_n(args.warmup)
+    eng.positions
+    with profile(activities=[ProfilerActivity.CUDA]) as prof:
+        eng.run_n(args.steps)
+        eng.positions
+    ev = [e for e in prof.events() if e.device_type.name == "CUDA" and "Memcpy" not in e.name]
+    ev.sort(key=lambda e: e.time_range.start)
+
+    def short(name):
+        return name.replace("void ", "").replace("dmd::(anonymous namespace)::", "").replace("dmd::", "")[:44]
+
+    starts = [e.time_range.start for e in ev if "k_step_begin" in e.name]
+    if len(starts) > 1:
+        print(f"steps {len(starts)}  mean step period {(starts[-1] - starts[0]) / (len(starts) - 1):.1f} us")
+    for si in range(min(args.show, max(len(starts) - 1, 0))):
+        t0, t1 = starts[si], starts[si + 1]
+        print(f"--- step {si}: {t1 - t0:.1f} us")
+        for e in ev:
+            if t0 <= e.time_range.start < t1:
+                print(f"{short(e.name):44s} start {e.time_range.start - t0:7.1f}  end "
+                      f"{e.time_range.end - t0:7.1f}  dur {e.time_range.end - e.time_range.start:6.1f}")
+    agg = {}
+    for e in ev:
+        a = agg.setdefault(short(e.name), [0, 0.0])
+        a[0] += 1
+        a[1] += e.time_range.end - e.time_range.start
+    print(f"--- totals over {args.steps} steps")
+    for k, (n, t) in sorted(agg.items(), key=lambda x: -x[1][1]):
+        print(f"{k:44s} {n:6d} launches {t:10.1f} us  {t / n:7.2f} us avg")
+
+
+if __name__ == "__main__":
+    main()
