@@ -1,21 +1,32 @@
 #!/usr/bin/env python
-"""Headline benchmark: MD throughput (atom-steps/s) of the force-and-integrate path.
+"""MD throughput (atom-steps/s) of the force-and-integrate path on one B200.
 
-Workload (the configuration the metric is quoted on): flexible 3-site water,
-10,000 molecules (30,000 atoms) in a 6.69 nm cubic box, SPME 64^3 (order 4,
-beta 3.12 nm^-1, cutoff 1.0 nm), Nose-Hoover NVT at 300 K, dt 0.5 fs; seeded
-synthetic jittered-lattice start (no dataset).  Physically consistent profile
-(gradient-consistent forces; the reference's own flexible-water forces are
-unstable), mixed precision (FP32 pair / mesh / bonded arithmetic, int64
-fixed-point forces, FP64 integration).  The all-FP64 GPU path is timed on the
-same system for the mixed-vs-FP64 comparison, and both are checked against the
-FP64 CPU oracle at the starting configuration.
+Default workload (the configuration the headline metric is quoted on):
+flexible 3-site water, 10,000 molecules (30,000 atoms) in a 6.69 nm cubic box,
+SPME 64^3 (order 4, beta 3.12 nm^-1, cutoff 1.0 nm), Nose-Hoover NVT at 300 K,
+dt 0.5 fs; seeded synthetic jittered-lattice start (no dataset).  Physically
+consistent profile (gradient-consistent forces; the reference's own
+flexible-water forces are unstable), mixed precision (FP32 pair / mesh /
+bonded arithmetic, int64 fixed-point forces, FP64 integration).  The all-FP64
+GPU path is timed on the same system for the mixed-vs-FP64 comparison, and
+both are checked against the FP64 CPU oracle at the starting configuration.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--workload water30k|argon4k|water750k|batch256|serve]
 
-Defaults: K = 2000 timed steps (long enough for ~30 clock samples), W = 20.
+Other workloads (same JSON line, their own config):
+  argon4k    LJ argon NVE, 4,000 atoms (10x10x10 FCC, 5.75 nm box), dt 2 fs
+  water750k  the water model at 250,000 molecules (19.56 nm box), SPME 192^3,
+             Berendsen thermostat + Berendsen barostat (NPT), dt 0.5 fs
+  batch256   256 independent replicas in one device batch (192 LJ fluids of
+             500-20,000 atoms, 64 united-atom decane melts of 50-400 chains),
+             against the FP64 batch and the same replicas run one per launch
+  serve      a Poisson stream of MD jobs (70% LJ argon 1k-50k atoms, 30% water
+             with SPME 3k-96k atoms, 1,000-20,000 steps each) continuously
+             batched under a 150 GB HBM budget; p50/p99 step and job latency
+
 The CPU baseline (and the whole reference arm) is the reference's own C++ path
-compiled by oracle/Makefile, one core, a bounded 10-step sample.
+compiled by oracle/Makefile, one core, a bounded sample.
 
 N > 1 runs one independent replica per GPU (one process per GPU, weak
 scaling, no collective on the data path); the step time is the max over ranks.
@@ -25,6 +36,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -38,14 +50,31 @@ sys.path.insert(0, ROOT)
 L2_FLUSH_BYTES = 256 << 20          # > 126 MB L2: each timed step starts with a cold L2
 MEASURED_PEAK_HBM_GBS = 6538.9      # fallback when MEASURED_PEAKS.json is absent: measured copy BW
 SM_COUNT, FP32_LANES = 148, 128
-# Algorithmic work of the pair kernel per atom and evaluation (water, rc 1.0 nm,
-# 210 half-neighbours): tile-stream bytes and FLOPs (70 FLOP per LJ + erfc pair).
-PAIR_BYTES_PER_ATOM = 650.0
-PAIR_FLOP_PER_ATOM = 14690.0
-# DRAM bytes (read + write) of one pair-kernel launch on this workload, from the
-# ncu capture summarised in profiles/k_nb_f32_water30k.md (7.05 MB read, 0 written:
-# the 30k-atom working set stays in the 126 MB L2 apart from the first touch).
-PAIR_DRAM_BYTES = 7.05e6
+WORKLOADS = ("water30k", "argon4k", "water750k", "batch256", "serve")
+CPU_MAX_ATOMS = 100_000             # above this the reference's O(N^2) list build takes hours
+
+# Algorithmic work of the pair kernel per atom and evaluation, as a tile-streaming
+# pair kernel must do it: bytes = (half j-tiles per i-tile) x (32 x 16 B j payload
+# + 8 B list entry) / 32 + 40 B (own float4 read + three int64 force writes);
+# FLOPs = half-pairs within the cutoff x 38 (LJ) or 70 (LJ + erfc Ewald).
+# Water (rc 1.0 nm, 100.2 atoms/nm^3, 210 half-neighbours): 650 B, 14,690 FLOP.
+# Argon (rc 1.0 nm, 21.0 atoms/nm^3, 44 half-neighbours): 241 B, 1,675 FLOP.
+PAIR_WORK = {"water": (650.0, 14690.0), "argon": (241.0, 1675.0)}
+# DRAM bytes (read + write) of one pair-kernel launch, from the ncu captures in
+# profiles/ (water 30k: 7.05 MB read, 0 written -- the working set stays in L2).
+PAIR_DRAM_BYTES = {"water30k": 7.05e6}
+
+
+def lj_pair_work(n: int, box: float, rc: float, flop_per_pair: float = 38.0):
+    """Per-atom algorithmic (bytes, FLOP) of the pair kernel for a homogeneous
+    system of n atoms in a cubic box (the same model as PAIR_WORK): half j-tiles
+    per i-tile = atoms within rc + one tile edge of a tile, halved, / 32."""
+    rho = n / box ** 3
+    edge = (32.0 / rho) ** (1.0 / 3.0)
+    vol = 4.0 / 3.0 * math.pi
+    tiles = min(0.5 * rho * vol * (rc + edge) ** 3, n) / 32.0
+    half_pairs = min(0.5 * rho * vol * rc ** 3, 0.5 * n)
+    return tiles * (32 * 16 + 8) / 32.0 + 40.0, half_pairs * flop_per_pair
 
 
 def _dist():
@@ -56,7 +85,7 @@ def _dist():
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+    """nvidia-smi clocks / throttle reasons sampled every 50 ms during the timed region."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -112,10 +141,35 @@ def _peaks():
     return 6650.0, "fallback"
 
 
-def workload(rank: int):
+# ---------------------------------------------------------------------------
+# workloads
+
+def water30k(rank: int):
     from dmd_b200 import workloads
     return workloads.water_box(n_mol=10_000, box=6.69, seed=7 + rank, spacing=0.1045,
                                thermostat="nose-hoover", dt=0.0005)
+
+
+def argon4k(rank: int):
+    from dmd_b200 import workloads
+    return workloads.argon_fcc(n_cells=10, a=0.575, T=120.0, seed=2024 + rank, dt=0.002)
+
+
+def water750k(rank: int):
+    from dmd_b200 import workloads
+    return workloads.water_box(n_mol=250_000, box=19.56, seed=7 + rank, spacing=0.1019,
+                               thermostat="berendsen", barostat="berendsen", dt=0.0005)
+
+
+SINGLE = {
+    "water30k": dict(make=water30k, kind="water", pme=64, ensemble="nose-hoover NVT 300 K",
+                     desc="seeded jittered-lattice water, random orientations"),
+    "argon4k": dict(make=argon4k, kind="argon", pme=None, ensemble="NVE (velocities at 120 K)",
+                    desc="FCC argon lattice, Maxwell-Boltzmann velocities from a seed"),
+    "water750k": dict(make=water750k, kind="water", pme=192,
+                      ensemble="Berendsen T 300 K + Berendsen P 1 bar (NPT)",
+                      desc="seeded jittered-lattice water, random orientations"),
+}
 
 
 def rel_rms(a, b):
@@ -123,146 +177,380 @@ def rel_rms(a, b):
     return float(np.linalg.norm(a - b) / np.linalg.norm(b))
 
 
-def run_ours(args):
-    import numpy as np
-    import torch
-    ws, rank, local = _dist()
-    torch.cuda.set_device(local)
-    if ws > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    from dmd_b200.core import Engine
+class Ranks:
+    """Process-group plumbing: barrier and max over ranks (no-ops at N = 1)."""
 
-    w = workload(rank)
+    def __init__(self, local: int):
+        import torch
+        self.ws, self.rank, self.local = _dist()
+        torch.cuda.set_device(local)
+        if self.ws > 1:
+            import datetime
+            import torch.distributed as dist
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    def barrier(self):
+        if self.ws > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    def max(self, v: float) -> float:
+        if self.ws == 1:
+            return v
+        import torch
+        import torch.distributed as dist
+        t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{self.local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.ws > 1:
+            import torch.distributed as dist
+            dist.barrier()
+            dist.destroy_process_group()
+
+
+def roofline(kind_bytes: float, kind_flop: float, nb_ms: float, clocks: dict, traffic,
+             kernel: str, fp32_binding: bool, launch_note: str) -> dict:
+    hbm_peak, peak_kind = _peaks()
+    t_nb = nb_ms / 1e3
+    achieved = kind_bytes / t_nb / 1e9
+    tflops = kind_flop / t_nb / 1e12
+    f_sm = (clocks.get("sm_mhz") or 1965.0) * 1e6
+    p32 = SM_COUNT * FP32_LANES * 2 * f_sm / 1e12
+    return {
+        "kernel": kernel,
+        "bound": "hbm", "achieved": round(achieved, 2), "peak": hbm_peak, "unit": "GB/s",
+        "frac": round(achieved / hbm_peak, 4),
+        "traffic": traffic,
+        "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+        "launch_ms": round(nb_ms, 5),
+        "launch_note": launch_note,
+        "algorithmic_bytes_per_launch": kind_bytes, "algorithmic_flop_per_launch": kind_flop,
+        "fp32": {"achieved_tflops": round(tflops, 3), "peak_tflops": round(p32, 2),
+                 "frac": round(tflops / p32, 4),
+                 "peak_note": "148 SMs x 128 FP32 lanes x 2 x median SM clock of the run"},
+        "binding_roof": ("fp32 (arithmetic intensity above the ridge)" if fp32_binding
+                         else "hbm (arithmetic intensity below the ridge)"),
+    }
+
+
+def run_single(args, R: Ranks):
+    """One system per GPU: water30k, argon4k or water750k."""
+    from dmd_b200.core import Engine
+    spec = SINGLE[args.workload]
+    w = spec["make"](R.rank)
     cfg = w.config()
     n_atoms = w.n_atoms
     dt = cfg.dt
 
-    def barrier():
-        if ws > 1:
-            import torch.distributed as dist
-            dist.barrier()
-
-    def max_over_ranks(v: float) -> float:
-        if ws == 1:
-            return v
-        import torch.distributed as dist
-        t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
     def timed(precision):
-        eng = Engine(cfg, precision=precision, profile="phys", device=local)
+        eng = Engine(cfg, precision=precision, profile="phys", device=R.local)
         eng.run_n(args.warmup)
         eng.positions  # sync
-        barrier()
-        sampler = ClockSampler(local)
+        R.barrier()
+        sampler = ClockSampler(R.local)
         sampler.start()
         t = eng.step_timed(args.steps, L2_FLUSH_BYTES)
         clocks = sampler.stop()
-        barrier()
-        step_ms = max_over_ranks(t["step_ms"])
-        nb_ms = max_over_ranks(t["nonbonded_ms"] / max(t["nonbonded_launches"], 1))
+        R.barrier()
+        step_ms = R.max(t["step_ms"])
+        nb_ms = R.max(t["nonbonded_ms"] / max(t["nonbonded_launches"], 1))
         return eng, t, step_ms, nb_ms, clocks
 
     eng, t_mixed, step_ms, nb_ms, clocks = timed("mixed")
-    value = ws * n_atoms * args.steps / (step_ms / 1e3)
+    value = R.ws * n_atoms * args.steps / (step_ms / 1e3)
     s = eng.scalars()
+    evals_per_step = t_mixed["nonbonded_launches"] / args.steps
+    # accuracy is checked at the starting configuration, except on a perfect
+    # lattice (argon FCC: every force vanishes by symmetry), where it is checked
+    # at the configuration the timed run reached
+    acc_pos = eng.positions if spec["kind"] == "argon" else None
+    eng.close()
     _, t64, step_ms64, _, _ = timed("fp64")
-    value64 = ws * n_atoms * args.steps / (step_ms64 / 1e3)
+    value64 = R.ws * n_atoms * args.steps / (step_ms64 / 1e3)
 
     # end to end through the public API: one run_n(1) call per MD step plus the
     # potential-energy read, host buffers, wall clock
-    eng_e = Engine(cfg, precision="mixed", profile="phys", device=local)
+    eng_e = Engine(cfg, precision="mixed", profile="phys", device=R.local)
     eng_e.run_n(args.warmup)
     _ = eng_e.potential_energy
-    barrier()
+    R.barrier()
     t0 = time.perf_counter()
-    pe = 0.0
     for _ in range(args.steps):
         eng_e.run_n(1)
-        pe = eng_e.potential_energy
-    e2e_s = max_over_ranks(time.perf_counter() - t0)
-    e2e_value = ws * n_atoms * args.steps / e2e_s
+        _ = eng_e.potential_energy
+    e2e_s = R.max(time.perf_counter() - t0)
+    e2e_value = R.ws * n_atoms * args.steps / e2e_s
+    eng_e.close()
 
-    out = None
-    if rank == 0:
-        # accuracy at the starting configuration against the FP64 CPU oracle
-        from oracle.oracle import Oracle
-        F_o, e_o = Oracle().forces(cfg, "phys")
-        acc = {}
-        for prec in ("mixed", "fp64"):
-            e0 = Engine(cfg, precision=prec, profile="phys", device=local)
+    if R.rank != 0:
+        return None
+    # accuracy at the starting configuration against the FP64 CPU oracle
+    from oracle.oracle import Oracle
+    F_o, e_o = Oracle().forces(cfg, "phys", pos=acc_pos)
+    acc = {"configuration": "start" if acc_pos is None else
+           f"after the {args.warmup + args.steps}-step timed run"}
+    for prec in ("mixed", "fp64"):
+        e0 = Engine(cfg, precision=prec, profile="phys", device=R.local)
+        if acc_pos is not None:
+            e0.set_positions(acc_pos)
+        F, e = e0.compute_forces()
+        acc[prec] = {"rel_rms_force_err": rel_rms(F, F_o),
+                     "rel_energy_err": abs(sum(e.values()) - e_o["total"]) / abs(e_o["total"])}
+        e0.close()
+    cpu = None
+    if not args.skip_cpu and R.ws == 1 and n_atoms > CPU_MAX_ATOMS:
+        cpu = {"value": None, "unit": "atom-steps/s", "cores": 1, "kind": "reference",
+               "sample": f"not timed: the reference's first step alone builds its O(N^2) pair list "
+                         f"({n_atoms * (n_atoms - 1) // 2:.2e} pair tests on one core); see the "
+                         f"water30k line for the reference's rate on the same water model"}
+    elif not args.skip_cpu and R.ws == 1:
+        cpu = cpu_reference([cfg], args.cpu_steps, f"the same {n_atoms:,}-atom system")
+    b_atom, f_atom = PAIR_WORK[spec["kind"]]
+    roof = roofline(b_atom * n_atoms, f_atom * n_atoms, nb_ms, clocks,
+                    PAIR_DRAM_BYTES.get(args.workload),
+                    "k_nb_f32 (LJ + real-space Ewald pair kernel)" if spec["kind"] == "water"
+                    else "k_nb_f32 (LJ pair kernel)",
+                    spec["kind"] == "water",
+                    "average over the timed steps" + (
+                        ", measured while the bonded + PME chain runs beside it on a second stream"
+                        if spec["pme"] else ""))
+    config = {"workload": f"{args.workload}", "n_atoms": n_atoms, "box_nm": cfg.box_size,
+              "cutoff_nm": cfg.lj_cutoff, "skin_nm": 0.1, "dt_ps": dt,
+              "ensemble": spec["ensemble"], "profile": "phys",
+              "force_evaluations_per_step": round(evals_per_step, 3),
+              "l2": "flushed between timed steps (256 MiB overwrite outside the step events)",
+              "parallelism": f"replicas x{R.ws} (one independent system per GPU)"}
+    if spec["pme"]:
+        config.update({"pme_mesh": spec["pme"], "pme_order": 4, "ewald_beta": 3.12})
+    return {
+        "metric": "atom-steps/s", "value": round(value, 1), "unit": "atom-steps/s",
+        "n_gpus": R.ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(step_ms / args.steps, 5), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "precision": "mixed: FP32 pair/mesh/bonded math, int64 fixed-point forces, FP64 integration",
+        "data": f"synthetic ({spec['desc']})",
+        "config": config,
+        "ns_per_day": round(dt * 1e-3 * args.steps / (step_ms / 1e3) * 86400, 2),
+        "fp64_path": {"value": round(value64, 1), "ms_per_step": round(step_ms64 / args.steps, 5),
+                      "mixed_over_fp64": round(value / value64, 3)},
+        "accuracy_vs_fp64_cpu_oracle": acc,
+        "e2e": {"value": round(e2e_value, 1), "unit": "atom-steps/s",
+                "h2d_bytes_per_step": 8, "d2h_bytes_per_step": 8 + 2 * 232,
+                "how": "Engine.run_n(1) + Engine.potential_energy per MD step (C ABI, host "
+                       "buffers, host wall clock); inputs are the step target, result the "
+                       "energy scalars"},
+        "roofline": roof,
+        "cpu_baseline": cpu,
+        "gpu_launches": int(t_mixed["kernel_launches"]),
+        "clocks": clocks,
+        "list_builds": int(s.list_builds),
+    }
+
+
+def run_batch(args, R: Ranks):
+    """256 independent replicas advanced together in one device batch."""
+    from dmd_b200 import workloads as W
+    from dmd_b200.batch import Batch
+    from dmd_b200.core import Engine
+    ws_ = W.batch_256(seed=1234 + 1000 * R.rank)
+    cfgs = [w.config() for w in ws_]
+    n_atoms = sum(w.n_atoms for w in ws_)
+    target = args.warmup + args.steps + 1
+
+    def timed(precision):
+        b = Batch(precision=precision, profile="phys", device=R.local)
+        slots = [b.admit(c, target) for c in cfgs]
+        b.step(args.warmup)
+        R.barrier()
+        sampler = ClockSampler(R.local)
+        sampler.start()
+        t = b.step_timed(args.steps, L2_FLUSH_BYTES)
+        clocks = sampler.stop()
+        R.barrier()
+        return b, slots, t, clocks
+
+    b, slots, t_mixed, clocks = timed("mixed")
+    step_ms = R.max(t_mixed["step_ms"])
+    nb_ms = R.max(t_mixed["nonbonded_ms"] / max(t_mixed["nonbonded_launches"], 1))
+    value = R.ws * n_atoms * args.steps / (step_ms / 1e3)
+    list_builds = sum(int(b.scalars(s).list_builds) for s in slots)
+    used = b.used_bytes
+
+    # end to end through the public API: Batch.step(1) per MD step (each call
+    # returns after the device finished and the per-replica status records were
+    # read back), then every replica's potential energy
+    n_e2e = min(args.steps, 50)
+    b_e = Batch(precision="mixed", profile="phys", device=R.local)
+    for c in cfgs:
+        b_e.admit(c, args.warmup + n_e2e)
+    b_e.step(args.warmup)
+    R.barrier()
+    t0 = time.perf_counter()
+    for _ in range(n_e2e):
+        b_e.step(1)
+    pe = [b_e.scalars(s).potential_energy for s in b_e.slots]
+    e2e_s = R.max(time.perf_counter() - t0)
+    e2e_value = R.ws * n_atoms * n_e2e / e2e_s
+    b_e.close()
+    b.close()
+
+    b64, _, t64, _ = timed("fp64")
+    step_ms64 = R.max(t64["step_ms"])
+    value64 = R.ws * n_atoms * args.steps / (step_ms64 / 1e3)
+    b64.close()
+
+    # the same replicas one per launch: each replica alone in its own engine,
+    # stepped with the same kernels; device time summed over replicas
+    solo_steps = max(3, min(args.steps, 20))
+    solo_ms = 0.0
+    for c in cfgs:
+        e = Engine(c, precision="mixed", profile="phys", device=R.local)
+        e.run_n(args.warmup)
+        solo_ms += e.step_timed(solo_steps)["step_ms"]
+        e.close()
+    solo_ms = R.max(solo_ms)
+    value_solo = R.ws * n_atoms * solo_steps / (solo_ms / 1e3)
+
+    if R.rank != 0:
+        return None
+    from oracle.oracle import Oracle
+    o = Oracle()
+    sample = [0, 1, 2, 192, 193]
+    acc = {}
+    for prec in ("mixed", "fp64"):
+        errs, eerrs = [], []
+        for k in sample:
+            F_o, e_o = o.forces(cfgs[k], "phys")
+            e0 = Engine(cfgs[k], precision=prec, profile="phys", device=R.local)
             F, e = e0.compute_forces()
-            acc[prec] = {"rel_rms_force_err": rel_rms(F, F_o),
-                         "rel_energy_err": abs(sum(e.values()) - e_o["total"]) / abs(e_o["total"])}
             e0.close()
-        # CPU baseline: the reference algorithm (REF profile, O(N^2) list every 5
-        # steps, FP64) on one host core, bounded sample
-        cpu = None
-        if not args.skip_cpu and ws == 1:
-            cpu = cpu_reference(cfg, n_atoms, args.cpu_steps)
-        hbm_peak, peak_kind = _peaks()
-        t_nb = nb_ms / 1e3
-        b_alg = PAIR_BYTES_PER_ATOM * n_atoms
-        f_alg = PAIR_FLOP_PER_ATOM * n_atoms
-        f_sm = (clocks.get("sm_mhz") or 1965.0) * 1e6
-        p32 = SM_COUNT * FP32_LANES * 2 * f_sm / 1e12
-        achieved = b_alg / t_nb / 1e9
-        tflops = f_alg / t_nb / 1e12
-        roof = {
-            "kernel": "k_nb_f32 (LJ + real-space Ewald pair kernel)",
-            "bound": "hbm", "achieved": round(achieved, 2), "peak": hbm_peak, "unit": "GB/s",
-            "frac": round(achieved / hbm_peak, 4),
-            "traffic": PAIR_DRAM_BYTES,
-            "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
-            "launch_ms": round(nb_ms, 5),
-            "launch_note": "average over the timed steps, measured while the bonded + PME chain "
-                           "runs beside it on a second stream",
-            "algorithmic_bytes_per_launch": b_alg, "algorithmic_flop_per_launch": f_alg,
-            "fp32": {"achieved_tflops": round(tflops, 3), "peak_tflops": round(p32, 2),
-                     "frac": round(tflops / p32, 4),
-                     "peak_note": "148 SMs x 128 FP32 lanes x 2 x median SM clock of the run"},
-            "binding_roof": "fp32 (arithmetic intensity 22.6 FLOP/B > ridge)",
-        }
-        out = {
-            "metric": "atom-steps/s", "value": round(value, 1), "unit": "atom-steps/s",
-            "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": round(step_ms / args.steps, 5), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "precision": "mixed: FP32 pair/mesh/bonded math, int64 fixed-point forces, FP64 integration",
-            "data": "synthetic (seeded jittered-lattice water, random orientations)",
-            "config": {"workload": "water_30k_nvt_pme64", "n_atoms": n_atoms, "box_nm": cfg.box_size,
-                       "pme_mesh": 64, "cutoff_nm": 1.0, "skin_nm": 0.1, "dt_ps": dt,
-                       "thermostat": "nose-hoover 300 K", "profile": "phys",
-                       "l2": "flushed between timed steps (256 MiB overwrite outside the step events)",
-                       "parallelism": f"replicas x{ws} (one independent system per GPU)"},
-            "ns_per_day": round(dt * 1e-3 * args.steps / (step_ms / 1e3) * 86400, 2),
-            "fp64_path": {"value": round(value64, 1), "ms_per_step": round(step_ms64 / args.steps, 5),
-                          "mixed_over_fp64": round(value / value64, 3)},
-            "accuracy_vs_fp64_cpu_oracle": acc,
-            "e2e": {"value": round(e2e_value, 1), "unit": "atom-steps/s",
-                    "h2d_bytes_per_step": 8, "d2h_bytes_per_step": 8 + 2 * 232,
-                    "how": "Engine.run_n(1) + Engine.potential_energy per MD step (C ABI, host "
-                           "buffers, host wall clock); inputs are the step target, result the "
-                           "energy scalars"},
-            "roofline": roof,
-            "cpu_baseline": cpu,
-            "gpu_launches": int(t_mixed["kernel_launches"]),
-            "clocks": clocks,
-            "list_builds": int(s.list_builds),
-        }
-    if ws > 1:
-        import torch.distributed as dist
-        dist.barrier()
-        dist.destroy_process_group()
-    return out
+            errs.append(rel_rms(F, F_o))
+            eerrs.append(abs(sum(e.values()) - e_o["total"]) / abs(e_o["total"]))
+        acc[prec] = {"rel_rms_force_err_max": max(errs), "rel_energy_err_max": max(eerrs),
+                     "replicas": sample}
+    cpu = None
+    if not args.skip_cpu and R.ws == 1:
+        cpu = cpu_reference([cfgs[k] for k in (0, 1, 192)], args.cpu_steps,
+                            "replicas 0, 1 (LJ) and 192 (decane) of the same batch, one after another")
+    # pair-kernel algorithmic work, summed over the replicas
+    b_alg = f_alg = 0.0
+    for w, c in zip(ws_, cfgs):
+        ba, fa = lj_pair_work(w.n_atoms, c.box_size, c.lj_cutoff)
+        b_alg += ba * w.n_atoms
+        f_alg += fa * w.n_atoms
+    roof = roofline(b_alg, f_alg, nb_ms, clocks, None,
+                    "k_nb_f32 (LJ pair kernel over all 256 replicas in one launch)", False,
+                    "average over the timed steps, one launch covers every replica")
+    n_lj = sum(1 for w in ws_ if w.name.startswith("lj_"))
+    return {
+        "metric": "atom-steps/s", "value": round(value, 1), "unit": "atom-steps/s",
+        "n_gpus": R.ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(step_ms / args.steps, 5), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "precision": "mixed: FP32 pair/mesh/bonded math, int64 fixed-point forces, FP64 integration",
+        "data": "synthetic (seeded LJ fluids on jittered lattices, decane melts grown as "
+                "self-avoiding random walks; one seed per replica)",
+        "config": {"workload": "batch256", "replicas": len(cfgs), "lj_fluids": n_lj,
+                   "decane_melts": len(cfgs) - n_lj, "n_atoms_total": n_atoms,
+                   "atoms_min": min(w.n_atoms for w in ws_),
+                   "atoms_max": max(w.n_atoms for w in ws_), "dt_ps": 0.002, "ensemble": "NVE",
+                   "profile": "phys", "device_bytes": used,
+                   "l2": "flushed between timed steps (256 MiB overwrite outside the step events)",
+                   "parallelism": f"replicas x{R.ws} (one 256-replica batch per GPU)"},
+        "fp64_path": {"value": round(value64, 1), "ms_per_step": round(step_ms64 / args.steps, 5),
+                      "mixed_over_fp64": round(value / value64, 3)},
+        "one_per_launch": {"value": round(value_solo, 1), "steps": solo_steps,
+                           "batched_over_one_per_launch": round(value / value_solo, 3),
+                           "how": "each replica alone in its own engine (same kernels, one CUDA "
+                                  "graph per step), device step times summed over the replicas"},
+        "accuracy_vs_fp64_cpu_oracle": acc,
+        "e2e": {"value": round(e2e_value, 1), "unit": "atom-steps/s", "steps": n_e2e,
+                "h2d_bytes_per_step": 4, "d2h_bytes_per_step": 240 * len(cfgs),
+                "how": "Batch.step(1) per MD step through the C ABI (returns after the device "
+                       "finished; reads back each replica's 240-byte status record), potential "
+                       "energies of all replicas read at the end; host wall clock"},
+        "roofline": roof,
+        "cpu_baseline": cpu,
+        "gpu_launches": int(t_mixed["kernel_launches"]),
+        "clocks": clocks,
+        "list_builds": list_builds,
+        "potential_energy_finite": bool(all(math.isfinite(x) for x in pe)),
+    }
 
 
-def cpu_reference(cfg, n_atoms, steps):
+def run_serve(args, R: Ranks):
+    """A Poisson stream of MD jobs, continuously batched under an HBM budget."""
+    from dmd_b200.core import Engine
+    from dmd_b200.serve import job_mix, serve
+    out = {}
+    for prec in ("mixed", "fp64"):
+        jobs = job_mix(args.jobs, args.rate, seed=2025 + R.rank, scale=args.scale)
+        R.barrier()
+        sampler = ClockSampler(R.local)
+        sampler.start()
+        res = serve(jobs, budget_bytes=150 * 10**9, precision=prec, profile="phys",
+                    chunk=args.chunk)
+        clocks = sampler.stop()
+        res["atom_steps_per_s"] = R.ws * res["work_atom_steps"] / R.max(res["wall_s"])
+        out[prec] = (res, clocks, jobs)
+    if R.rank != 0:
+        return None
+    res, clocks, jobs = out["mixed"]
+    res64 = out["fp64"][0]
+    from oracle.oracle import Oracle
+    o = Oracle()
+    acc = {}
+    sample = [j for j in jobs if j.n_atoms <= 20000][:3]
+    for prec in ("mixed", "fp64"):
+        errs = []
+        for j in sample:
+            F_o, _ = o.forces(j.cfg, "phys")
+            e0 = Engine(j.cfg, precision=prec, profile="phys", device=R.local)
+            F, _ = e0.compute_forces()
+            e0.close()
+            errs.append(rel_rms(F, F_o))
+        acc[prec] = {"rel_rms_force_err_max": max(errs), "jobs": [j.jid for j in sample]}
+    cpu = None
+    if not args.skip_cpu and R.ws == 1:
+        cpu = cpu_reference([j.cfg for j in sample[:2]], args.cpu_steps,
+                            f"jobs {sample[0].jid} and {sample[1].jid} of the same stream")
+    steps_total = sum(j.n_steps for j in jobs)
+    return {
+        "metric": "atom-steps/s", "value": round(res["atom_steps_per_s"], 1),
+        "unit": "atom-steps/s", "n_gpus": R.ws, "steps": steps_total, "warmup": 0,
+        "ms_per_step": round(res["step_latency_ms"]["p50"], 5), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "precision": "mixed: FP32 pair/mesh/bonded math, int64 fixed-point forces, FP64 integration",
+        "data": "synthetic (seeded job stream: LJ argon and SPME water, one seed per job)",
+        "config": {"workload": "serve", "jobs": len(jobs), "rate_jobs_per_s": args.rate,
+                   "scale": args.scale, "chunk_steps": args.chunk, "budget_gb": 150,
+                   "atoms_min": min(j.n_atoms for j in jobs),
+                   "atoms_max": max(j.n_atoms for j in jobs), "profile": "phys",
+                   "l2": "not flushed (jobs' state stays resident, far above L2 in total)",
+                   "parallelism": f"replicas x{R.ws} (one job stream per GPU)"},
+        "latency": {"step_ms": res["step_latency_ms"], "job_s": res["job_latency"]},
+        "wall_s": round(res["wall_s"], 3),
+        "fp64_path": {"value": round(res64["atom_steps_per_s"], 1),
+                      "latency": {"step_ms": res64["step_latency_ms"], "job_s": res64["job_latency"]},
+                      "mixed_over_fp64": round(res["atom_steps_per_s"] / res64["atom_steps_per_s"], 3)},
+        "accuracy_vs_fp64_cpu_oracle": acc,
+        "e2e": {"value": round(res["atom_steps_per_s"], 1), "unit": "atom-steps/s",
+                "h2d_bytes_per_step": None, "d2h_bytes_per_step": None,
+                "how": "the whole stream through dmd_b200.serve (C ABI batch API, host wall clock "
+                       "from the first arrival to the last completion; job inputs uploaded at "
+                       "admission, final positions read at completion)"},
+        "roofline": None,
+        "cpu_baseline": cpu,
+        "gpu_launches": None,
+        "clocks": clocks,
+    }
+
+
+def cpu_reference(cfgs, steps, what_sample):
     """The reference's CPU path on one host core (the reference has no threading
-    on this path), timed on a bounded sample from the start of the run.
+    on this path), timed on a bounded sample from the start of each run.
 
     Preferred: the reference's own C++ (src/ compiled unmodified by oracle/Makefile;
     CoulombPME against the FFTW-API shim, since FFTW3 is not installed), stepped
@@ -271,48 +559,95 @@ def cpu_reference(cfg, n_atoms, steps):
     present, the oracle's restatement of the same algorithm (REF profile)."""
     from oracle.oracle import Oracle, Ref, ref_available
     if ref_available():
-        eng, kind = Ref().engine(cfg), "reference"
+        make, kind = (lambda c: Ref().engine(c)), "reference"
         what = "reference C++ (src/, unmodified; PME via the FFTW-API shim)"
     else:
-        eng, kind = Oracle().engine(cfg, "ref", brute_list=True), "port"
+        make, kind = (lambda c: Oracle().engine(c, "ref", brute_list=True)), "port"
         what = "oracle restatement of the reference algorithm (REF profile)"
-    t0 = time.perf_counter()
-    eng.step(steps)
-    dt = time.perf_counter() - t0
-    return {"value": round(n_atoms * steps / dt, 1), "unit": "atom-steps/s", "cores": 1,
+    atom_steps, secs = 0, 0.0
+    for cfg in cfgs:
+        eng = make(cfg)
+        t0 = time.perf_counter()
+        eng.step(steps)
+        secs += time.perf_counter() - t0
+        atom_steps += len(cfg.masses) * steps
+    return {"value": round(atom_steps / secs, 1), "unit": "atom-steps/s", "cores": 1,
             "kind": kind,
-            "sample": f"{steps} MD steps of the same 30,000-atom water box from the start "
-                      f"({what}; includes {(steps + 4) // 5} O(N^2) list rebuilds), {dt:.1f} s"}
+            "sample": f"{steps} MD steps from the start of {what_sample} ({what}; includes "
+                      f"{(steps + 4) // 5} O(N^2) list rebuilds per system), {secs:.1f} s"}
 
 
 def run_reference(args):
     ws, rank, _ = _dist()
     if rank != 0:
         return None
-    w = workload(0)
-    cfg = w.config()
+    if args.workload in SINGLE:
+        w = SINGLE[args.workload]["make"](0)
+        cfgs = [w.config()]
+        what = f"the same {w.n_atoms:,}-atom system"
+    elif args.workload == "batch256":
+        from dmd_b200 import workloads as W
+        ws_ = W.batch_256(seed=1234)
+        cfgs = [ws_[k].config() for k in (0, 1, 192)]
+        what = "replicas 0, 1 (LJ) and 192 (decane) of the 256-replica batch"
+    else:
+        from dmd_b200.serve import job_mix
+        jobs = [j for j in job_mix(args.jobs, args.rate, seed=2025, scale=args.scale)
+                if j.n_atoms <= 20000][:2]
+        cfgs = [j.cfg for j in jobs]
+        what = "two jobs of the served stream"
     steps = min(args.steps, args.cpu_steps)
-    cpu = cpu_reference(cfg, w.n_atoms, steps)
+    if sum(len(c.masses) for c in cfgs) > CPU_MAX_ATOMS:
+        return {"impl": "reference", "metric": "atom-steps/s", "value": None,
+                "unit": "atom-steps/s", "n_gpus": ws,
+                "unavailable": "the reference's O(N^2) pair-list build of this system alone "
+                               "takes hours on one core; not timed"}
+    cpu = cpu_reference(cfgs, steps, what)
     v = cpu["value"]
     return {"impl": "reference", "metric": "atom-steps/s", "value": v, "unit": "atom-steps/s",
             "n_gpus": ws, "steps": steps, "warmup": 0, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "water_30k_nvt_pme64", "n_atoms": w.n_atoms, "profile": "ref",
+            "config": {"workload": args.workload, "n_atoms": sum(len(c.masses) for c in cfgs),
+                       "profile": "ref",
                        "implementation": cpu["sample"].split("(")[1].split(";")[0],
                        "sample_steps": steps},
             "cpu_baseline": cpu,
             "e2e": {"value": v, "unit": "atom-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+def run_ours(args):
+    ws, rank, local = _dist()
+    R = Ranks(local)
+    try:
+        if args.workload in SINGLE:
+            return run_single(args, R)
+        if args.workload == "batch256":
+            return run_batch(args, R)
+        return run_serve(args, R)
+    finally:
+        R.close()
+
+
+DEFAULT_STEPS = {"water30k": 2000, "argon4k": 2000, "water750k": 200, "batch256": 200, "serve": 10}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=WORKLOADS, default="water30k")
     ap.add_argument("--cpu-steps", type=int, default=10)
     ap.add_argument("--skip-cpu", action="store_true")
+    # served stream
+    ap.add_argument("--jobs", type=int, default=24)
+    ap.add_argument("--rate", type=float, default=2.0, help="Poisson arrivals (jobs/s)")
+    ap.add_argument("--scale", type=float, default=1.0, help="shrinks job sizes and steps")
+    ap.add_argument("--chunk", type=int, default=100, help="steps per device call")
     args = ap.parse_args()
+    if args.steps is None:
+        args.steps = DEFAULT_STEPS[args.workload]
     if args.warmup < 3:
         args.warmup = 3
     out = run_reference(args) if args.impl == "reference" else run_ours(args)

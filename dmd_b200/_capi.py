@@ -96,6 +96,7 @@ def lib() -> C.CDLL:
     sig = {
         "dmdgpu_create": (C.c_int, [C.POINTER(dmdgpu_system), C.POINTER(dmdgpu_options), C.POINTER(vp)]),
         "dmdgpu_step": (C.c_int, [vp, C.c_int32]),
+        "dmdgpu_repack": (C.c_int, [vp]),
         "dmdgpu_run": (C.c_int, [vp]),
         "dmdgpu_get_state": (C.c_int, [vp, C.c_int32, _dp, _dp, _dp]),
         "dmdgpu_set_state": (C.c_int, [vp, C.c_int32, _dp, _dp, _dp]),
@@ -115,6 +116,7 @@ def lib() -> C.CDLL:
         "dmdgpu_batch_create": (C.c_int, [C.c_int64, C.POINTER(dmdgpu_options), C.POINTER(vp)]),
         "dmdgpu_batch_admit": (C.c_int, [vp, C.POINTER(dmdgpu_system), C.c_int64, C.POINTER(C.c_int32)]),
         "dmdgpu_batch_step": (C.c_int, [vp, C.c_int32]),
+        "dmdgpu_batch_step_timed": (C.c_int, [vp, C.c_int32, C.c_int64, C.POINTER(dmdgpu_timing)]),
         "dmdgpu_batch_poll": (C.c_int, [vp, _ip, C.c_int32, C.POINTER(C.c_int32)]),
         "dmdgpu_batch_get_state": (C.c_int, [vp, C.c_int32, C.c_int32, _dp, _dp, _dp]),
         "dmdgpu_batch_get_scalars": (C.c_int, [vp, C.c_int32, C.POINTER(dmdgpu_scalars)]),

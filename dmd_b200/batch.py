@@ -78,6 +78,14 @@ class Batch:
         """Advance every running slot by up to n steps (each stops at its own target)."""
         self._check(self._lib.dmdgpu_batch_step(self._h, int(n)))
 
+    def step_timed(self, n: int, l2_flush_bytes: int = 0) -> dict:
+        """step(n) as one CUDA graph with device timing of every step and of every
+        non-bonded / PME launch (optional L2 flush between steps)."""
+        t = _capi.dmdgpu_timing()
+        self._check(self._lib.dmdgpu_batch_step_timed(self._h, int(n), int(l2_flush_bytes),
+                                                      C.byref(t)))
+        return {k: getattr(t, k) for k, _ in t._fields_}
+
     def poll(self) -> list[int]:
         """Slots that reached their step target since the last poll."""
         cap = max(1, len(self._n))

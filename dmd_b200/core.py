@@ -299,6 +299,13 @@ class Engine:
         """cudaStream_t (as an integer) every launch of this engine is issued on."""
         return int(self._lib.dmdgpu_stream(self._h) or 0)
 
+    def repack(self):
+        """Rebuild the device table with the state carried over bit for bit (pair
+        list rebuilt, forces evaluated again at the current positions): what a
+        running slot of a Batch goes through when another slot is admitted or
+        released."""
+        self._check(self._lib.dmdgpu_repack(self._h))
+
     def step_timed(self, steps: int, l2_flush_bytes: int = 0) -> dict:
         """Advance `steps` steps as one CUDA graph with device timing of every step
         and of every non-bonded / PME launch (optional L2 flush between steps)."""

@@ -261,6 +261,12 @@ int64_t dmdgpu_footprint_bytes(const dmdgpu_system* sys, const dmdgpu_options* o
     }
 }
 
+int dmdgpu_repack(dmdgpu_ctx* c) {
+    if (!c || !c->b) return DMDGPU_ERR_INVALID;
+    int rc = c->b->repack();
+    return rc ? ctx_fail(c, rc) : DMDGPU_OK;
+}
+
 int64_t dmdgpu_kernel_launches(dmdgpu_ctx* c) { return (c && c->b) ? c->b->launches() : 0; }
 
 void* dmdgpu_stream(dmdgpu_ctx* c) { return (c && c->b) ? static_cast<void*>(c->b->stream()) : nullptr; }
@@ -307,6 +313,13 @@ int dmdgpu_batch_admit(dmdgpu_batch* b, const dmdgpu_system* sys, int64_t n_step
 int dmdgpu_batch_step(dmdgpu_batch* b, int32_t n) {
     if (!b || !b->b) return DMDGPU_ERR_INVALID;
     int rc = b->b->step(n);
+    if (rc) b->err = b->b->error();
+    return rc;
+}
+
+int dmdgpu_batch_step_timed(dmdgpu_batch* b, int32_t n, int64_t flush_bytes, dmdgpu_timing* out) {
+    if (!b || !b->b || n <= 0 || !out) return DMDGPU_ERR_INVALID;
+    int rc = b->b->step_timed(n, flush_bytes, out);
     if (rc) b->err = b->b->error();
     return rc;
 }

@@ -352,8 +352,14 @@ int Batch::add(const dmdgpu_system& in, long long n_steps, unsigned comp_mask, i
     int rc = build_host(*hr, comp_mask);
     if (rc) return rc;
     hr->target = n_steps;
-    if (budget_ > 0 && used_bytes_ + footprint(s) > budget_)
-        return fail(DMDGPU_ERR_BUDGET, "HBM budget exceeded");
+    if (budget_ > 0) {
+        // admitted systems count from admission on, packed or not yet
+        long long committed = 0;
+        for (const auto& r : reps_)
+            if (r) committed += footprint(r->sys);
+        if (std::max(used_bytes_, committed) + footprint(s) > budget_)
+            return fail(DMDGPU_ERR_BUDGET, "HBM budget exceeded");
+    }
     // reuse a free slot id
     int slot = -1;
     for (size_t k = 0; k < reps_.size(); ++k)
@@ -375,6 +381,15 @@ int Batch::release(int slot) {
     return DMDGPU_OK;
 }
 
+// What a running replica goes through when another slot is admitted or released:
+// the table is rebuilt with its state carried over bit for bit, its pair list is
+// rebuilt and its forces are evaluated again at the same positions.
+int Batch::repack() {
+    CK(cudaSetDevice(device_));
+    packed_ = false;
+    return pack();
+}
+
 int Batch::replica_index(int slot) const {
     for (size_t k = 0; k < order_.size(); ++k)
         if (order_[k] == slot) return static_cast<int>(k);
@@ -393,7 +408,9 @@ int Batch::pack() {
         CK(cudaMemcpyAsync(h_st_, d_st_, sizeof(RepState) * order_.size(), cudaMemcpyDeviceToHost, stream_));
         CK(cudaStreamSynchronize(stream_));
         for (size_t k = 0; k < order_.size(); ++k) {
-            if (!reps_[order_[k]]) continue;
+            // a released slot may already hold a newly admitted system: only
+            // replicas that were packed carry device state over
+            if (!reps_[order_[k]] || !reps_[order_[k]]->on_device) continue;
             HostRep& o = *reps_[order_[k]];
             HostSystem& s = o.sys;
             const int a0 = o.rep.atom_begin, n = s.n;
@@ -407,6 +424,7 @@ int Batch::pack() {
             st.rebuild = 1;          // slots change: rebuild every list
             st.have_forces = 0;      // forces are recomputed at the same positions
             st.n_chunks = 0;
+            st.green_L = 0.0;        // the new arena holds no PME influence function yet
             o.init = st;
         }
     }
@@ -455,14 +473,17 @@ int Batch::pack() {
         n_excl += s.ei.size();
         if (P.flags & F_PME) {
             const int K = P.pme_K;
+            // every replica's meshes start on a 64-element boundary: cuFFT reads a
+            // real array that is not 8-byte aligned (odd K^3 offsets) incorrectly
+            auto align64 = [](long long v) { return (v + 63) & ~63LL; };
             P.mesh_fix_off = mesh_fix;
             P.mesh_fix_n = phys_ ? static_cast<long long>(K) * K * K
                                  : static_cast<long long>(K) * K * 2 * (K / 2 + 1);
-            mesh_fix += P.mesh_fix_n;
+            mesh_fix = align64(mesh_fix + P.mesh_fix_n);
             P.mesh_real_off = mesh_real;
-            mesh_real += static_cast<long long>(K) * K * K + 64;
+            mesh_real = align64(mesh_real + static_cast<long long>(K) * K * K + 64);
             P.mesh_cplx_off = mesh_cplx;
-            mesh_cplx += static_cast<long long>(K) * K * (K / 2 + 1) + 64;
+            mesh_cplx = align64(mesh_cplx + static_cast<long long>(K) * K * (K / 2 + 1) + 64);
             P.bsp_off = static_cast<int>(n_bsp);
             n_bsp += K;
             P.pme_block_begin = pme_blocks;
@@ -773,6 +794,7 @@ int Batch::pack() {
         cufftSetStream(b, aux_stream_);
         plans_[K] = {f, b};
     }
+    for (int k : order_) reps_[k]->on_device = true;
     packed_ = true;
     graph_dirty_ = true;
     return DMDGPU_OK;
@@ -863,7 +885,7 @@ void Batch::enqueue_step() {
     enqueue_eval(PASS_SECOND);
     launch_kick2(dev_, any_andersen_ref_, any_andersen_phys_, stream_, &launches_);
     launch_replica_update(dev_, stream_, &launches_);
-    if (any_baro_) launch_apply_scale(dev_, fp64_, stream_, &launches_);
+    if (any_baro_ && !phys_) launch_apply_scale(dev_, fp64_, stream_, &launches_);
 }
 
 // AndersenThermostat::apply (andersen.cpp:14-32): the REF profile reproduces the
@@ -907,7 +929,7 @@ int Batch::run_steps(int n) {
         for (int i = 0; i < n; ++i) {
             enqueue_step();
             CK(cudaGetLastError());
-            if (i == 0) need_eval1_ = any_baro_ || any_ref_lj_;
+            if (i == 0) need_eval1_ = (any_baro_ && !phys_) || any_ref_lj_;
         }
         graph_dirty_ = true;
         return DMDGPU_OK;
@@ -928,7 +950,7 @@ int Batch::run_steps(int n) {
         need_eval1_ = true;
         enqueue_step();
         CK(cudaGetLastError());
-        need_eval1_ = any_baro_ || any_ref_lj_;
+        need_eval1_ = (any_baro_ && !phys_) || any_ref_lj_;
         --n;
         if (graph_) cudaGraphExecDestroy(graph_);
         graph_ = nullptr;
@@ -1363,8 +1385,9 @@ int Batch::save_checkpoint(int slot, const char* path) {
     os.write(reinterpret_cast<const char*>(h.sys.type.data()), 4 * n);
     int32_t ljc = sc.lj_step_since_rebuild;
     os.write(reinterpret_cast<const char*>(&ljc), 4);
-    // trailer: box, Nose-Hoover zeta, Andersen call counter, profile
-    uint32_t tv = 2;
+    // trailer: box, Nose-Hoover zeta, Andersen call counter, profile and (v3)
+    // the PHYS barostat scale still to be applied with the next drift
+    uint32_t tv = 3;
     double box = sc.box, zeta = sc.zeta;
     int k = replica_index(slot);
     int64_t acalls = h_st_[k].andersen_calls;
@@ -1377,6 +1400,8 @@ int Batch::save_checkpoint(int slot, const char* path) {
     os.write(reinterpret_cast<const char*>(&acalls), 8);
     os.write(reinterpret_cast<const char*>(&aseed), 4);
     os.write(reinterpret_cast<const char*>(&prof), 4);
+    double pscale = phys_ ? h_st_[k].pscale : 1.0;
+    os.write(reinterpret_cast<const char*>(&pscale), 8);
     return os.good() ? DMDGPU_OK : fail(DMDGPU_ERR_PARM, "checkpoint write failed");
 }
 
@@ -1417,6 +1442,7 @@ int Batch::load_checkpoint(int slot, const char* path) {
     int64_t acalls = 0;
     uint32_t aseed = 42;
     int32_t prof = -1;
+    double pscale = 1.0;
     bool trailer = false;
     if (is.read(reinterpret_cast<char*>(&tmagic), 4) && tmagic == TR_MAGIC) {
         is.read(reinterpret_cast<char*>(&tv), 4);
@@ -1426,6 +1452,7 @@ int Batch::load_checkpoint(int slot, const char* path) {
         is.read(reinterpret_cast<char*>(&aseed), 4);
         is.read(reinterpret_cast<char*>(&prof), 4);
         trailer = static_cast<bool>(is);
+        if (trailer && tv >= 3 && !is.read(reinterpret_cast<char*>(&pscale), 8)) pscale = 1.0;
     }
     const int k = replica_index(slot);
     const int a0 = h.rep.atom_begin;
@@ -1451,6 +1478,7 @@ int Batch::load_checkpoint(int slot, const char* path) {
         st.zeta = zeta;
         st.andersen_calls = acalls;
         h.andersen_seed = aseed;
+        st.pscale = phys_ ? pscale : 1.0;
     }
     CK(cudaMemcpy(d_st_ + k, &st, sizeof(RepState), cudaMemcpyHostToDevice));
     h.target = st.step;

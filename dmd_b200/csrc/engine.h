@@ -57,6 +57,7 @@ struct HostRep {
     unsigned andersen_seed = 42;
     bool done = false;
     bool polled = false;
+    bool on_device = false;    // packed into the current device table (its state lives there)
 };
 
 struct DeviceArena {
@@ -76,6 +77,7 @@ class Batch {
     int add(const dmdgpu_system& sys, long long n_steps, unsigned comp_mask, int* slot);
     int release(int slot);
     int pack();                 // (re)build the packed device table from host replicas
+    int repack();               // rebuild the table now, carrying every replica's state
     long long footprint(const HostSystem& s) const;
 
     int step(int n);            // advance every running replica by up to n steps

@@ -308,8 +308,9 @@ template <typename T>
 __global__ void k_pme_convert(Dev d, long long n_fix) {
     const long long e = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (e >= n_fix) return;
-    // replica of fixed-mesh element e: linear scan over the (few) PME replicas
-    int r = 0;
+    // replica of fixed-mesh element e: linear scan over the (few) PME replicas;
+    // elements in the alignment gaps between replica meshes belong to none
+    int r = -1;
     for (int k = 0; k < d.n_rep; ++k) {
         const Rep& R = d.rep[k];
         if ((R.flags & F_PME) && e >= R.mesh_fix_off && e < R.mesh_fix_off + R.mesh_fix_n) {
@@ -317,6 +318,7 @@ __global__ void k_pme_convert(Dev d, long long n_fix) {
             break;
         }
     }
+    if (r < 0) return;
     const Rep& R = d.rep[r];
     if (!d.st[r].eval) return;
     const int loc = static_cast<int>(e - R.mesh_fix_off);  // meshes are < 2^31 points

@@ -5,15 +5,21 @@
 // Device form (per step, every replica of the batch in the same launches):
 //   k_step_begin        which replicas advance
 //   [eval #1]           only where the first evaluation would differ from the
-//                       previous step's second one (barostat moved the atoms,
+//                       previous step's second one (REF barostat moved the atoms,
 //                       no forces yet, or the REF list cadence rebuilds now)
-//   k_kick_drift        pending thermostat scale, half kick, drift, clear forces,
-//                       write the sorted FP32/FP64 mirror, skin check
-//   [eval #2]
+//   k_kick_drift        pending thermostat scale, half kick, PHYS pending
+//                       barostat scale, drift, clear forces, write the sorted
+//                       FP32/FP64 mirror, skin check
+//   [eval #2]           (its k_eval_begin scales the PHYS box to match)
 //   k_kick2             half kick (+ Andersen), per-tile KE / virial partials
 //   k_replica_update    KE, thermostat (Berendsen / Nose-Hoover scale, applied
 //                       lazily in the next kick), Berendsen barostat factor
-//   k_apply_scale       barostat position scaling (only when a barostat exists)
+//                       (REF: applied now; PHYS: pending for the next drift)
+//   k_apply_scale       REF barostat position scaling (only when a barostat exists)
+// PHYS therefore evaluates forces once per step with or without a barostat:
+// the first kick of a step uses the forces of the previous evaluation and the
+// scaling is applied with the drift, so every evaluation sees the positions
+// the next kick is for.
 // Integration arithmetic is FP64 with the reference's operation order
 // (src/integrate/integrator.cpp:4-20) and no FMA contraction.
 #include "device.cuh"
@@ -28,7 +34,10 @@ __global__ void k_step_begin(Dev d) {
     if (r >= d.n_rep) return;
     RepState* s = d.st + r;
     s->active = (s->step < s->target_step) ? 1 : 0;
-    s->pscale = 1.0;
+    // PHYS keeps the barostat scale chosen at the end of the previous step: it is
+    // applied to the positions by k_kick_drift and to the box by k_eval_begin
+    // (second pass), so an evaluation before the drift sees the unscaled pair.
+    if (!(d.rep[r].flags & F_PHYS)) s->pscale = 1.0;
 }
 
 __global__ void k_eval_begin(Dev d, int pass) {
@@ -43,12 +52,19 @@ __global__ void k_eval_begin(Dev d, int pass) {
     const bool ref_lj = !(R.flags & F_PHYS) && (R.flags & F_LJ);
     int ev;
     if (pass == PASS_FIRST) {
-        ev = s->active && (R.barostat != 0 || !s->have_forces || (ref_lj && s->lj_counter >= 10));
+        ev = s->active && ((R.barostat != 0 && !(R.flags & F_PHYS)) || !s->have_forces ||
+                           (ref_lj && s->lj_counter >= 10));
         // LennardJones::compute advances its counter on every call (lennard_jones.cpp:91)
         if (s->active && !ev && ref_lj) s->lj_counter += 1;
     } else if (pass == PASS_SECOND) {
         ev = s->active;
         s->vscale = 1.0;  // consumed by k_kick_drift
+        if (s->active && (R.flags & F_PHYS) && s->pscale != 1.0) {
+            // the box follows the positions k_kick_drift has just scaled
+            s->L *= s->pscale;
+            s->invL = 1.0 / s->L;
+            s->pscale = 1.0;
+        }
     } else {
         ev = 1;
     }
@@ -119,7 +135,10 @@ __device__ __forceinline__ void skin_check(const Dev& d, RepState* s, const Rep&
 }
 
 // Integrator::half_kick + advance (integrator.cpp:4-20), with the pending
-// thermostat scale of the previous step applied first.
+// thermostat scale of the previous step applied first.  PHYS with a barostat:
+// the pending position scale s (1 otherwise, an exact multiply) is applied
+// before the drift, x <- s x + v dt, and the mirror is written for the box
+// s L that k_eval_begin stores next.
 __global__ void k_kick_drift(Dev d) {
     const int slot = blockIdx.x * blockDim.x + threadIdx.x;
     if (slot >= d.n_slots) return;
@@ -139,9 +158,10 @@ __global__ void k_kick_drift(Dev d) {
     vx = __dadd_rn(vx, __dmul_rn(__dmul_rn(fx, inv_mass), half_dt));
     vy = __dadd_rn(vy, __dmul_rn(__dmul_rn(fy, inv_mass), half_dt));
     vz = __dadd_rn(vz, __dmul_rn(__dmul_rn(fz, inv_mass), half_dt));
-    const double x = __dadd_rn(d.x[a], __dmul_rn(vx, dt));
-    const double y = __dadd_rn(d.y[a], __dmul_rn(vy, dt));
-    const double z = __dadd_rn(d.z[a], __dmul_rn(vz, dt));
+    const double sc = s->pscale;
+    const double x = __dadd_rn(__dmul_rn(d.x[a], sc), __dmul_rn(vx, dt));
+    const double y = __dadd_rn(__dmul_rn(d.y[a], sc), __dmul_rn(vy, dt));
+    const double z = __dadd_rn(__dmul_rn(d.z[a], sc), __dmul_rn(vz, dt));
     d.vx[a] = vx;
     d.vy[a] = vy;
     d.vz[a] = vz;
@@ -154,7 +174,7 @@ __global__ void k_kick_drift(Dev d) {
     d.fbx[a] = 0;
     d.fby[a] = 0;
     d.fbz[a] = 0;
-    write_mirror(d, slot, a, x, y, z, s->L);
+    write_mirror(d, slot, a, x, y, z, s->L * sc);
     skin_check(d, s, R, a, x, y, z);
 }
 
@@ -327,8 +347,10 @@ __global__ void k_replica_update(Dev d) {
         if (mu <= 0.0) mu = 0.0;
         const double sc = cbrt(mu);
         s->pscale = sc;
-        s->L = L * sc;
-        s->invL = 1.0 / s->L;
+        if (!(R.flags & F_PHYS)) {  // REF: positions and box scale now (k_apply_scale)
+            s->L = L * sc;
+            s->invL = 1.0 / s->L;
+        }
     }
     s->step += 1;
     s->time += dt;

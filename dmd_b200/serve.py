@@ -43,6 +43,9 @@ class Job:
     admitted: float = math.nan
     done: float = math.nan
     result: dict = dataclasses.field(default_factory=dict)
+    steps_done: int = 0
+    packed: bool = False           # in the device table (admitted before the last device call)
+    repacks: list = dataclasses.field(default_factory=list)  # own step counts at table rebuilds
 
 
 def job_mix(n_jobs: int, rate: float, seed: int = 2025, scale: float = 1.0):
@@ -80,6 +83,7 @@ def serve(jobs, budget_bytes=150 * 10**9, precision="mixed", profile="phys", chu
     t0 = time.perf_counter()
     clock_steps = 0
     atom_steps = 0
+    dirty = False              # a slot was admitted or released since the last device call
 
     def now():
         return float(clock_steps) if virtual else time.perf_counter() - t0
@@ -97,6 +101,7 @@ def serve(jobs, budget_bytes=150 * 10**9, precision="mixed", profile="phys", chu
             j.admitted = now()
             running[j.slot] = j
             queue.pop(0)
+            dirty = True
         if not running:
             if virtual:
                 clock_steps = int(math.ceil(queue[0].arrival))
@@ -104,12 +109,22 @@ def serve(jobs, budget_bytes=150 * 10**9, precision="mixed", profile="phys", chu
                 time.sleep(max(0.0, queue[0].arrival - now()))
             continue
         live = sum(j.n_atoms for j in running.values())
+        if dirty:
+            # the device table is rebuilt at this call: running jobs carry their
+            # state over and rebuild their pair lists (Engine.repack alone)
+            for j in running.values():
+                if j.packed:
+                    j.repacks.append(j.steps_done)
+            dirty = False
         t = time.perf_counter()
         b.step(chunk)
         dt = time.perf_counter() - t
         step_lat.append(dt / chunk)
         clock_steps += chunk
         atom_steps += live * chunk
+        for j in running.values():
+            j.packed = True
+            j.steps_done = min(j.n_steps, j.steps_done + chunk)
         for slot in b.poll():
             j = running.pop(slot)
             j.done = now()
@@ -117,6 +132,7 @@ def serve(jobs, budget_bytes=150 * 10**9, precision="mixed", profile="phys", chu
             j.result = {"positions": b.positions(slot), "potential_energy": s.potential_energy,
                         "step": int(s.step)}
             b.release(slot)
+            dirty = True
     wall = time.perf_counter() - t0
     done = [j.done - j.arrival for j in jobs]
     done_steps = sum(j.n_atoms * j.n_steps for j in jobs)
@@ -131,6 +147,25 @@ def serve(jobs, budget_bytes=150 * 10**9, precision="mixed", profile="phys", chu
         "work_atom_steps": done_steps,
         "padded_atom_steps": atom_steps,
     }
+
+
+def run_alone(job: Job, precision="mixed", profile="phys", device=None):
+    """The same job in an engine of its own, with its table rebuilt at the same
+    steps as in the stream (Engine.repack): positions, velocities, potential
+    energy.  Fixed-point force sums and per-replica reductions make this equal
+    to the job's result in the mix, bit for bit."""
+    from .core import Engine
+    e = Engine(job.cfg, precision=precision, profile=profile, device=device)
+    done = 0
+    for at in job.repacks:
+        if at > done:
+            e.run_n(at - done)
+            done = at
+        e.repack()
+    e.run_n(job.n_steps - done)
+    out = e.positions, e.velocities, e.potential_energy
+    e.close()
+    return out
 
 
 def main():

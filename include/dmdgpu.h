@@ -181,6 +181,14 @@ int dmdgpu_load_checkpoint(dmdgpu_ctx *ctx, const char *path);
 /* Device bytes a context for this system would hold (admission accounting). */
 int64_t dmdgpu_footprint_bytes(const dmdgpu_system *sys, const dmdgpu_options *opt);
 
+/* Rebuild this context's device table with its state carried over bit for bit:
+ * the pair list is rebuilt and forces are evaluated again at the current
+ * positions before the next step.  This is what a running slot of a batch goes
+ * through when another slot is admitted or released, so a system run alone with
+ * dmdgpu_repack at the same steps reproduces its batched trajectory exactly.
+ * No counterpart in the reference. */
+int dmdgpu_repack(dmdgpu_ctx *ctx);
+
 /* Kernel launches issued by this context so far (this library's own kernels). */
 int64_t dmdgpu_kernel_launches(dmdgpu_ctx *ctx);
 
@@ -222,6 +230,11 @@ int dmdgpu_batch_create(int64_t budget_bytes, const dmdgpu_options *opt, dmdgpu_
 int dmdgpu_batch_admit(dmdgpu_batch *b, const dmdgpu_system *sys, int64_t n_steps, int32_t *slot);
 /* Advance every running slot by up to n_steps (a slot stops at its own n_steps). */
 int dmdgpu_batch_step(dmdgpu_batch *b, int32_t n_steps);
+/* dmdgpu_batch_step with device timing, as dmdgpu_step_timed does for one
+ * context (one CUDA graph, events around every step and every non-bonded / PME
+ * launch, optional L2 flush between steps); slots stop at their own targets. */
+int dmdgpu_batch_step_timed(dmdgpu_batch *b, int32_t n_steps, int64_t l2_flush_bytes,
+                            dmdgpu_timing *out);
 /* Slots that finished since the last poll: copies up to cap ids into slots. */
 int dmdgpu_batch_poll(dmdgpu_batch *b, int32_t *slots, int32_t cap, int32_t *n_done);
 int dmdgpu_batch_get_state(dmdgpu_batch *b, int32_t slot, int32_t which, double *x, double *y,

@@ -817,6 +817,7 @@ struct OrcEngine {
     unsigned int andersen_seed{42};
     orc_energy e{};
     bool have_forces{false};
+    double pscale{1.0};  // phys: barostat scale chosen at the end of a step, applied with the next drift
 };
 
 void* orc_engine_create(const orc_system* s, const orc_run* r) {
@@ -1049,8 +1050,25 @@ void eng_barostat(OrcEngine* E) {  // berendsen_barostat.cpp:14-66
     }
     if (mu <= 0.0) mu = 0.0;
     double sc = std::cbrt(mu);
+    if (E->s.profile == 1) {  // phys: applied with the next step's drift (eng_apply_pending_scale)
+        E->pscale = sc;
+        return;
+    }
     for (size_t i = 0; i < n; ++i) { E->x[i] *= sc; E->y[i] *= sc; E->z[i] *= sc; }
     E->L *= sc;
+}
+
+// phys correction of Q13 with a barostat: the reference scales positions and box
+// at the end of a step and evaluates forces twice in the next one; here the
+// scale waits for the next drift, so the first kick of a step uses the forces of
+// the previous evaluation and the single evaluation of the step sees the scaled
+// positions.
+void eng_apply_pending_scale(OrcEngine* E) {
+    if (E->pscale == 1.0) return;
+    const double sc = E->pscale;
+    for (size_t i = 0; i < E->m.size(); ++i) { E->x[i] *= sc; E->y[i] *= sc; E->z[i] *= sc; }
+    E->L *= sc;
+    E->pscale = 1.0;
 }
 
 }  // namespace
@@ -1058,14 +1076,16 @@ void eng_barostat(OrcEngine* E) {  // berendsen_barostat.cpp:14-66
 extern "C" {
 
 // SimulationEngine::step (simulation_engine.cpp:53-86).  The phys profile skips the
-// first evaluation when it would repeat the previous step's second one (no barostat),
-// which does not change any result because phys forces depend on positions only.
+// first evaluation when it would repeat the previous step's second one, which does
+// not change any result because phys forces depend on positions only; with a
+// barostat it applies the pending scale before the drift (eng_apply_pending_scale).
 void orc_engine_step(void* h, int nsteps) {
     auto* E = static_cast<OrcEngine*>(h);
     for (int it = 0; it < nsteps; ++it) {
-        bool skip = (E->s.profile == 1) && E->have_forces && E->run.barostat == 0;
+        bool skip = (E->s.profile == 1) && E->have_forces;
         if (!skip) eng_compute(E);
         eng_half_kick(E);
+        if (E->s.profile == 1) eng_apply_pending_scale(E);
         eng_advance(E);
         eng_compute(E);
         eng_half_kick(E);

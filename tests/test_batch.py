@@ -2,12 +2,12 @@
 
 A slot's result must be the same alone and in the mix.  The batch shares kernel
 launches, not arithmetic (fixed-point force sums, per-replica reductions in a
-fixed order), so a fixed mix is compared bitwise.  Admitting or releasing a job
-repacks the table and rebuilds every running replica's pair list at that step;
-in the mixed path the FP32 tile-local coordinates then round differently than
-in a run alone (pair sets stay exact), so jobs that lived through a repack are
-held to the mixed-precision tolerance instead: positions within 1e-5 nm,
-potential energy within 1e-5 relative.
+fixed order), so results are compared bit for bit.  Admitting or releasing a
+job rebuilds the device table: every running replica carries its state over,
+rebuilds its pair list and evaluates its forces again at the same positions.
+In the mixed path the rebuilt list's FP32 tile frame rounds differently from
+the frame it replaces, so the reference run alone goes through the same
+rebuilds at the same steps (Engine.repack) -- and is then identical bit for bit.
 """
 import numpy as np
 import pytest
@@ -15,25 +15,30 @@ import pytest
 from dmd_b200 import workloads as W
 
 pytestmark = pytest.mark.gpu
-POS_TOL = 1e-5  # nm, for jobs that lived through a repack (see above)
 
 
 def _mix():
-    """Uneven LJ fluids, decane melts and two water boxes with different PME meshes."""
+    """Uneven LJ fluids, decane melts and four water boxes with different PME
+    meshes (K = 20, 24, 23, 21: odd K^3 mesh sizes next to each other)."""
     cfgs = [W.lj_fluid(600, 0.65, 1.2, 11).config(), W.lj_fluid(1500, 0.80, 0.9, 12).config(),
             W.lj_fluid(2600, 0.72, 1.4, 13).config(), W.decane_melt(12, 14).config(),
             W.decane_melt(20, 15).config()]
-    for n_mol, seed in ((300, 16), (500, 17)):
+    for n_mol, seed in ((300, 16), (500, 17), (450, 18), (360, 19)):
         box = (n_mol / 33.43) ** (1 / 3)
         cfgs.append(W.water_box(n_mol=n_mol, box=box, seed=seed,
                                 spacing=box / round(box / 0.1045)).config())
     return cfgs
 
 
-def _alone(cfg, steps, precision):
+def _alone(cfg, steps, precision, repacks=()):
     from dmd_b200.core import Engine
     e = Engine(cfg, precision=precision, profile="phys")
-    e.run_n(steps)
+    done = 0
+    for at in repacks:
+        e.run_n(at - done)
+        done = at
+        e.repack()
+    e.run_n(steps - done)
     return e.positions, e.velocities, e.potential_energy
 
 
@@ -56,25 +61,29 @@ def test_batch_matches_alone(precision):
 
 def test_serving_admit_and_release_midway():
     """Continuous batching: B arrives while A runs, C after A is released; every
-    result equals the same job run alone."""
+    result equals the same job run alone with its table rebuilt at the same steps."""
     from dmd_b200.batch import Batch
     cfgs = _mix()
     a_cfg, b_cfg, c_cfg = cfgs[1], cfgs[5], cfgs[3]
     b = Batch(precision="mixed", profile="phys")
     a = b.admit(a_cfg, 25)
     b.step(10)
-    s_b = b.admit(b_cfg, 20)          # repack while A is mid-run
+    s_b = b.admit(b_cfg, 20)          # repack while A is mid-run (A at step 10)
     b.step(15)                        # A done at 25, B at 15
     assert b.poll() == [a]
-    pa = b.positions(a)
+    pa, pe_a = b.positions(a), b.scalars(a).potential_energy
     b.release(a)
-    s_c = b.admit(c_cfg, 12)          # C takes the freed memory
+    s_c = b.admit(c_cfg, 12)          # C takes the freed slot id and memory (B at step 15)
+    assert s_c == a
     b.step(12)                        # B done at 20 (stops there), C at 12
     assert sorted(b.poll()) == sorted([s_b, s_c])
-    for slot, cfg, n, got in ((a, a_cfg, 25, pa), (s_b, b_cfg, 20, None), (s_c, c_cfg, 12, None)):
-        p, _, _ = _alone(cfg, n, "mixed")
-        got = got if got is not None else b.positions(slot)
-        assert np.abs(got - p).max() < POS_TOL, (slot, np.abs(got - p).max())
+    for cfg, n, reps, got, pe in ((a_cfg, 25, [10], pa, pe_a),
+                                  (b_cfg, 20, [15], b.positions(s_b), b.scalars(s_b).potential_energy),
+                                  (c_cfg, 12, [], b.positions(s_c), b.scalars(s_c).potential_energy)):
+        p, _, pe_alone = _alone(cfg, n, "mixed", reps)
+        assert got.shape == p.shape
+        assert np.array_equal(got, p), (n, np.abs(got - p).max())
+        assert pe == pe_alone
     assert b.active == 0
 
 
@@ -91,14 +100,16 @@ def test_budget_admission():
 
 def test_serve_stream_results_equal_alone():
     """The request loop: jobs arriving over time (virtual clock in steps) are
-    admitted while others run; each result equals the same job run alone."""
-    from dmd_b200.serve import job_mix, serve
+    admitted while others run; each result equals the same job run alone (with
+    its table rebuilt at the same steps), bit for bit."""
+    from dmd_b200.serve import job_mix, run_alone, serve
     jobs = job_mix(6, rate=0.05, seed=7, scale=0.02)
     out = serve(jobs, precision="mixed", profile="phys", chunk=10, virtual=True)
     assert out["jobs"] == 6
     assert out["job_latency"]["p99"] >= out["job_latency"]["p50"] > 0
+    assert any(j.repacks for j in jobs)       # the mix did overlap
     for j in jobs:
         assert j.result["step"] == j.n_steps
-        p, _, pe = _alone(j.cfg, j.n_steps, "mixed")
-        assert np.abs(j.result["positions"] - p).max() < POS_TOL, j.jid
-        assert abs(j.result["potential_energy"] - pe) <= 1e-5 * abs(pe), j.jid
+        p, _, pe = run_alone(j, "mixed", "phys")
+        assert np.array_equal(j.result["positions"], p), (j.jid, np.abs(j.result["positions"] - p).max())
+        assert j.result["potential_energy"] == pe, j.jid

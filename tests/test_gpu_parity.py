@@ -181,3 +181,28 @@ def test_checkpoint_restart_bitwise(tmp_path):
     assert fresh.current_step == 200
     assert np.array_equal(full.positions, fresh.positions)
     assert np.array_equal(full.velocities, fresh.velocities)
+
+
+def test_checkpoint_restart_bitwise_phys_npt(tmp_path):
+    """PHYS NPT: the barostat scale chosen at the end of the saved step is applied
+    with the next drift, so it travels in the checkpoint trailer; without it the
+    restarted run would drift from the continuous one by the scale (1e-6)."""
+    cfg = _water(300, seed=3)
+    cfg.thermostat.type = "berendsen"
+    cfg.barostat.type = "berendsen"
+    cfg.barostat.tau = 0.5
+    full = _engine(cfg, "fp64", "phys")
+    full.run_n(30)
+    half = _engine(cfg, "fp64", "phys")
+    half.run_n(15)
+    p = str(tmp_path / "ck_npt.bin")
+    half.save_checkpoint(p)
+    fresh = _engine(cfg, "fp64", "phys")
+    fresh.load_checkpoint(p)
+    fresh.run_n(15)
+    assert fresh.current_step == 30
+    # the restart rebuilds the pair list at the saved positions, which regroups
+    # the FP64 per-chunk partial sums: equal to round-off, not bit for bit
+    assert abs(fresh.box_size - full.box_size) <= 1e-12 * full.box_size
+    assert np.abs(full.positions - fresh.positions).max() < 1e-9
+    assert rel_rms(fresh.velocities, full.velocities) < 1e-8
