@@ -6,9 +6,10 @@ a step relative to the step's first kernel, so overlap between the main stream
 mean step period and per-kernel totals.
 
     python -m dmd_b200.timeline [--steps 30] [--precision mixed] [--show 3]
+                                [--workload water30k|water750k|argon4k|batch256]
 
-Runs on the headline workload (water 30k NVT, PHYS profile).  A diagnostic:
-numbers printed under a profiler are not benchmark values.
+Runs on the headline workload (water 30k NVT, PHYS profile) by default.  A
+diagnostic: numbers printed under a profiler are not benchmark values.
 """
 from __future__ import annotations
 
@@ -23,6 +24,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--show", type=int, default=3, help="steps printed kernel by kernel")
+    ap.add_argument("--workload", default="water30k",
+                    choices=["water30k", "water750k", "argon4k", "batch256"])
     args = ap.parse_args()
     import torch
     from torch.profiler import ProfilerActivity, profile
@@ -31,14 +34,29 @@ def main():
     from dmd_b200.core import Engine
     from dmd_b200 import workloads as W
 
-    cfg = W.water_box(n_mol=10_000, box=6.69, seed=7, spacing=0.1045, thermostat="nose-hoover",
-                      dt=0.0005).config()
-    eng = Engine(cfg, precision=args.precision, profile="phys")
-    eng.run_n(args.warmup)
-    eng.positions
-    with profile(activities=[ProfilerActivity.CUDA]) as prof:
-        eng.run_n(args.steps)
+    if args.workload == "batch256":
+        from dmd_b200.batch import Batch
+        eng = Batch(precision=args.precision, profile="phys")
+        for w in W.batch_256():
+            eng.admit(w.config(), args.warmup + args.steps)
+        eng.step(args.warmup)
+        with profile(activities=[ProfilerActivity.CUDA]) as prof:
+            eng.step(args.steps)
+    else:
+        if args.workload == "water30k":
+            w = W.water_box(n_mol=10_000, box=6.69, seed=7, spacing=0.1045, thermostat="nose-hoover",
+                            dt=0.0005)
+        elif args.workload == "water750k":
+            w = W.water_box(n_mol=250_000, box=19.56, seed=7, spacing=0.1019, thermostat="berendsen",
+                            barostat="berendsen", dt=0.0005)
+        else:
+            w = W.argon_fcc(n_cells=10, a=0.575, T=120.0, seed=2024, dt=0.002)
+        eng = Engine(w.config(), precision=args.precision, profile="phys")
+        eng.run_n(args.warmup)
         eng.positions
+        with profile(activities=[ProfilerActivity.CUDA]) as prof:
+            eng.run_n(args.steps)
+            eng.positions
     ev = [e for e in prof.events() if e.device_type.name == "CUDA" and "Memcpy" not in e.name]
     ev.sort(key=lambda e: e.time_range.start)
 
