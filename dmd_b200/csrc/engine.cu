@@ -16,7 +16,9 @@
 #include <cstring>
 #include <fstream>
 #include <random>
+#include <mutex>
 #include <stdexcept>
+#include <tuple>
 
 #include "engine.h"
 #include "launch.h"
@@ -58,6 +60,30 @@ void sort_grid(int n, double L, int& nvx, int& nvz) {
     nvz = std::min(std::max(static_cast<int>(std::floor(L / 0.1)), 1), 1024);
 }
 
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Autotuner cache: the pair kernel's launch shape chosen for a kind of batch,
+// shared by every batch of the process (the serving loop repacks often).
+// Key: device, precision, whether a PME chain runs beside the pair kernel, and
+// the batch's atom count in powers of two.
+namespace {
+struct TuneKey {
+    int device, fp64, pme, bucket;
+    bool operator<(const TuneKey& o) const {
+        return std::tie(device, fp64, pme, bucket) < std::tie(o.device, o.fp64, o.pme, o.bucket);
+    }
+};
+std::mutex g_tune_mu;
+std::map<TuneKey, int> g_tune;
+constexpr int kTuneSteps = 6;               // timed steps per candidate
+constexpr int kTuneCand[] = {2, 3};         // pair-kernel blocks per SM
+
+TuneKey tune_key(int device, bool fp64, bool pme, long long n_atoms) {
+    int b = 0;
+    while ((1LL << (b + 1)) <= n_atoms) ++b;
+    return TuneKey{device, fp64 ? 1 : 0, pme ? 1 : 0, b};
+}
 }  // namespace
 
 Batch::Batch(const dmdgpu_options& opt, long long budget) : opt_(opt), budget_(budget) {
@@ -795,6 +821,12 @@ int Batch::pack() {
         plans_[K] = {f, b};
     }
     for (int k : order_) reps_[k]->on_device = true;
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_tune.find(tune_key(device_, fp64_, any_pme_, dev_.n_atoms));
+        tuned_ = fp64_ || it != g_tune.end();
+        nb_blocks_per_sm_ = (it != g_tune.end()) ? it->second : (any_pme_ ? 2 : 3);
+    }
     packed_ = true;
     graph_dirty_ = true;
     return DMDGPU_OK;
@@ -861,7 +893,7 @@ void Batch::enqueue_eval(int pass) {
         e0 = next_event();
         record(e0, stream_);
     }
-    launch_nonbonded(d, fp64_, phys_, n_sm_, stream_, &launches_);
+    launch_nonbonded(d, fp64_, phys_, n_sm_, nb_blocks_per_sm_, stream_, &launches_);
     if (prof_nb_) {
         e1 = next_event();
         record(e1, stream_);
@@ -952,6 +984,12 @@ int Batch::run_steps(int n) {
         CK(cudaGetLastError());
         need_eval1_ = (any_baro_ && !phys_) || any_ref_lj_;
         --n;
+        if (!tuned_) {
+            int used = 0;
+            int rc = autotune(n, &used);
+            if (rc) return rc;
+            n -= used;
+        }
         if (graph_) cudaGraphExecDestroy(graph_);
         graph_ = nullptr;
         cudaGraph_t g;
@@ -973,6 +1011,47 @@ int Batch::run_steps(int n) {
         CK(cudaGraphLaunch(graph_, stream_));
         launches_ += per_step_launches_;
     }
+    return DMDGPU_OK;
+}
+
+// Pair-kernel launch shape by measurement: each candidate runs kTuneSteps real
+// steps (eagerly, in the same order as the captured step) timed with events on
+// the main stream, which the bonded / PME stream joins every step; the fastest
+// median step wins and is cached for this kind of batch.  The candidates give
+// bit-identical results, so tuning steps are ordinary steps of the run.  Runs
+// only when the call has enough steps to spare.
+int Batch::autotune(int max_steps, int* used) {
+    *used = 0;
+    const int n_cand = static_cast<int>(sizeof(kTuneCand) / sizeof(kTuneCand[0]));
+    if (max_steps < n_cand * kTuneSteps) return DMDGPU_OK;
+    std::vector<cudaEvent_t> ev(kTuneSteps + 1);
+    for (auto& e : ev) CK(cudaEventCreate(&e));
+    int best = nb_blocks_per_sm_;
+    float best_ms = 1e30f;
+    for (int c = 0; c < n_cand; ++c) {
+        nb_blocks_per_sm_ = kTuneCand[c];
+        std::vector<float> t(kTuneSteps);
+        CK(cudaEventRecord(ev[0], stream_));
+        for (int i = 0; i < kTuneSteps; ++i) {
+            enqueue_step();
+            CK(cudaEventRecord(ev[i + 1], stream_));
+        }
+        CK(cudaGetLastError());
+        CK(cudaEventSynchronize(ev[kTuneSteps]));
+        for (int i = 0; i < kTuneSteps; ++i) CK(cudaEventElapsedTime(&t[i], ev[i], ev[i + 1]));
+        std::sort(t.begin(), t.end());
+        const float med = t[kTuneSteps / 2];
+        if (med < best_ms) {
+            best_ms = med;
+            best = kTuneCand[c];
+        }
+        *used += kTuneSteps;
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    nb_blocks_per_sm_ = best;
+    tuned_ = true;
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune[tune_key(device_, fp64_, any_pme_, dev_.n_atoms)] = best;
     return DMDGPU_OK;
 }
 

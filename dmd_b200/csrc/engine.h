@@ -108,6 +108,7 @@ class Batch {
     void enqueue_rebuild();
     void enqueue_step();
     int run_steps(int n);
+    int autotune(int max_steps, int* used);
     int sync_status();
     int replica_index(int slot) const;
     void free_device();
@@ -139,6 +140,8 @@ class Batch {
     bool packed_ = false;
     bool graph_dirty_ = true;
     bool need_eval1_ = true;
+    int nb_blocks_per_sm_ = 2;  // pair-kernel launch shape (autotuned)
+    bool tuned_ = false;
     long long launches_ = 0;
     long long per_step_launches_ = 0;
     long long used_bytes_ = 0;

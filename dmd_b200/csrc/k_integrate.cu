@@ -139,14 +139,16 @@ __device__ __forceinline__ void skin_check(const Dev& d, RepState* s, const Rep&
 // the pending position scale s (1 otherwise, an exact multiply) is applied
 // before the drift, x <- s x + v dt, and the mirror is written for the box
 // s L that k_eval_begin stores next.
+// One thread per atom in reference order: the FP64 state, masses and bonded
+// forces are read and written coalesced; only the pair forces and the mirror
+// are addressed through the atom's slot.
 __global__ void k_kick_drift(Dev d) {
-    const int slot = blockIdx.x * blockDim.x + threadIdx.x;
-    if (slot >= d.n_slots) return;
-    const int r = d.tile_rep[slot >> 5];
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= d.n_atoms) return;
+    const int r = d.atom_rep[a];
     RepState* s = d.st + r;
     if (!s->active) return;
-    const int a = d.atom_of_slot[slot];
-    if (a < 0) return;
+    const int slot = d.slot_of_atom[a];
     const Rep& R = d.rep[r];
     const double dt = R.dt, half_dt = 0.5 * dt;
     const double inv_mass = 1.0 / d.mass[a];
@@ -418,7 +420,7 @@ void launch_eval_end(const Dev& d, cudaStream_t st, long long* n) {
     ++*n;
 }
 void launch_kick_drift(const Dev& d, bool, cudaStream_t st, long long* n) {
-    k_kick_drift<<<(d.n_slots + 255) / 256, 256, 0, st>>>(d);
+    k_kick_drift<<<(d.n_atoms + 255) / 256, 256, 0, st>>>(d);
     ++*n;
 }
 void launch_kick2(const Dev& d, bool andersen_ref, bool andersen_phys, cudaStream_t st, long long* n) {

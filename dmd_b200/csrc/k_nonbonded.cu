@@ -17,6 +17,8 @@
 //    so the interacting set is exactly the reference's.
 //  * fp64: unwrapped FP64 coordinates with the reference's minimum image and
 //    LJ operation order, no FMA contraction in the per-pair force.
+#include <algorithm>
+
 #include "device.cuh"
 #include "launch.h"
 
@@ -127,7 +129,11 @@ __device__ __forceinline__ float pair_f(float r2, float c6f, float c12f, float q
 // zero coefficients.  Pairs whose FP32 r^2 lies within 1e-5 (relative) of a
 // cutoff are left out of the loop and redone afterwards with the FP64 reference
 // membership test, so the interacting set is exactly the reference's.
-template <bool PHYS, bool ENERGY>
+//
+// PHYS = false evaluates LJ only (the REF profile, and PHYS replicas without
+// charges); SAME = true is the PHYS form whose LJ and Coulomb cutoffs are equal
+// (one band test, one cutoff test per pair).
+template <bool PHYS, bool SAME, bool ENERGY>
 __device__ __forceinline__ void nb_chunk(const Dev& d, const Rep& R, RepState* s, int c, int lane,
                                          ChunkStage& S, const float4* lj_tab, Acc& acc) {
     const double L = s->L;
@@ -188,11 +194,18 @@ __device__ __forceinline__ void nb_chunk(const Dev& d, const Rep& R, RepState* s
             const float4 p = lj[pt[u]];
             const float dx = pj.x - xi.x, dy = pj.y - xi.y, dz = pj.z - xi.z;
             const float r2 = fmaxf(dx * dx + dy * dy + dz * dz, 1e-6f);
-            const bool near = bit & ((fabsf(r2 - rl2) < wl) | (fabsf(r2 - rcc2) < wc));
+            bool near, in_l, in_c;
+            if (!PHYS || SAME) {
+                near = bit & (fabsf(r2 - rl2) < wl);
+                in_l = bit & !near & (r2 < rl2);
+                in_c = in_l;
+            } else {
+                near = bit & ((fabsf(r2 - rl2) < wl) | (fabsf(r2 - rcc2) < wc));
+                const bool use = bit & !near;
+                in_l = use & (r2 < rl2);
+                in_c = use & (r2 < rcc2);
+            }
             b8 |= static_cast<uint32_t>(near) << u;
-            const bool use = bit & !near;
-            const bool in_l = use & (r2 < rl2);
-            const bool in_c = use & (r2 < rcc2);
             const float c6f = in_l ? p.z : 0.f, c12f = in_l ? p.w : 0.f;
             const float qq = (PHYS && in_c) ? keqi * pj.w : 0.f;
             float ir6, rinv, erfc_ar;
@@ -298,8 +311,18 @@ __global__ void __launch_bounds__(256, 3) k_nb_f32(Dev d) {
         if (!s->eval) continue;
         const Rep& R = d.rep[r];
         const int c = R.chunk_begin + (w - d.chunk_prefix[r]);
-        if (s->want_e) nb_chunk<PHYS, true>(d, R, s, c, lane, s_stage[wib], lj_tab, acc);
-        else nb_chunk<PHYS, false>(d, R, s, c, lane, s_stage[wib], lj_tab, acc);
+        // warp-uniform choice of the pair form for this replica
+        const bool coul = PHYS && (R.flags & F_COUL_REAL);
+        const bool same = coul && (R.flags & F_LJ) && R.rc_lj2 == R.rc_c2;
+        if (s->want_e) {
+            if (!coul) nb_chunk<false, false, true>(d, R, s, c, lane, s_stage[wib], lj_tab, acc);
+            else if (same) nb_chunk<true, true, true>(d, R, s, c, lane, s_stage[wib], lj_tab, acc);
+            else nb_chunk<true, false, true>(d, R, s, c, lane, s_stage[wib], lj_tab, acc);
+        } else {
+            if (!coul) nb_chunk<false, false, false>(d, R, s, c, lane, s_stage[wib], lj_tab, acc);
+            else if (same) nb_chunk<true, true, false>(d, R, s, c, lane, s_stage[wib], lj_tab, acc);
+            else nb_chunk<true, false, false>(d, R, s, c, lane, s_stage[wib], lj_tab, acc);
+        }
     }
     flush_acc(d, cur, acc);
 }
@@ -408,15 +431,17 @@ __global__ void __launch_bounds__(256) k_nb_f64(Dev d) {
 
 }  // namespace
 
-void launch_nonbonded(const Dev& d, bool fp64, bool phys, int n_sm, cudaStream_t st, long long* nlaunch) {
+void launch_nonbonded(const Dev& d, bool fp64, bool phys, int n_sm, int blocks_per_sm, cudaStream_t st,
+                      long long* nlaunch) {
     if (fp64) {
         if (phys) k_nb_f64<true><<<n_sm * 8, 256, 0, st>>>(d);
         else k_nb_f64<false><<<n_sm * 8, 256, 0, st>>>(d);
     } else {
-        // persistent, 2 of the 3 blocks per SM its registers allow: the rest of
-        // the SM stays free for the bonded / PME kernels running alongside
-        if (phys) k_nb_f32<true><<<n_sm * 2, 256, 0, st>>>(d);
-        else k_nb_f32<false><<<n_sm * 2, 256, 0, st>>>(d);
+        // persistent: up to the 3 blocks per SM its registers allow; fewer leave
+        // room on every SM for the bonded / PME kernels running alongside
+        const int g = n_sm * std::min(std::max(blocks_per_sm, 1), 3);
+        if (phys) k_nb_f32<true><<<g, 256, 0, st>>>(d);
+        else k_nb_f32<false><<<g, 256, 0, st>>>(d);
     }
     *nlaunch += 1;
 }

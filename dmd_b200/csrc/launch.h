@@ -13,7 +13,10 @@ void launch_rebuild(const Dev& d, const int* bin_rep, int n_sm, cudaStream_t st,
 
 // k_nonbonded.cu: LJ + real-space Ewald over the chunk list (replicas with `eval`).
 // Pair energies and virial are summed only for replicas whose `want_e` is set.
-void launch_nonbonded(const Dev& d, bool fp64, bool phys, int n_sm, cudaStream_t st,
+// The mixed-precision kernel is persistent with blocks_per_sm blocks of 256
+// threads per SM (1..3, chosen by the engine's autotuner); results do not depend
+// on it (one warp per chunk, fixed-point sums).
+void launch_nonbonded(const Dev& d, bool fp64, bool phys, int n_sm, int blocks_per_sm, cudaStream_t st,
                       long long* nlaunch);
 
 // k_forces.cu

@@ -316,7 +316,7 @@ extern "C" int dmdgpu_nonbonded_noalloc(const dmdgpu_nb_params* p, const double*
     int n_sm = 148;
     cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
     launch_rebuild(d, bin_rep, n_sm, st, &nl);
-    launch_nonbonded(d, fp64, phys, n_sm, st, &nl);
+    launch_nonbonded(d, fp64, phys, n_sm, 2, st, &nl);
     k_noalloc_out<<<(n + 255) / 256, 256, 0, st>>>(d, d_fx, d_fy, d_fz, d_energies);
     if (cudaGetLastError() != cudaSuccess) return DMDGPU_ERR_GPU;
     // the call is synchronous: the status word says whether the list fitted
