@@ -28,7 +28,8 @@ PRECISIONS = {"mixed": 0, "fp64": 1}
 COULOMB = {"cutoff": 0, "direct": 0, "pme": 1}
 THERMO = {"none": 0, "berendsen": 1, "nose-hoover": 2, "andersen": 3}
 BARO = {"none": 0, "berendsen": 1}
-E_TERMS = ("lj", "coul_real", "coul_recip", "coul_self", "coul_excl", "bond", "angle", "dihedral")
+E_TERMS = ("lj", "coul_real", "coul_recip", "coul_self", "coul_excl", "bond", "angle", "dihedral",
+           "improper")
 
 
 class dmdgpu_system(C.Structure):
@@ -46,7 +47,8 @@ class dmdgpu_system(C.Structure):
         ("n_dihedrals", C.c_int32), ("dihedral_i", _ip), ("dihedral_j", _ip), ("dihedral_k", _ip),
         ("dihedral_l", _ip), ("dihedral_periodicity", _ip), ("dihedral_k_phi", _dp),
         ("dihedral_phi0", _dp),
-        ("n_impropers", C.c_int32),
+        ("n_impropers", C.c_int32), ("improper_i", _ip), ("improper_j", _ip), ("improper_k", _ip),
+        ("improper_l", _ip), ("improper_k_phi", _dp), ("improper_phi0", _dp),
         ("coulomb_type", C.c_int32), ("coulomb_cutoff", C.c_double), ("ewald_coeff", C.c_double),
         ("pme_grid_spacing", C.c_double), ("pme_order", C.c_int32),
         ("n_excl", C.c_int32), ("excl_i", _ip), ("excl_j", _ip),
@@ -75,7 +77,7 @@ class dmdgpu_scalars(C.Structure):
     _fields_ = [("step", C.c_int64), ("time", C.c_double), ("potential_energy", C.c_double),
                 ("box", C.c_double), ("kinetic_energy", C.c_double), ("temperature", C.c_double),
                 ("pressure", C.c_double), ("virial", C.c_double), ("zeta", C.c_double),
-                ("e_terms", C.c_double * 8), ("list_builds", C.c_int64),
+                ("e_terms", C.c_double * 9), ("list_builds", C.c_int64),
                 ("lj_step_since_rebuild", C.c_int32), ("status", C.c_int32),
                 ("list_chunks", C.c_int64)]
 
@@ -204,7 +206,12 @@ class SystemDesc:
             s.dihedral_k, s.dihedral_l = i(cfg.dihedral_k, nd), i(cfg.dihedral_l, nd)
             s.dihedral_periodicity = i(cfg.dihedral_periodicity, nd)
             s.dihedral_k_phi, s.dihedral_phi0 = d(cfg.dihedral_k_phi, nd), d(cfg.dihedral_phi0, nd)
-        s.n_impropers = len(cfg.improper_i)
+        ni = len(cfg.improper_i)
+        s.n_impropers = ni
+        if ni:
+            s.improper_i, s.improper_j = i(cfg.improper_i, ni), i(cfg.improper_j, ni)
+            s.improper_k, s.improper_l = i(cfg.improper_k, ni), i(cfg.improper_l, ni)
+            s.improper_k_phi, s.improper_phi0 = d(cfg.improper_k_phi, ni), d(cfg.improper_phi0, ni)
         if cfg.coulomb_type not in COULOMB:
             raise ValueError(f"unknown coulomb_type {cfg.coulomb_type!r}")
         s.coulomb_type = COULOMB[cfg.coulomb_type]

@@ -259,7 +259,7 @@ class Engine:
     def compute_forces(self):
         """Single-point forces (N x 3) and energy terms at the current positions."""
         fx, fy, fz = np.empty(self._n), np.empty(self._n), np.empty(self._n)
-        e = np.zeros(8)
+        e = np.zeros(len(_capi.E_TERMS))
         self._check(self._lib.dmdgpu_compute_forces(self._h, _capi.dptr(fx), _capi.dptr(fy),
                                                     _capi.dptr(fz), _capi.dptr(e)))
         return np.stack([fx, fy, fz], axis=1), dict(zip(_capi.E_TERMS, e))

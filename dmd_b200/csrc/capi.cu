@@ -80,6 +80,15 @@ SysView view_of(const dmd::HostSystem& h, const double* x, const double* y, cons
         s.dihedral_k_phi = h.dkp.data();
         s.dihedral_phi0 = h.dp0.data();
     }
+    if (mask & dmd::C_IMP) {
+        s.n_impropers = static_cast<int>(h.ii.size());
+        s.improper_i = h.ii.data();
+        s.improper_j = h.ij.data();
+        s.improper_k = h.ik.data();
+        s.improper_l = h.il.data();
+        s.improper_k_phi = h.ikp.data();
+        s.improper_phi0 = h.ip0.data();
+    }
     s.coulomb_type = h.coulomb_type;
     s.coulomb_cutoff = h.coul_cutoff;
     s.ewald_coeff = h.ewald;
@@ -184,10 +193,10 @@ int dmdgpu_component_compute(dmdgpu_ctx* c, int32_t component, const double* px,
                              const double* pz, double box, double* fx, double* fy, double* fz,
                              double* energy) {
     if (!c || !c->b || !px || !py || !pz || !fx || !fy || !fz || !energy) return DMDGPU_ERR_INVALID;
-    static const unsigned masks[7] = {dmd::C_LJ, dmd::C_BOND, dmd::C_ANGLE, dmd::C_DIH, dmd::C_CREAL,
-                                      dmd::C_PME, dmd::C_EXCL};
-    if (component < 0 || component > 6) {
-        c->err = "component must be 0..6";
+    static const unsigned masks[8] = {dmd::C_LJ, dmd::C_BOND, dmd::C_ANGLE, dmd::C_DIH, dmd::C_CREAL,
+                                      dmd::C_PME, dmd::C_EXCL, dmd::C_IMP};
+    if (component < 0 || component > 7) {
+        c->err = "component must be 0..7";
         return DMDGPU_ERR_PARM;
     }
     const dmd::HostSystem& h = c->b->system(c->slot);
@@ -204,7 +213,7 @@ int dmdgpu_component_compute(dmdgpu_ctx* c, int32_t component, const double* px,
         }
         const int n = h.n;
         std::vector<double> gx(n), gy(n), gz(n);
-        double e[8];
+        double e[9];
         int rc = tmp.compute_forces(slot, gx.data(), gy.data(), gz.data(), e);
         if (rc) {
             c->err = tmp.error();
@@ -215,7 +224,7 @@ int dmdgpu_component_compute(dmdgpu_ctx* c, int32_t component, const double* px,
             fy[i] += gy[i];
             fz[i] += gz[i];
         }
-        static const int term[7][2] = {{0, -1}, {5, -1}, {6, -1}, {7, -1}, {1, -1}, {2, 3}, {4, -1}};
+        static const int term[8][2] = {{0, -1}, {5, -1}, {6, -1}, {7, -1}, {1, -1}, {2, 3}, {4, -1}, {8, -1}};
         double add = e[term[component][0]];
         if (term[component][1] >= 0) add += e[term[component][1]];
         *energy += add;

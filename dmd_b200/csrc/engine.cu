@@ -242,8 +242,6 @@ int Batch::add(const dmdgpu_system& in, long long n_steps, unsigned comp_mask, i
     if (!(in.box_size > 0)) return fail(DMDGPU_ERR_PARM, "box_size must be positive");
     if (!in.masses || !in.pos_x || !in.pos_y || !in.pos_z)
         return fail(DMDGPU_ERR_PARM, "masses and positions are required");
-    if (in.n_impropers != 0)
-        return fail(DMDGPU_ERR_PARM, "harmonic impropers are not supported on this path");
     if (in.constraint_type != 0)
         return fail(DMDGPU_ERR_PARM, "SHAKE/RATTLE constraints are not supported on this path");
     if (in.thermostat_type < 0 || in.thermostat_type > 3)
@@ -311,6 +309,21 @@ int Batch::add(const dmdgpu_system& in, long long n_steps, unsigned comp_mask, i
         s.dn = vec_of(in.dihedral_periodicity, m);
         s.dkp = vec_of(in.dihedral_k_phi, m);
         s.dp0 = vec_of(in.dihedral_phi0, m);
+    }
+    if (in.n_impropers > 0) {
+        const int m = in.n_impropers;
+        if (!in.improper_i || !in.improper_j || !in.improper_k || !in.improper_l ||
+            !in.improper_k_phi || !in.improper_phi0)
+            return fail(DMDGPU_ERR_PARM, "improper arrays missing");
+        if (!check_idx(in.improper_i, m) || !check_idx(in.improper_j, m) ||
+            !check_idx(in.improper_k, m) || !check_idx(in.improper_l, m))
+            return fail(DMDGPU_ERR_PARM, "improper index out of range");
+        s.ii = vec_of(in.improper_i, m);
+        s.ij = vec_of(in.improper_j, m);
+        s.ik = vec_of(in.improper_k, m);
+        s.il = vec_of(in.improper_l, m);
+        s.ikp = vec_of(in.improper_k_phi, m);
+        s.ip0 = vec_of(in.improper_phi0, m);
     }
     if (in.n_excl > 0) {
         if (!check_idx(in.excl_i, in.n_excl) || !check_idx(in.excl_j, in.n_excl))
@@ -465,7 +478,7 @@ int Batch::pack() {
     }
     // offsets
     long long n_atoms = 0, n_tiles = 0, n_bins = 0, n_chunks = 0, n_lj = 0, n_bond = 0, n_ang = 0,
-              n_dih = 0, n_excl = 0, mesh_fix = 0, mesh_real = 0, mesh_cplx = 0, n_bsp = 0;
+              n_dih = 0, n_imp = 0, n_excl = 0, mesh_fix = 0, mesh_real = 0, mesh_cplx = 0, n_bsp = 0;
     int pme_blocks = 0;
     any_pme_ = any_baro_ = any_ref_lj_ = any_andersen_ref_ = any_andersen_phys_ = false;
     for (int k = 0; k < R; ++k) {
@@ -496,6 +509,7 @@ int Batch::pack() {
         n_bond += s.bi.size();
         n_ang += s.ai.size();
         n_dih += s.di.size();
+        n_imp += s.ii.size();
         n_excl += s.ei.size();
         if (P.flags & F_PME) {
             const int K = P.pme_K;
@@ -608,6 +622,8 @@ int Batch::pack() {
         std::vector<int4> dijkl;
         std::vector<int> dn;
         std::vector<double2> dkp;
+        std::vector<int4> iijkl;
+        std::vector<double2> ikp;
         std::vector<int2> ex;
         std::vector<std::vector<int>> exl(n_atoms);
         std::vector<double> bsp(std::max<long long>(n_bsp, 1));
@@ -669,6 +685,10 @@ int Batch::pack() {
                 dijkl.push_back(make_int4(a0 + s.di[t], a0 + s.dj[t], a0 + s.dk[t], a0 + s.dl[t]));
                 dn.push_back(s.dn[t]);
                 dkp.push_back(make_double2(s.dkp[t], s.dp0[t]));
+            }
+            for (size_t t = 0; t < s.ii.size(); ++t) {
+                iijkl.push_back(make_int4(a0 + s.ii[t], a0 + s.ij[t], a0 + s.ik[t], a0 + s.il[t]));
+                ikp.push_back(make_double2(s.ikp[t], s.ip0[t]));
             }
             for (size_t t = 0; t < s.ei.size(); ++t) {
                 const int gi = a0 + s.ei[t], gj = a0 + s.ej[t];
@@ -734,6 +754,7 @@ int Batch::pack() {
         d.n_bonds = static_cast<int>(bij.size());
         d.n_angles = static_cast<int>(aijk.size());
         d.n_dih = static_cast<int>(dijkl.size());
+        d.n_imp = static_cast<int>(iijkl.size());
         d.n_excl = static_cast<int>(ex.size());
         int2* dbij = A.alloc<int2>(bij.size());
         double2* dbkr = A.alloc<double2>(bkr.size());
@@ -742,6 +763,8 @@ int Batch::pack() {
         int4* ddijkl = A.alloc<int4>(dijkl.size());
         int* ddn = A.alloc<int>(dn.size());
         double2* ddkp = A.alloc<double2>(dkp.size());
+        int4* diijkl = A.alloc<int4>(iijkl.size());
+        double2* dikp = A.alloc<double2>(ikp.size());
         int2* dex = A.alloc<int2>(ex.size());
         int* dexs = A.alloc<int>(ex_start.size());
         int* dexl = A.alloc<int>(ex_list.size());
@@ -752,6 +775,8 @@ int Batch::pack() {
         up(ddijkl, dijkl.data(), sizeof(int4) * dijkl.size());
         up(ddn, dn.data(), sizeof(int) * dn.size());
         up(ddkp, dkp.data(), sizeof(double2) * dkp.size());
+        up(diijkl, iijkl.data(), sizeof(int4) * iijkl.size());
+        up(dikp, ikp.data(), sizeof(double2) * ikp.size());
         up(dex, ex.data(), sizeof(int2) * ex.size());
         up(dexs, ex_start.data(), sizeof(int) * ex_start.size());
         up(dexl, ex_list.data(), sizeof(int) * ex_list.size());
@@ -762,6 +787,8 @@ int Batch::pack() {
         d.dih_ijkl = ddijkl;
         d.dih_n = ddn;
         d.dih_kp = ddkp;
+        d.imp_ijkl = diijkl;
+        d.imp_kp = dikp;
         d.excl = dex;
         d.ex_start = dexs;
         d.ex_list = dexl;
@@ -1320,7 +1347,7 @@ int Batch::get_scalars(int slot, dmdgpu_scalars* out) {
     out->step = s.step;
     out->time = s.time;
     out->box = s.L;
-    double e[8];
+    double e[9];
     e[0] = static_cast<double>(s.e_acc[E_LJ]) / ESCALE;
     e[1] = static_cast<double>(s.e_acc[E_CREAL]) / ESCALE;
     e[2] = (P.flags & F_PME) ? s.e_recip : 0.0;
@@ -1329,8 +1356,9 @@ int Batch::get_scalars(int slot, dmdgpu_scalars* out) {
     e[5] = static_cast<double>(s.e_acc[E_BOND]) / ESCALE;
     e[6] = static_cast<double>(s.e_acc[E_ANGLE]) / ESCALE;
     e[7] = static_cast<double>(s.e_acc[E_DIH]) / ESCALE;
+    e[8] = static_cast<double>(s.e_acc[E_IMP]) / ESCALE;
     double pe = 0.0;
-    for (int t = 0; t < 8; ++t) {
+    for (int t = 0; t < 9; ++t) {
         out->e_terms[t] = e[t];
         pe += e[t];
     }
@@ -1372,7 +1400,7 @@ int Batch::compute_forces(int slot, double* fx, double* fy, double* fz, double* 
         dmdgpu_scalars s;
         rc = get_scalars(slot, &s);
         if (rc) return rc;
-        std::memcpy(e_terms, s.e_terms, sizeof(double) * 8);
+        std::memcpy(e_terms, s.e_terms, sizeof(double) * 9);
     }
     return DMDGPU_OK;
 }

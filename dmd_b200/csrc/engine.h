@@ -16,7 +16,7 @@ namespace dmd {
 // Component selection for single-component evaluation (ForceComponent parity).
 enum CompMask : unsigned {
     C_LJ = 1u << 0, C_BOND = 1u << 1, C_ANGLE = 1u << 2, C_DIH = 1u << 3, C_CREAL = 1u << 4,
-    C_PME = 1u << 5, C_EXCL = 1u << 6, C_ALL = 0x7fu
+    C_PME = 1u << 5, C_EXCL = 1u << 6, C_IMP = 1u << 7, C_ALL = 0xffu
 };
 
 // Host copy of one system (a SimulationConfig) plus its packing metadata.
@@ -34,6 +34,8 @@ struct HostSystem {
     std::vector<double> akt, at0;
     std::vector<int> di, dj, dk, dl, dn;
     std::vector<double> dkp, dp0;
+    std::vector<int> ii, ij, ik, il;
+    std::vector<double> ikp, ip0;
     std::vector<int> ei, ej;
     int coulomb_type = 0;
     double coul_cutoff = 1.2, ewald = 0.34, spacing = 0.12;

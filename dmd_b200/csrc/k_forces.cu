@@ -4,7 +4,8 @@
 // reference's minimum image, then the term is evaluated in `real` (FP32 in the
 // mixed path).  REF formulas follow src/force/harmonic_bond.cpp:12-47,
 // harmonic_angle.cpp:10-63 (force sign quirk kept), periodic_dihedral.cpp:10-137
-// (the reference's gradient vectors); PHYS uses -grad E.
+// and harmonic_improper.cpp:10-130 (the reference's gradient vectors); PHYS
+// uses -grad E.
 //
 // SPME (src/force/coulomb_pme.cpp): spread (order-4 B-spline, int64 fixed-point
 // atomics onto the mesh), convert (fixed -> real, REF reinterprets the
@@ -120,13 +121,20 @@ __device__ __forceinline__ void do_angle(const Dev& d, int n) {
     add_energy(d, r, E_ANGLE, ef, vf, valid);
 }
 
-template <typename T, bool PHYS>
-__device__ __forceinline__ void do_dihedral(const Dev& d, int n) {
+// Torsions: PeriodicDihedral (periodic_dihedral.cpp:10-137) and, with IMP,
+// HarmonicImproper (harmonic_improper.cpp:10-130).  Both measure the angle
+// between the planes (i, j, k) and (j, k, l) as atan2 of the same clamped sine
+// and cosine; the dihedral's energy is k (1 + cos(n phi - phi0)), the
+// improper's k/2 (chi - chi0)^2 (chi - chi0 not wrapped, as in the reference).
+// REF forces are the reference's gradient vectors times -dE/dangle; PHYS
+// forces are -grad E.
+template <typename T, bool PHYS, bool IMP>
+__device__ __forceinline__ void do_torsion(const Dev& d, int n) {
     int r = 0;
     long long ef = 0, vf = 0;
     bool valid = false;
-    if (n < d.n_dih) {
-        const int4 q = d.dih_ijkl[n];
+    if (n < (IMP ? d.n_imp : d.n_dih)) {
+        const int4 q = IMP ? d.imp_ijkl[n] : d.dih_ijkl[n];
         r = d.atom_rep[q.x];
         RepState* s = d.st + r;
         if (s->eval) {
@@ -156,12 +164,14 @@ __device__ __forceinline__ void do_dihedral(const Dev& d, int n) {
                 T sph = trip / (bcn * n1n * n2n);
                 sph = fmax(T(-1), fmin(T(1), sph));
                 const T phi = atan2(sph, cph);
-                const int p = d.dih_n[n];
-                const double2 kp = d.dih_kp[n];
+                const int p = IMP ? 0 : d.dih_n[n];
+                const double2 kp = IMP ? d.imp_kp[n] : d.dih_kp[n];
                 const T k = (T)kp.x, phi0 = (T)kp.y;
-                ef = to_fix(k * (T(1) + cos(p * phi - phi0)), ESCALE, s);
+                const T dphi = phi - phi0;                           // improper
+                const T ncos = IMP ? T(0) : (T)(p * phi - phi0);    // dihedral
+                ef = to_fix(IMP ? T(0.5) * k * dphi * dphi : k * (T(1) + cos(ncos)), ESCALE, s);
                 if (!PHYS) {
-                    const T pref = k * p * sin(p * phi - phi0);
+                    const T pref = IMP ? -k * dphi : k * p * sin(ncos);
                     if (fabs(pref) >= tiny) {
                         const T gix = (bcy * n1z - bcz * n1y) / n1s, giy = (bcz * n1x - bcx * n1z) / n1s,
                                 giz = (bcx * n1y - bcy * n1x) / n1s;
@@ -181,7 +191,7 @@ __device__ __forceinline__ void do_dihedral(const Dev& d, int n) {
                         add_force(d, q.w, pref * glx, pref * gly, pref * glz, s);
                     }
                 } else {
-                    const T dd = -k * p * sin(p * phi - phi0);  // dE/dphi
+                    const T dd = IMP ? k * dphi : -k * p * sin(ncos);  // dE/dphi
                     const T fix_ = -dd * bcn / n1s * n1x, fiy_ = -dd * bcn / n1s * n1y, fiz_ = -dd * bcn / n1s * n1z;
                     const T flx = dd * bcn / n2s * n2x, fly = dd * bcn / n2s * n2y, flz = dd * bcn / n2s * n2z;
                     const T pp = (bax * bcx + bay * bcy + baz * bcz) / bcs;
@@ -200,7 +210,7 @@ __device__ __forceinline__ void do_dihedral(const Dev& d, int n) {
             }
         }
     }
-    add_energy(d, r, E_DIH, ef, vf, valid);
+    add_energy(d, r, IMP ? E_IMP : E_DIH, ef, vf, valid);
 }
 
 // CoulombExclusion (coulomb_exclusion.cpp:16-56).  REF: E -= k q q / r with the
@@ -485,16 +495,19 @@ __global__ void k_pme_gather(Dev d) {
 }
 
 // One launch for every bonded-type term: blocks [0, nb) bonds, then angles,
-// dihedrals and exclusion pairs (exclusions always in FP64, see do_exclusion).
+// dihedrals, impropers and exclusion pairs (exclusions always in FP64, see
+// do_exclusion).
 template <typename T, bool PHYS>
-__global__ void k_bonded(Dev d, int nb, int na, int nd) {
+__global__ void k_bonded(Dev d, int nb, int na, int nd, int ni) {
     int b = blockIdx.x;
     if (b < nb) { do_bond<T, PHYS>(d, b * blockDim.x + threadIdx.x); return; }
     b -= nb;
     if (b < na) { do_angle<T, PHYS>(d, b * blockDim.x + threadIdx.x); return; }
     b -= na;
-    if (b < nd) { do_dihedral<T, PHYS>(d, b * blockDim.x + threadIdx.x); return; }
+    if (b < nd) { do_torsion<T, PHYS, false>(d, b * blockDim.x + threadIdx.x); return; }
     b -= nd;
+    if (b < ni) { do_torsion<T, PHYS, true>(d, b * blockDim.x + threadIdx.x); return; }
+    b -= ni;
     do_exclusion<double, PHYS>(d, b * blockDim.x + threadIdx.x);
 }
 
@@ -503,15 +516,15 @@ __global__ void k_bonded(Dev d, int nb, int na, int nd) {
 void launch_bonded(const Dev& d, bool fp64, bool phys, cudaStream_t st, long long* nlaunch) {
     const int T = 256;
     const int nb = (d.n_bonds + T - 1) / T, na = (d.n_angles + T - 1) / T, nd = (d.n_dih + T - 1) / T,
-              ne = (d.n_excl + T - 1) / T;
-    const int g = nb + na + nd + ne;
+              ni = (d.n_imp + T - 1) / T, ne = (d.n_excl + T - 1) / T;
+    const int g = nb + na + nd + ni + ne;
     if (g == 0) return;
     if (fp64) {
-        if (phys) k_bonded<double, true><<<g, T, 0, st>>>(d, nb, na, nd);
-        else k_bonded<double, false><<<g, T, 0, st>>>(d, nb, na, nd);
+        if (phys) k_bonded<double, true><<<g, T, 0, st>>>(d, nb, na, nd, ni);
+        else k_bonded<double, false><<<g, T, 0, st>>>(d, nb, na, nd, ni);
     } else {
-        if (phys) k_bonded<float, true><<<g, T, 0, st>>>(d, nb, na, nd);
-        else k_bonded<float, false><<<g, T, 0, st>>>(d, nb, na, nd);
+        if (phys) k_bonded<float, true><<<g, T, 0, st>>>(d, nb, na, nd, ni);
+        else k_bonded<float, false><<<g, T, 0, st>>>(d, nb, na, nd, ni);
     }
     ++*nlaunch;
 }

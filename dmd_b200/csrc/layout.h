@@ -41,7 +41,7 @@ enum Status : int {
 };
 
 enum ETerm : int { E_LJ = 0, E_CREAL = 1, E_CRECIP = 2, E_CSELF = 3, E_CEXCL = 4, E_BOND = 5,
-                   E_ANGLE = 6, E_DIH = 7, E_VIR = 8, N_EACC = 9 };
+                   E_ANGLE = 6, E_DIH = 7, E_IMP = 8, E_VIR = 9, N_EACC = 10 };
 
 // Per-replica constants.
 struct Rep {
@@ -143,7 +143,7 @@ struct Dev {
     int* build_work;                   // list-build i-tile counter (reset per rebuild)
     unsigned* grid_bar;                // [2] rebuild grid barrier: arrivals, generation
     // bonded terms (global atom indices)
-    int n_bonds, n_angles, n_dih;
+    int n_bonds, n_angles, n_dih, n_imp;
     const int2* bond_ij;
     const double2* bond_kr;
     const int4* ang_ijk;
@@ -151,6 +151,8 @@ struct Dev {
     const int4* dih_ijkl;
     const int* dih_n;
     const double2* dih_kp;
+    const int4* imp_ijkl;
+    const double2* imp_kp;             // (k, chi0)
     // LJ tables per type pair
     const double2* lj64;               // (eps, sig^6)
     const float4* lj32;                // (c6, c12, 6 c6, 12 c12), c6 = 4 eps sig^6, c12 = 4 eps sig^12

@@ -49,6 +49,9 @@ class Workload:
     dih_k: np.ndarray = field(default_factory=lambda: np.zeros(0))
     dih_n: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int32))
     dih_phi0: np.ndarray = field(default_factory=lambda: np.zeros(0))
+    impropers: np.ndarray = field(default_factory=lambda: np.zeros((0, 4), np.int32))
+    imp_k: np.ndarray = field(default_factory=lambda: np.zeros(0))
+    imp_phi0: np.ndarray = field(default_factory=lambda: np.zeros(0))
     exclusions: np.ndarray = field(default_factory=lambda: np.zeros((0, 2), np.int32))
 
     @property
@@ -85,6 +88,10 @@ class Workload:
                                 "k_phi": float(kp), "periodicity": int(n), "phi0": float(p0)}
                                for (i, j, k, l), kp, n, p0 in
                                zip(self.dihedrals, self.dih_k, self.dih_n, self.dih_phi0)]
+        if len(self.impropers):
+            ff["impropers"] = [{"i": int(i), "j": int(j), "k": int(k), "l": int(l), "k_phi": float(kp),
+                                "phi0": float(p0)}
+                               for (i, j, k, l), kp, p0 in zip(self.impropers, self.imp_k, self.imp_phi0)]
         system = {
             "cell": {"box_size": float(self.box), "positions": self.pos.tolist()},
             "atoms": {"mass": self.mass.tolist(), "charge": self.charge.tolist(),
@@ -127,6 +134,10 @@ class Workload:
             d = self.dihedrals
             cfg.dihedral_i, cfg.dihedral_j, cfg.dihedral_k, cfg.dihedral_l = d[:, 0], d[:, 1], d[:, 2], d[:, 3]
             cfg.dihedral_k_phi, cfg.dihedral_periodicity, cfg.dihedral_phi0 = self.dih_k, self.dih_n, self.dih_phi0
+        if len(self.impropers):
+            m = self.impropers
+            cfg.improper_i, cfg.improper_j, cfg.improper_k, cfg.improper_l = m[:, 0], m[:, 1], m[:, 2], m[:, 3]
+            cfg.improper_k_phi, cfg.improper_phi0 = self.imp_k, self.imp_phi0
         cfg.excl_i = self.exclusions[:, 0].tolist() if len(self.exclusions) else []
         cfg.excl_j = self.exclusions[:, 1].tolist() if len(self.exclusions) else []
         apply_config(cfg, self.config_json())
@@ -248,13 +259,17 @@ DECANE = dict(sig_ch3=0.375, eps_ch3=0.814, sig_ch2=0.395, eps_ch2=0.382, m_ch3=
 
 
 def decane_melt(n_chains: int, seed: int, chains_per_nm3: float = 3.09, n_steps: int = 1000,
-                dt: float = 0.002, T: float = 300.0, d_min: float = 0.25) -> Workload:
+                dt: float = 0.002, T: float = 300.0, d_min: float = 0.25,
+                impropers: bool = False) -> Workload:
     """United-atom n-decane melt.  Chains grow as seeded random walks with fixed
     bond length and angle and torsions drawn near trans/gauche; a site is
     accepted only if it is at least d_min from every site placed before it
     (other than the preceding sites of its own chain), so the melt has no
     overlaps.  1-2, 1-3 and 1-4 exclusions; the Lorentz-Berthelot cross pair is
-    written explicitly (the engine has no combining rule)."""
+    written explicitly (the engine has no combining rule).  ``impropers`` adds
+    two harmonic impropers per chain (sites 0-3 and 6-9, k 80 kJ/mol/rad^2,
+    chi0 0.6 rad): a test system for the HarmonicImproper term, not part of the
+    decane model."""
     D = DECANE
     rng = np.random.default_rng(seed)
     box = (n_chains / chains_per_nm3) ** (1.0 / 3.0)
@@ -351,7 +366,14 @@ def decane_melt(n_chains: int, seed: int, chains_per_nm3: float = 3.09, n_steps:
         thermostat=_thermo(), barostat=_baro(), lj_cutoff=rc,
         bonds=bonds, bond_k=np.full(len(bonds), D["kb"]), bond_r0=np.full(len(bonds), b),
         angles=angles, angle_k=np.full(len(angles), D["ka"]), angle_t0=np.full(len(angles), th),
-        dihedrals=dih, dih_k=dk, dih_n=dn, dih_phi0=dp, exclusions=excl)
+        dihedrals=dih, dih_k=dk, dih_n=dn, dih_phi0=dp, exclusions=excl,
+        **(_decane_impropers(n_chains) if impropers else {}))
+
+
+def _decane_impropers(n_chains: int) -> dict:
+    c = np.arange(n_chains)[:, None] * 10
+    q = np.concatenate([c + np.arange(4), c + 6 + np.arange(4)]).astype(np.int32)
+    return dict(impropers=q, imp_k=np.full(len(q), 80.0), imp_phi0=np.full(len(q), 0.6))
 
 
 def batch_256(seed: int = 1234, n_lj: int = 192, n_dec: int = 64, scale: float = 1.0):

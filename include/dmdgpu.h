@@ -55,7 +55,7 @@ enum { DMDGPU_PRECISION_MIXED = 0, DMDGPU_PRECISION_FP64 = 1 };
  * System + run description.  Mirrors SimulationConfig
  * (src/sim/simulation_config.h:27-84) as filled by SystemBuilder/apply_config
  * (python/dmd/system.py, python/dmd/config.py): a cubic box, per-atom SoA
- * arrays, one bond / angle / dihedral term set each.  vel_* may be NULL (zero
+ * arrays, one bond / angle / dihedral / improper term set each.  vel_* may be NULL (zero
  * velocities); atom_types may be NULL (all type 0).
  */
 typedef struct dmdgpu_system {
@@ -79,7 +79,10 @@ typedef struct dmdgpu_system {
     int32_t n_dihedrals;
     const int32_t *dihedral_i, *dihedral_j, *dihedral_k, *dihedral_l, *dihedral_periodicity;
     const double *dihedral_k_phi, *dihedral_phi0;
-    int32_t n_impropers; /* must be 0: harmonic impropers are not on this path */
+    /* HarmonicImproper (src/force/harmonic_improper.cpp:10-130): E = k/2 (chi - chi0)^2 */
+    int32_t n_impropers;
+    const int32_t *improper_i, *improper_j, *improper_k, *improper_l;
+    const double *improper_k_phi, *improper_phi0;
     /* electrostatics */
     int32_t coulomb_type;
     double coulomb_cutoff, ewald_coeff, pme_grid_spacing;
@@ -116,8 +119,9 @@ typedef struct dmdgpu_scalars {
     double box;
     double kinetic_energy, temperature, pressure, virial;
     double zeta;             /* Nose-Hoover friction */
-    /* energy terms: lj, coul_real, coul_recip, coul_self, coul_excl, bond, angle, dihedral */
-    double e_terms[8];
+    /* energy terms: lj, coul_real, coul_recip, coul_self, coul_excl, bond, angle, dihedral,
+     * improper */
+    double e_terms[9];
     int64_t list_builds;
     int32_t lj_step_since_rebuild; /* LennardJones::step_since_rebuild (REF cadence) */
     int32_t status;
@@ -151,7 +155,7 @@ int dmdgpu_get_scalars(dmdgpu_ctx *ctx, dmdgpu_scalars *out);
 
 /* Single-point evaluation of every component at the current positions
  * (ForceEngine::compute, src/force/force_engine.cpp:10-25) with a freshly built
- * list.  Forces are written (not accumulated); e_terms receives 8 doubles
+ * list.  Forces are written (not accumulated); e_terms receives 9 doubles
  * (see dmdgpu_scalars.e_terms) and may be NULL. */
 int dmdgpu_compute_forces(dmdgpu_ctx *ctx, double *fx, double *fy, double *fz, double *e_terms);
 
@@ -160,7 +164,8 @@ int dmdgpu_compute_forces(dmdgpu_ctx *ctx, double *fx, double *fy, double *fz, d
  * forces are added (never zeroed) and the energy is added to *energy.
  * component: 0 LennardJones, 1 HarmonicBond, 2 HarmonicAngle, 3 PeriodicDihedral,
  * 4 CoulombDirect (real-space Ewald), 5 CoulombPME (reciprocal + self),
- * 6 CoulombExclusion.  The context's own positions are left unchanged. */
+ * 6 CoulombExclusion, 7 HarmonicImproper.  The context's own positions are left
+ * unchanged. */
 int dmdgpu_component_compute(dmdgpu_ctx *ctx, int32_t component, const double *pos_x,
                              const double *pos_y, const double *pos_z, double box,
                              double *forces_x, double *forces_y, double *forces_z,

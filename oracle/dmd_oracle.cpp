@@ -196,11 +196,15 @@ struct orc_system {
     int n_dih;
     const int *dih_i, *dih_j, *dih_k, *dih_l, *dih_n;
     const double *dih_kphi, *dih_phi0;
+    int n_imp;
+    const int *imp_i, *imp_j, *imp_k, *imp_l;
+    const double *imp_kphi, *imp_phi0;
     int profile;  // 0 ref, 1 phys
 };
 
 struct orc_energy {
-    double lj, coul_real, coul_recip, coul_self, coul_excl, bond, angle, dihedral, total, virial;
+    double lj, coul_real, coul_recip, coul_self, coul_excl, bond, angle, dihedral, improper, total,
+        virial;
 };
 
 // ---- exported small helpers (pinned against the reference's unit tests) ----
@@ -341,13 +345,19 @@ void angles(const Sys& s, const double* x, const double* y, const double* z, dou
     eout += energy;
 }
 
-// PeriodicDihedral::compute (periodic_dihedral.cpp:10-137).  ref: the reference's
-// gradient vectors; phys: the analytic gradient of the same energy.
-void dihedrals(const Sys& s, const double* x, const double* y, const double* z, double L,
-               double* fx, double* fy, double* fz, double& eout, double& vir) {
+// PeriodicDihedral::compute (periodic_dihedral.cpp:10-137) and, with IMP,
+// HarmonicImproper::compute (harmonic_improper.cpp:10-130): the same plane
+// geometry and angle; E = k (1 + cos(n phi - phi0)) or k/2 (chi - chi0)^2.
+// ref: the reference's gradient vectors times -dE/dangle; phys: the analytic
+// gradient of the same energy.
+template <bool IMP>
+void torsions(const Sys& s, const double* x, const double* y, const double* z, double L,
+              double* fx, double* fy, double* fz, double& eout, double& vir) {
     double energy = 0.0;
-    for (int n = 0; n < s.n_dih; ++n) {
-        int ai = s.dih_i[n], aj = s.dih_j[n], ak = s.dih_k[n], al = s.dih_l[n];
+    const int nt = IMP ? s.n_imp : s.n_dih;
+    for (int n = 0; n < nt; ++n) {
+        int ai = IMP ? s.imp_i[n] : s.dih_i[n], aj = IMP ? s.imp_j[n] : s.dih_j[n];
+        int ak = IMP ? s.imp_k[n] : s.dih_k[n], al = IMP ? s.imp_l[n] : s.dih_l[n];
         double ba_x = x[ai] - x[aj], ba_y = y[ai] - y[aj], ba_z = z[ai] - z[aj];
         min_image(L, ba_x, ba_y, ba_z);
         double bc_x = x[ak] - x[aj], bc_y = y[ak] - y[aj], bc_z = z[ak] - z[aj];
@@ -375,13 +385,14 @@ void dihedrals(const Sys& s, const double* x, const double* y, const double* z, 
         double sin_phi = triple / (bc_norm * n1_norm * n2_norm);
         sin_phi = std::max(-1.0, std::min(1.0, sin_phi));
         double phi = std::atan2(sin_phi, cos_phi);
-        int p = s.dih_n[n];
-        double k = s.dih_kphi[n];
-        double phi0 = s.dih_phi0[n];
-        double cos_np = std::cos(p * phi - phi0);
-        energy += k * (1.0 + cos_np);
+        int p = IMP ? 0 : s.dih_n[n];
+        double k = IMP ? s.imp_kphi[n] : s.dih_kphi[n];
+        double phi0 = IMP ? s.imp_phi0[n] : s.dih_phi0[n];
+        double dchi = phi - phi0;
+        if (IMP) energy += 0.5 * k * dchi * dchi;
+        else energy += k * (1.0 + std::cos(p * phi - phi0));
         if (s.profile == 0) {
-            double pref = k * p * std::sin(p * phi - phi0);
+            double pref = IMP ? -k * dchi : k * p * std::sin(p * phi - phi0);
             if (std::abs(pref) < 1e-30) continue;
             double gi_x = (bc_y * n1_z - bc_z * n1_y) / n1_sq;
             double gi_y = (bc_z * n1_x - bc_x * n1_z) / n1_sq;
@@ -415,7 +426,7 @@ void dihedrals(const Sys& s, const double* x, const double* y, const double* z, 
         } else {
             // dE/dphi = -k p sin(p phi - phi0); phi is the IUPAC angle of
             // m = r_ij x r_kj and n = r_kj x r_kl (r_ij = ba, r_kj = bc, r_kl = dc).
-            double ddphi = -k * p * std::sin(p * phi - phi0);
+            double ddphi = IMP ? k * dchi : -k * p * std::sin(p * phi - phi0);
             double f_i_x = -ddphi * bc_norm / n1_sq * n1_x;
             double f_i_y = -ddphi * bc_norm / n1_sq * n1_y;
             double f_i_z = -ddphi * bc_norm / n1_sq * n1_z;
@@ -439,6 +450,14 @@ void dihedrals(const Sys& s, const double* x, const double* y, const double* z, 
         }
     }
     eout += energy;
+}
+void dihedrals(const Sys& s, const double* x, const double* y, const double* z, double L,
+               double* fx, double* fy, double* fz, double& eout, double& vir) {
+    torsions<false>(s, x, y, z, L, fx, fy, fz, eout, vir);
+}
+void impropers(const Sys& s, const double* x, const double* y, const double* z, double L,
+               double* fx, double* fy, double* fz, double& eout, double& vir) {
+    torsions<true>(s, x, y, z, L, fx, fy, fz, eout, vir);
 }
 
 // CoulombExclusion::compute (coulomb_exclusion.cpp:16-56).  ref: E -= k q q / r with
@@ -699,6 +718,7 @@ void eval_forces(const Sys& s, const double* x, const double* y, const double* z
         if (s.n_bonds) { t = 0.0; bonds(s, x, y, z, L, fx, fy, fz, t, v); e.bond = t; pe += t; }
         if (s.n_angles) { t = 0.0; angles(s, x, y, z, L, fx, fy, fz, t, v); e.angle = t; pe += t; }
         if (s.n_dih) { t = 0.0; dihedrals(s, x, y, z, L, fx, fy, fz, t, v); e.dihedral = t; pe += t; }
+        if (s.n_imp) { t = 0.0; impropers(s, x, y, z, L, fx, fy, fz, t, v); e.improper = t; pe += t; }
         // CoulombDirect: list never built in engine runs -> contributes 0 (Q1)
         if (s.coulomb_type == 1) {
             double er = 0.0, es = 0.0;
@@ -722,10 +742,11 @@ void eval_forces(const Sys& s, const double* x, const double* y, const double* z
     bonds(s, x, y, z, L, fx, fy, fz, e.bond, vir);
     angles(s, x, y, z, L, fx, fy, fz, e.angle, vir);
     dihedrals(s, x, y, z, L, fx, fy, fz, e.dihedral, vir);
+    impropers(s, x, y, z, L, fx, fy, fz, e.improper, vir);
     if (s.coulomb_type == 1) pme(s, x, y, z, L, fx, fy, fz, e.coul_recip, e.coul_self, vir);
     if (has_coulomb_excl(s)) exclusions(s, x, y, z, L, fx, fy, fz, e.coul_excl, vir);
     e.total = e.lj + e.coul_real + e.coul_recip + e.coul_self + e.coul_excl + e.bond + e.angle +
-              e.dihedral;
+              e.dihedral + e.improper;
     e.virial = vir;
 }
 
@@ -782,6 +803,7 @@ void orc_component(const orc_system* s, int which, const double* x, const double
             break;
         }
         case 6: exclusions(*s, x, y, z, L, fx, fy, fz, *energy, v); break;
+        case 7: impropers(*s, x, y, z, L, fx, fy, fz, *energy, v); break;
         default: break;
     }
     if (virial) *virial += v;
@@ -804,7 +826,9 @@ struct orc_run {
 struct OrcEngine {
     orc_system s;
     // owned copies of every array referenced by s
-    std::vector<double> q, lj_sigma, lj_eps, bond_k, bond_r0, ang_kt, ang_t0, dih_kphi, dih_phi0;
+    std::vector<double> q, lj_sigma, lj_eps, bond_k, bond_r0, ang_kt, ang_t0, dih_kphi, dih_phi0, imp_kphi,
+        imp_phi0;
+    std::vector<int> imp_i, imp_j, imp_k, imp_l;
     std::vector<int> type, excl_i, excl_j, bond_i, bond_j, ang_i, ang_j, ang_k, dih_i, dih_j,
         dih_k, dih_l, dih_n;
     std::vector<double> m, x, y, z, vx, vy, vz, fx, fy, fz;
@@ -849,6 +873,12 @@ void* orc_engine_create(const orc_system* s, const orc_run* r) {
     cpi(E->dih_n, s->dih_n, s->n_dih); E->s.dih_n = E->dih_n.data();
     cpd(E->dih_kphi, s->dih_kphi, s->n_dih); E->s.dih_kphi = E->dih_kphi.data();
     cpd(E->dih_phi0, s->dih_phi0, s->n_dih); E->s.dih_phi0 = E->dih_phi0.data();
+    cpi(E->imp_i, s->imp_i, s->n_imp); E->s.imp_i = E->imp_i.data();
+    cpi(E->imp_j, s->imp_j, s->n_imp); E->s.imp_j = E->imp_j.data();
+    cpi(E->imp_k, s->imp_k, s->n_imp); E->s.imp_k = E->imp_k.data();
+    cpi(E->imp_l, s->imp_l, s->n_imp); E->s.imp_l = E->imp_l.data();
+    cpd(E->imp_kphi, s->imp_kphi, s->n_imp); E->s.imp_kphi = E->imp_kphi.data();
+    cpd(E->imp_phi0, s->imp_phi0, s->n_imp); E->s.imp_phi0 = E->imp_phi0.data();
     E->run = *r;
     E->L = s->box;
     E->dt = r->dt;

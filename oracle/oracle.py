@@ -53,14 +53,16 @@ class orc_system(C.Structure):
         ("ang_t0", _dp),
         ("n_dih", C.c_int), ("dih_i", _ip), ("dih_j", _ip), ("dih_k", _ip), ("dih_l", _ip),
         ("dih_n", _ip), ("dih_kphi", _dp), ("dih_phi0", _dp),
+        ("n_imp", C.c_int), ("imp_i", _ip), ("imp_j", _ip), ("imp_k", _ip), ("imp_l", _ip),
+        ("imp_kphi", _dp), ("imp_phi0", _dp),
         ("profile", C.c_int),
     ]
 
 
 class orc_energy(C.Structure):
     _fields_ = [(k, C.c_double) for k in ("lj", "coul_real", "coul_recip", "coul_self",
-                                          "coul_excl", "bond", "angle", "dihedral", "total",
-                                          "virial")]
+                                          "coul_excl", "bond", "angle", "dihedral", "improper",
+                                          "total", "virial")]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -132,6 +134,11 @@ class _Sys:
                                                   i(cfg.dihedral_k), i(cfg.dihedral_l))
             s.dih_n, s.dih_kphi, s.dih_phi0 = (i(cfg.dihedral_periodicity), d(cfg.dihedral_k_phi),
                                                d(cfg.dihedral_phi0))
+        s.n_imp = len(cfg.improper_i)
+        if s.n_imp:
+            s.imp_i, s.imp_j, s.imp_k, s.imp_l = (i(cfg.improper_i), i(cfg.improper_j),
+                                                  i(cfg.improper_k), i(cfg.improper_l))
+            s.imp_kphi, s.imp_phi0 = d(cfg.improper_k_phi), d(cfg.improper_phi0)
         s.profile = {"ref": 0, "phys": 1}[profile]
         self.s = s
         self._k = k
@@ -322,6 +329,8 @@ class ref_run_desc(C.Structure):
         ("ang_t0", _dp),
         ("n_dih", C.c_int), ("dih_i", _ip), ("dih_j", _ip), ("dih_k", _ip), ("dih_l", _ip),
         ("dih_n", _ip), ("dih_kphi", _dp), ("dih_phi0", _dp),
+        ("n_imp", C.c_int), ("imp_i", _ip), ("imp_j", _ip), ("imp_k", _ip), ("imp_l", _ip),
+        ("imp_kphi", _dp), ("imp_phi0", _dp),
         ("n_excl", C.c_int), ("excl_i", _ip), ("excl_j", _ip),
         ("coulomb_type", C.c_int), ("coul_cutoff", C.c_double), ("ewald", C.c_double),
         ("pme_spacing", C.c_double), ("pme_order", C.c_int),
@@ -358,6 +367,8 @@ class Ref:
                                  _dp, _dp, _dp]),
             "ref_dihedral": (None, [C.c_int, _dp, _dp, _dp, D, C.c_int, _ip, _ip, _ip, _ip, _ip, _dp,
                                     _dp, _dp, _dp, _dp, _dp]),
+            "ref_improper": (None, [C.c_int, _dp, _dp, _dp, D, C.c_int, _ip, _ip, _ip, _ip, _dp, _dp,
+                                    _dp, _dp, _dp, _dp]),
             "ref_kinetic_energy": (D, [C.c_int, _dp, _dp, _dp, _dp]),
             "ref_temperature": (D, [D, C.c_int]),
             "ref_engine_create": (vp, [C.POINTER(ref_run_desc)]),
@@ -427,6 +438,13 @@ class Ref:
              _i(cfg.dihedral_periodicity), _d(cfg.dihedral_k_phi), _d(cfg.dihedral_phi0)]
         return self._bonded(self.L.ref_dihedral, pos, box or cfg.box_size, len(pos),
                             len(cfg.dihedral_i), *[p for _, p in a])
+
+    def improper(self, cfg, pos=None, box=None):
+        pos = np.stack([cfg.pos_x, cfg.pos_y, cfg.pos_z], 1) if pos is None else pos
+        a = [_i(cfg.improper_i), _i(cfg.improper_j), _i(cfg.improper_k), _i(cfg.improper_l),
+             _d(cfg.improper_k_phi), _d(cfg.improper_phi0)]
+        return self._bonded(self.L.ref_improper, pos, box or cfg.box_size, len(pos),
+                            len(cfg.improper_i), *[p for _, p in a])
 
     def exclusion(self, cfg, pos=None, box=None):
         pos = np.stack([cfg.pos_x, cfg.pos_y, cfg.pos_z], 1) if pos is None else pos
@@ -498,6 +516,11 @@ class RefEngine:
                                                   i(cfg.dihedral_k), i(cfg.dihedral_l))
             s.dih_n, s.dih_kphi, s.dih_phi0 = (i(cfg.dihedral_periodicity), d(cfg.dihedral_k_phi),
                                                d(cfg.dihedral_phi0))
+        s.n_imp = len(cfg.improper_i)
+        if s.n_imp:
+            s.imp_i, s.imp_j, s.imp_k, s.imp_l = (i(cfg.improper_i), i(cfg.improper_j),
+                                                  i(cfg.improper_k), i(cfg.improper_l))
+            s.imp_kphi, s.imp_phi0 = d(cfg.improper_k_phi), d(cfg.improper_phi0)
         s.n_excl = len(cfg.excl_i)
         if s.n_excl:
             s.excl_i, s.excl_j = i(cfg.excl_i), i(cfg.excl_j)

@@ -197,6 +197,24 @@ void ref_dihedral(int n, const double* x, const double* y, const double* z, doub
               std::span<double>(fy, n), std::span<double>(fz, n), *energy);
 }
 
+void ref_improper(int n, const double* x, const double* y, const double* z, double L, int ni,
+                  const int* ii, const int* ij, const int* ik, const int* il, const double* kphi,
+                  const double* phi0, double* fx, double* fy, double* fz, double* energy) {
+    ImproperParams p;
+    p.n = ni;
+    p.i = veci(ii, ni);
+    p.j = veci(ij, ni);
+    p.k = veci(ik, ni);
+    p.l = veci(il, ni);
+    p.k_phi = vec(kphi, ni);
+    p.phi0 = vec(phi0, ni);
+    HarmonicImproper im(std::move(p));
+    Cell cell(L, L, L);
+    im.compute(std::span<const double>(x, n), std::span<const double>(y, n),
+               std::span<const double>(z, n), cell, std::span<double>(fx, n),
+               std::span<double>(fy, n), std::span<double>(fz, n), *energy);
+}
+
 // ---- thermostat / barostat helpers ---------------------------------------
 double ref_kinetic_energy(int n, const double* m, const double* vx, const double* vy,
                           const double* vz) {
@@ -240,6 +258,9 @@ struct ref_run_desc {
     int n_dih;
     const int *dih_i, *dih_j, *dih_k, *dih_l, *dih_n;
     const double *dih_kphi, *dih_phi0;
+    int n_imp;
+    const int *imp_i, *imp_j, *imp_k, *imp_l;
+    const double *imp_kphi, *imp_phi0;
     int n_excl;
     const int *excl_i, *excl_j;
     int coulomb_type;  // 0 = cutoff/direct, 1 = pme
@@ -299,6 +320,17 @@ void* ref_engine_create(const ref_run_desc* d) {
         p.k_phi = vec(d->dih_kphi, d->n_dih);
         p.phi0 = vec(d->dih_phi0, d->n_dih);
         e->fe->add_component(std::make_unique<PeriodicDihedral>(std::move(p)));
+    }
+    if (d->n_imp > 0) {
+        ImproperParams p;
+        p.n = d->n_imp;
+        p.i = veci(d->imp_i, d->n_imp);
+        p.j = veci(d->imp_j, d->n_imp);
+        p.k = veci(d->imp_k, d->n_imp);
+        p.l = veci(d->imp_l, d->n_imp);
+        p.k_phi = vec(d->imp_kphi, d->n_imp);
+        p.phi0 = vec(d->imp_phi0, d->n_imp);
+        e->fe->add_component(std::make_unique<HarmonicImproper>(std::move(p)));
     }
     CoulombDirect* cd = nullptr;
     CoulombExclusion* ce = nullptr;

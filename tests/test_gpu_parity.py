@@ -36,8 +36,8 @@ def _water(n_mol=1000, seed=3):
     return W.water_box(n_mol=n_mol, box=box, seed=seed, spacing=box / round(box / 0.1045)).config()
 
 
-def _decane(n=30, seed=5):
-    return W.decane_melt(n, seed).config()
+def _decane(n=30, seed=5, impropers=False):
+    return W.decane_melt(n, seed, impropers=impropers).config()
 
 
 def _jitter(cfg, s=0.01, seed=0):
@@ -50,7 +50,7 @@ def _jitter(cfg, s=0.01, seed=0):
 
 
 SYSTEMS = {"argon": lambda: _jitter(_argon()), "water": lambda: _water(),
-           "decane": lambda: _jitter(_decane(), 0.005)}
+           "decane": lambda: _jitter(_decane(impropers=True), 0.005)}
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
@@ -68,13 +68,13 @@ def test_single_point_forces(oracle, system, profile, precision):
 
 
 COMPONENTS = [(0, "lj"), (1, "bond"), (2, "angle"), (3, "dihedral"), (4, "creal"), (5, "pme"),
-              (6, "excl")]
+              (6, "excl"), (7, "improper")]
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 @pytest.mark.parametrize("profile", ["ref", "phys"])
 def test_components_water_decane(oracle, profile, precision):
-    for cfg in (_jitter(_water(600), 0.01), _jitter(_decane(20), 0.005)):
+    for cfg in (_jitter(_water(600), 0.01), _jitter(_decane(20, impropers=True), 0.005)):
         pos = np.stack([cfg.pos_x, cfg.pos_y, cfg.pos_z], 1)
         eng = _engine(cfg, precision, profile)
         for comp, name in COMPONENTS:

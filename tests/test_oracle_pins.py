@@ -134,7 +134,7 @@ def test_components_bitwise_vs_reference(oracle, ref, which):
     elif which == "water":
         c = _small_water()
     else:
-        c = W.decane_melt(20, 5).config()
+        c = W.decane_melt(20, 5, impropers=True).config()
     rng = np.random.default_rng(2)
     pos = np.stack([c.pos_x, c.pos_y, c.pos_z], 1) + rng.normal(0, 0.005, (len(c.masses), 3))
     fr, er, _ = ref.lj(c, pos=pos)
@@ -151,6 +151,10 @@ def test_components_bitwise_vs_reference(oracle, ref, which):
     if len(c.dihedral_i):
         fr, er = ref.dihedral(c, pos=pos)
         fo, eo, _ = oracle.component(c, "ref", 3, pos=pos)
+        assert np.array_equal(fr, fo) and er == eo
+    if len(c.improper_i):
+        fr, er = ref.improper(c, pos=pos)
+        fo, eo, _ = oracle.component(c, "ref", 7, pos=pos)
         assert np.array_equal(fr, fo) and er == eo
     if len(c.excl_i):
         fr, er = ref.exclusion(c, pos=pos)
@@ -252,11 +256,11 @@ def _fd_check(oracle, c, comp, n_check=6, h=1e-6, tol=2e-6, seed=0):
 
 
 def test_phys_fd_bonded(oracle):
-    c = W.decane_melt(4, 9).config()
+    c = W.decane_melt(4, 9, impropers=True).config()
     rng = np.random.default_rng(5)
     c.pos_x = c.pos_x + rng.normal(0, 0.01, len(c.pos_x))
     c.pos_y = c.pos_y + rng.normal(0, 0.01, len(c.pos_x))
-    for comp in (1, 2, 3):
+    for comp in (1, 2, 3, 7):
         _fd_check(oracle, c, comp, n_check=10, tol=5e-6)
 
 
