@@ -61,8 +61,9 @@ CPU_MAX_ATOMS = 100_000             # above this the reference's O(N^2) list bui
 # Argon (rc 1.0 nm, 21.0 atoms/nm^3, 44 half-neighbours): 241 B, 1,675 FLOP.
 PAIR_WORK = {"water": (650.0, 14690.0), "argon": (241.0, 1675.0)}
 # DRAM bytes (read + write) of one pair-kernel launch, from the ncu captures in
-# profiles/ (water 30k: 7.05 MB read, 0 written -- the working set stays in L2).
-PAIR_DRAM_BYTES = {"water30k": 7.05e6}
+# profiles/ (water 30k: 7.05 MB read, 0 written -- the working set stays in L2;
+# water 750k: 177.3 + 13.1 MB; the 256-replica batch: 214.0 + 35.0 MB).
+PAIR_DRAM_BYTES = {"water30k": 7.05e6, "water750k": 190.4e6, "batch256": 249.0e6}
 
 
 def lj_pair_work(n: int, box: float, rc: float, flop_per_pair: float = 38.0):
@@ -440,7 +441,7 @@ def run_batch(args, R: Ranks):
         ba, fa = lj_pair_work(w.n_atoms, c.box_size, c.lj_cutoff)
         b_alg += ba * w.n_atoms
         f_alg += fa * w.n_atoms
-    roof = roofline(b_alg, f_alg, nb_ms, clocks, None,
+    roof = roofline(b_alg, f_alg, nb_ms, clocks, PAIR_DRAM_BYTES["batch256"],
                     "k_nb_f32 (LJ pair kernel over all 256 replicas in one launch)", False,
                     "average over the timed steps, one launch covers every replica")
     n_lj = sum(1 for w in ws_ if w.name.startswith("lj_"))

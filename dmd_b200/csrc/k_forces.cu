@@ -271,8 +271,11 @@ __device__ __forceinline__ void mesh_coord(double x, double invL, int K, int& m0
     m0 = static_cast<int>(floor(u)) - 1;
 }
 
-// 16 threads per atom: thread (iz, iy) = (sub >> 2, sub & 3) adds the atom's
-// 4 mesh points along x of one (y, z) row of its 4x4x4 stencil.
+// 16 threads per atom: thread (iy, ix) = (sub >> 2, sub & 3) adds the atom's
+// 4 mesh points along z at (x, y).  A warp instruction then covers 4
+// consecutive x of 8 rows, so the L2 sees a few contiguous sectors per
+// instruction instead of 32 scattered ones.  Each contribution is rounded to
+// the fixed-point mesh on its own; the integer sums do not depend on order.
 template <typename T>
 __global__ void k_pme_spread(Dev d) {
     const long long t = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -285,29 +288,27 @@ __global__ void k_pme_spread(Dev d) {
     const double q = d.q[a];
     if (q == 0.0) return;
     const int K = R.pme_K;
-    const int iz = (threadIdx.x >> 2) & 3, iy = threadIdx.x & 3;
+    const int ix = threadIdx.x & 3, iy = (threadIdx.x >> 2) & 3;
     int m0[3];
     double u[3];
     mesh_coord(d.x[a], s->invL, K, m0[0], u[0]);
     mesh_coord(d.y[a], s->invL, K, m0[1], u[1]);
     mesh_coord(d.z[a], s->invL, K, m0[2], u[2]);
-    T wx[4];
-#pragma unroll
-    for (int j = 0; j < 4; ++j) wx[j] = theta4<T>((T)(u[0] - (m0[0] + j)));
+    const T wx = theta4<T>((T)(u[0] - (m0[0] + ix)));
     const T wy = theta4<T>((T)(u[1] - (m0[1] + iy)));
-    const T wz = theta4<T>((T)(u[2] - (m0[2] + iz)));
     long long* mesh = d.mesh_fix + R.mesh_fix_off;
     const T qt = (T)q;
-    // m0 + j lies in [-1, K + 2]: one conditional wrap per index
-    const int gz = wrap_mesh(m0[2] + iz, K), gy = wrap_mesh(m0[1] + iy, K);
-    const T wyz = wy * wz;
-    // grid_[gz*ny*nx + gy*nx + gx] (coulomb_pme.cpp:131); the REF buffer is
-    // K*K*2(K/2+1) long, the PHYS one K^3: the index is the same.
-    const long long row = (static_cast<long long>(gz) * K + gy) * K;
+    const T qwx = qt * wx;
+    // m0 + j lies in [-1, K + 2]: one conditional wrap per index.  grid_[gz*ny*nx +
+    // gy*nx + gx] (coulomb_pme.cpp:131); the REF buffer is K*K*2(K/2+1) long, the
+    // PHYS one K^3: the index is the same.
+    const int gx = wrap_mesh(m0[0] + ix, K), gy = wrap_mesh(m0[1] + iy, K);
 #pragma unroll
-    for (int ix = 0; ix < 4; ++ix) {
-        const int gx = wrap_mesh(m0[0] + ix, K);
-        fix_add(mesh + row + gx, __double2ll_rn(static_cast<double>(qt * wx[ix] * wyz) * MSCALE));
+    for (int iz = 0; iz < 4; ++iz) {
+        const T wz = theta4<T>((T)(u[2] - (m0[2] + iz)));
+        const int gz = wrap_mesh(m0[2] + iz, K);
+        const long long idx = (static_cast<long long>(gz) * K + gy) * K + gx;
+        fix_add(mesh + idx, __double2ll_rn(static_cast<double>(qwx * (wy * wz)) * MSCALE));
     }
 }
 
@@ -427,8 +428,9 @@ __global__ void k_pme_influence(Dev d) {
 // interpolate_forces (coulomb_pme.cpp:205-283).  REF reads the potential with
 // the unpadded index from FFTW's padded buffer (padding reads as zero) and
 // scales it by 1/N (:303-306); PHYS reads the natural layout, unscaled.
-// 16 threads per atom as in the spread: each sums its row of 4 points, then the
-// group of 16 lanes reduces in a fixed butterfly order.
+// 16 threads per atom: thread (iz, iy) = (sub >> 2, sub & 3) sums its row of 4
+// points along x (adjacent addresses), then the atom's 16 lanes reduce in a
+// fixed butterfly order.
 template <typename T>
 __global__ void k_pme_gather(Dev d) {
     const long long t = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;

@@ -26,6 +26,8 @@ def main():
     ap.add_argument("--show", type=int, default=3, help="steps printed kernel by kernel")
     ap.add_argument("--workload", default="water30k",
                     choices=["water30k", "water750k", "argon4k", "batch256"])
+    ap.add_argument("--plain", action="store_true",
+                    help="run the steps without the profiler (a target for ncu)")
     args = ap.parse_args()
     import torch
     from torch.profiler import ProfilerActivity, profile
@@ -40,6 +42,9 @@ def main():
         for w in W.batch_256():
             eng.admit(w.config(), args.warmup + args.steps)
         eng.step(args.warmup)
+        if args.plain:
+            eng.step(args.steps)
+            return
         with profile(activities=[ProfilerActivity.CUDA]) as prof:
             eng.step(args.steps)
     else:
@@ -54,6 +59,10 @@ def main():
         eng = Engine(w.config(), precision=args.precision, profile="phys")
         eng.run_n(args.warmup)
         eng.positions
+        if args.plain:
+            eng.run_n(args.steps)
+            eng.positions
+            return
         with profile(activities=[ProfilerActivity.CUDA]) as prof:
             eng.run_n(args.steps)
             eng.positions
