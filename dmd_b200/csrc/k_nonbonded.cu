@@ -193,7 +193,29 @@ __device__ __forceinline__ void nb_chunk(const Dev& d, const Rep& R, RepState* s
             const float4 pj = px[u];
             const float4 p = lj[pt[u]];
             const float dx = pj.x - xi.x, dy = pj.y - xi.y, dz = pj.z - xi.z;
-            const float r2 = fmaxf(dx * dx + dy * dy + dz * dz, 1e-6f);
+            const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+            if (!ENERGY && (!PHYS || SAME)) {
+                // one cutoff: evaluate with the table coefficients and keep the
+                // force only for interacting pairs (a masked self pair of a
+                // diagonal chunk gives a non-finite f, which the select drops)
+                const bool near = bit & (fabsf(d2 - rl2) < wl);
+                const bool in = bit & !near & (d2 < rl2);
+                b8 |= static_cast<uint32_t>(near) << u;
+                float ir6, rinv, erfc_ar;
+                const float fa = pair_f<PHYS>(d2, p.z, p.w, keqi * pj.w, alpha, a2l2e, c2a, ir6, rinv, erfc_ar);
+                const float f = in ? fa : 0.f;
+                fix = fmaf(-f, dx, fix);
+                fiy = fmaf(-f, dy, fiy);
+                fiz = fmaf(-f, dz, fiz);
+                fjx = fmaf(f, dx, fjx);
+                fjy = fmaf(f, dy, fjy);
+                fjz = fmaf(f, dz, fjz);
+                fjx = __shfl_sync(FULL, fjx, src_lane);
+                fjy = __shfl_sync(FULL, fjy, src_lane);
+                fjz = __shfl_sync(FULL, fjz, src_lane);
+                continue;
+            }
+            const float r2 = fmaxf(d2, 1e-6f);
             bool near, in_l, in_c;
             if (!PHYS || SAME) {
                 near = bit & (fabsf(r2 - rl2) < wl);
@@ -241,7 +263,7 @@ __device__ __forceinline__ void nb_chunk(const Dev& d, const Rep& R, RepState* s
         const bool in_l = has_lj && exact_inside(d, ai, aj2, L, s->invL, R.rc_lj2);
         const bool in_c = has_c && exact_inside(d, ai, aj2, L, s->invL, R.rc_c2);
         const float dx = pj.x - xi.x, dy = pj.y - xi.y, dz = pj.z - xi.z;
-        const float r2 = fmaxf(dx * dx + dy * dy + dz * dz, 1e-6f);
+        const float r2 = fmaxf(fmaf(dz, dz, fmaf(dy, dy, dx * dx)), 1e-6f);
         const float qq = (PHYS && in_c) ? keqi * pj.w : 0.f;
         float ir6, rinv, erfc_ar;
         const float f = pair_f<PHYS>(r2, in_l ? p.z : 0.f, in_l ? p.w : 0.f, qq, alpha, a2l2e, c2a, ir6,
@@ -281,17 +303,18 @@ __device__ __forceinline__ void nb_chunk(const Dev& d, const Rep& R, RepState* s
 // from global memory).
 constexpr int LJ_SMEM = 512;
 
-template <bool PHYS>
+// LJS: the LJ table fits LJ_SMEM and is staged in shared memory (a compile-time
+// choice, so the table loads are shared-memory loads).
+template <bool PHYS, bool LJS>
 __global__ void __launch_bounds__(256, 3) k_nb_f32(Dev d) {
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
     __shared__ ChunkStage s_stage[8];
-    __shared__ float4 s_lj[LJ_SMEM];
-    const bool lj_shared = d.n_lj <= LJ_SMEM;
-    if (lj_shared)
+    __shared__ float4 s_lj[LJS ? LJ_SMEM : 1];
+    if (LJS)
         for (int k = threadIdx.x; k < d.n_lj; k += blockDim.x) s_lj[k] = d.lj32[k];
     __syncthreads();
-    const float4* lj_tab = lj_shared ? s_lj : d.lj32;
+    const float4* lj_tab = LJS ? s_lj : d.lj32;
     const int total = d.chunk_prefix[d.n_rep];
     Acc acc{0, 0, 0};
     int cur = -1;
@@ -440,8 +463,14 @@ void launch_nonbonded(const Dev& d, bool fp64, bool phys, int n_sm, int blocks_p
         // persistent: up to the 3 blocks per SM its registers allow; fewer leave
         // room on every SM for the bonded / PME kernels running alongside
         const int g = n_sm * std::min(std::max(blocks_per_sm, 1), 3);
-        if (phys) k_nb_f32<true><<<g, 256, 0, st>>>(d);
-        else k_nb_f32<false><<<g, 256, 0, st>>>(d);
+        const bool ljs = d.n_lj <= LJ_SMEM;
+        if (phys) {
+            if (ljs) k_nb_f32<true, true><<<g, 256, 0, st>>>(d);
+            else k_nb_f32<true, false><<<g, 256, 0, st>>>(d);
+        } else {
+            if (ljs) k_nb_f32<false, true><<<g, 256, 0, st>>>(d);
+            else k_nb_f32<false, false><<<g, 256, 0, st>>>(d);
+        }
     }
     *nlaunch += 1;
 }
