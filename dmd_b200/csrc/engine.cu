@@ -927,7 +927,8 @@ void Batch::enqueue_eval(int pass) {
         prof_nb_->emplace_back(e0, e1);
     }
     cudaStreamWaitEvent(stream_, ev_join_, 0);
-    launch_eval_end(d, stream_, &launches_);
+    // the second pass of a step is closed by k_replica_update
+    if (pass != PASS_SECOND) launch_eval_end(d, stream_, &launches_);
 }
 
 // Neighbour-list rebuild: one cooperative launch that returns at once unless
@@ -935,7 +936,6 @@ void Batch::enqueue_eval(int pass) {
 void Batch::enqueue_rebuild() { launch_rebuild(dev_, d_bin_rep_, n_sm_, stream_, &launches_); }
 
 void Batch::enqueue_step() {
-    launch_step_begin(dev_, stream_, &launches_);
     // The first evaluation repeats the previous step's second one unless the
     // barostat moved the atoms, the REF list cadence rebuilds now, or no forces
     // exist yet; only then is it issued (its kernels skip replicas that do not need it).

@@ -3,18 +3,19 @@
 // Reference sequence (SimulationEngine::step, src/sim/simulation_engine.cpp:53-86):
 //   compute; half_kick; advance; compute; half_kick; thermostat; barostat.
 // Device form (per step, every replica of the batch in the same launches):
-//   k_step_begin        which replicas advance
 //   [eval #1]           only where the first evaluation would differ from the
 //                       previous step's second one (REF barostat moved the atoms,
 //                       no forces yet, or the REF list cadence rebuilds now)
 //   k_kick_drift        pending thermostat scale, half kick, PHYS pending
 //                       barostat scale, drift, clear forces, write the sorted
-//                       FP32/FP64 mirror, skin check
-//   [eval #2]           (its k_eval_begin scales the PHYS box to match)
+//                       FP32/FP64 mirror, skin check (replicas with step < target)
+//   [eval #2]           (its k_eval_begin marks the replicas that advance and
+//                       scales the PHYS box to match the drift)
 //   k_kick2             half kick (+ Andersen), per-tile KE / virial partials
-//   k_replica_update    KE, thermostat (Berendsen / Nose-Hoover scale, applied
-//                       lazily in the next kick), Berendsen barostat factor
-//                       (REF: applied now; PHYS: pending for the next drift)
+//   k_replica_update    closes eval #2, KE, thermostat (Berendsen / Nose-Hoover
+//                       scale, applied lazily in the next kick), Berendsen
+//                       barostat factor (REF: applied now; PHYS: pending for the
+//                       next drift)
 //   k_apply_scale       REF barostat position scaling (only when a barostat exists)
 // PHYS therefore evaluates forces once per step with or without a barostat:
 // the first kick of a step uses the forces of the previous evaluation and the
@@ -29,17 +30,6 @@ namespace dmd {
 
 namespace {
 
-__global__ void k_step_begin(Dev d) {
-    int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= d.n_rep) return;
-    RepState* s = d.st + r;
-    s->active = (s->step < s->target_step) ? 1 : 0;
-    // PHYS keeps the barostat scale chosen at the end of the previous step: it is
-    // applied to the positions by k_kick_drift and to the box by k_eval_begin
-    // (second pass), so an evaluation before the drift sees the unscaled pair.
-    if (!(d.rep[r].flags & F_PHYS)) s->pscale = 1.0;
-}
-
 __global__ void k_eval_begin(Dev d, int pass) {
     int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r == 0) {
@@ -50,6 +40,12 @@ __global__ void k_eval_begin(Dev d, int pass) {
     RepState* s = d.st + r;
     const Rep& R = d.rep[r];
     const bool ref_lj = !(R.flags & F_PHYS) && (R.flags & F_LJ);
+    // which replicas advance this step (the host may have moved the targets)
+    if (pass != PASS_SINGLE) s->active = (s->step < s->target_step) ? 1 : 0;
+    // REF: the barostat scale of the previous step has been applied; PHYS keeps
+    // its pending scale for k_kick_drift (positions) and the second pass (box),
+    // so an evaluation before the drift sees the unscaled pair.
+    if (pass == PASS_FIRST && !(R.flags & F_PHYS)) s->pscale = 1.0;
     int ev;
     if (pass == PASS_FIRST) {
         ev = s->active && ((R.barostat != 0 && !(R.flags & F_PHYS)) || !s->have_forces ||
@@ -147,7 +143,7 @@ __global__ void k_kick_drift(Dev d) {
     if (a >= d.n_atoms) return;
     const int r = d.atom_rep[a];
     RepState* s = d.st + r;
-    if (!s->active) return;
+    if (!(s->step < s->target_step)) return;  // runs before this step's k_eval_begin
     const int slot = d.slot_of_atom[a];
     const Rep& R = d.rep[r];
     const double dt = R.dt, half_dt = 0.5 * dt;
@@ -298,23 +294,57 @@ __global__ void k_energy_reduce(Dev d) {
     reduce_pme(d, r, sh);
 }
 
+// Four block-wide sums at once in a fixed order: lane sums by shuffles, then
+// the block's warps in order by warp 0 (blockDim.x = 256).
+__device__ void block_sum4(double v[4], double (*sh)[4]) {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) v[k] = warp_sum_d(v[k]);
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0)
+        for (int k = 0; k < 4; ++k) sh[w][k] = v[k];
+    __syncthreads();
+    if (w == 0) {
+        const int nw = blockDim.x >> 5;
+        for (int k = 0; k < 4; ++k) {
+            double x = (lane < nw) ? sh[lane][k] : 0.0;
+#pragma unroll
+            for (int o = 4; o > 0; o >>= 1) x += __shfl_xor_sync(FULL, x, o);
+            v[k] = x;
+        }
+    }
+}
+
 // Thermostat (berendsen.cpp:13-28, nose_hoover.cpp:6-32) and Berendsen barostat
-// (berendsen_barostat.cpp:14-66); one block per replica.
+// (berendsen_barostat.cpp:14-66); one block per replica.  Tile partials of KE
+// and r.F and the PME blocks' energy / virial partials are summed together.
 __global__ void k_replica_update(Dev d) {
-    __shared__ double sh[256];
+    __shared__ double sh[8][4];
     const int r = blockIdx.x;
     RepState* s = d.st + r;
     if (!s->active) return;
     const Rep& R = d.rep[r];
-    double ke = 0.0, w = 0.0;
+    double v[4] = {0.0, 0.0, 0.0, 0.0};
     for (int t = R.tile_begin + threadIdx.x; t < R.tile_begin + R.n_tiles; t += blockDim.x) {
-        ke += d.tile_ke[t];
-        w += d.tile_vir[t];
+        v[0] += d.tile_ke[t];
+        v[1] += d.tile_vir[t];
     }
-    ke = block_sum(ke, sh);
-    w = block_sum(w, sh);
-    reduce_pme(d, r, sh);
+    if (R.flags & F_PME) {
+        for (int b = threadIdx.x; b < R.pme_blocks; b += blockDim.x) {
+            v[2] += d.pme_part[2 * (R.pme_block_begin + b)];
+            v[3] += d.pme_part[2 * (R.pme_block_begin + b) + 1];
+        }
+    }
+    block_sum4(v, sh);
     if (threadIdx.x != 0) return;
+    const double ke = v[0], w = v[1];
+    s->e_recip = v[2];
+    s->vir_recip = v[3];
+    // end of the step's second evaluation (k_eval_end's work, at the box it used)
+    if (s->eval) {
+        if (!(R.flags & F_PHYS) && (R.flags & F_LJ)) s->lj_counter += 1;
+        s->have_forces = 1;
+        if (R.flags & F_PME) s->green_L = s->L;
+    }
     const double n = static_cast<double>(R.n_atoms);
     const double dt = R.dt;
     auto temp = [&](double ek) { return R.n_atoms < 2 ? 0.0 : 2.0 * ek / ((3.0 * n - 3.0) * KB); };
@@ -402,10 +432,6 @@ __global__ void k_write_mirror(Dev d) {
 
 }  // namespace
 
-void launch_step_begin(const Dev& d, cudaStream_t st, long long* n) {
-    k_step_begin<<<(d.n_rep + 127) / 128, 128, 0, st>>>(d);
-    ++*n;
-}
 void launch_eval_begin(const Dev& d, int pass, cudaStream_t st, long long* n) {
     k_eval_begin<<<(d.n_rep + 127) / 128, 128, 0, st>>>(d, pass);
     ++*n;

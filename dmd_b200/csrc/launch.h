@@ -31,7 +31,6 @@ void launch_pme_gather(const Dev& d, bool fp64, cudaStream_t st, long long* nlau
 
 // k_integrate.cu
 enum EvalPass { PASS_FIRST = 1, PASS_SECOND = 2, PASS_SINGLE = 3 };
-void launch_step_begin(const Dev& d, cudaStream_t st, long long* nlaunch);
 void launch_eval_begin(const Dev& d, int pass, cudaStream_t st, long long* nlaunch);
 void launch_clear_forces(const Dev& d, cudaStream_t st, long long* nlaunch);
 void launch_eval_end(const Dev& d, cudaStream_t st, long long* nlaunch);

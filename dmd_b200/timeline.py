@@ -72,7 +72,7 @@ def main():
     def short(name):
         return name.replace("void ", "").replace("dmd::(anonymous namespace)::", "").replace("dmd::", "")[:44]
 
-    starts = [e.time_range.start for e in ev if "k_step_begin" in e.name]
+    starts = [e.time_range.start for e in ev if "k_kick_drift" in e.name]
     if len(starts) > 1:
         print(f"steps {len(starts)}  mean step period {(starts[-1] - starts[0]) / (len(starts) - 1):.1f} us")
     for si in range(min(args.show, max(len(starts) - 1, 0))):
