@@ -126,6 +126,9 @@ void Batch::free_device() {
     arena_.reset();
     if (h_st_) cudaFreeHost(h_st_);
     h_st_ = nullptr;
+    if (h_tgt_) cudaFreeHost(h_tgt_);
+    h_tgt_ = nullptr;
+    st_fresh_ = false;
     if (h_and_flag_) cudaFreeHost(h_and_flag_);
     if (h_and_v_) cudaFreeHost(h_and_v_);
     h_and_flag_ = nullptr;
@@ -834,6 +837,8 @@ int Batch::pack() {
         return fail(DMDGPU_ERR_OOM, std::string("device allocation/upload failed: ") + e.what());
     }
     CK(cudaMallocHost(&h_st_, sizeof(RepState) * R));
+    CK(cudaMallocHost(&h_tgt_, sizeof(long long) * R));
+    st_fresh_ = false;
     // cuFFT plans per mesh size
     for (int k = 0; k < R; ++k) {
         const Rep& P = reps_[order_[k]]->rep;
@@ -977,6 +982,7 @@ void Batch::andersen_ref_prepare() {
 }
 
 int Batch::run_steps(int n) {
+    st_fresh_ = false;  // device work follows: the host mirror is stale
     if (n <= 0) return DMDGPU_OK;
     static const bool eager = [] {
         const char* e = std::getenv("DMD_EAGER");
@@ -1086,6 +1092,7 @@ int Batch::sync_status() {
     if (!packed_ || order_.empty()) return DMDGPU_OK;
     CK(cudaMemcpyAsync(h_st_, d_st_, sizeof(RepState) * order_.size(), cudaMemcpyDeviceToHost, stream_));
     CK(cudaStreamSynchronize(stream_));
+    st_fresh_ = true;
     int rc = DMDGPU_OK;
     for (size_t k = 0; k < order_.size(); ++k) {
         HostRep& h = *reps_[order_[k]];
@@ -1129,12 +1136,20 @@ int Batch::extend_targets(long long n) {
         int rc = pack();
         if (rc) return rc;
     }
-    CK(cudaStreamSynchronize(stream_));
+    if (order_.empty()) return DMDGPU_OK;
+    // The step counters come from the host mirror when nothing ran since it was
+    // read (the common run_n loop: no device round trip); the new targets go
+    // to the device asynchronously from pinned memory, ahead of the next step.
+    if (!st_fresh_) {
+        CK(cudaMemcpyAsync(h_st_, d_st_, sizeof(RepState) * order_.size(), cudaMemcpyDeviceToHost, stream_));
+        CK(cudaStreamSynchronize(stream_));
+        st_fresh_ = true;
+    }
     for (size_t k = 0; k < order_.size(); ++k) {
-        long long cur = 0;
-        CK(cudaMemcpy(&cur, &d_st_[k].step, 8, cudaMemcpyDeviceToHost));
-        long long tgt = cur + n;
-        CK(cudaMemcpy(&d_st_[k].target_step, &tgt, 8, cudaMemcpyHostToDevice));
+        const long long tgt = h_st_[k].step + n;
+        h_tgt_[k] = tgt;
+        h_st_[k].target_step = tgt;
+        CK(cudaMemcpyAsync(&d_st_[k].target_step, h_tgt_ + k, 8, cudaMemcpyHostToDevice, stream_));
         reps_[order_[k]]->target = tgt;
         reps_[order_[k]]->done = false;
     }
@@ -1153,6 +1168,7 @@ void Batch::record(cudaEvent_t e, cudaStream_t st) {
 // n steps as one captured graph with timing events around every step and every
 // non-bonded / PME launch; optional L2 flush between steps (outside the events).
 int Batch::step_timed(int n, long long flush_bytes, dmdgpu_timing* out) {
+    st_fresh_ = false;  // device work follows: the host mirror is stale
     CK(cudaSetDevice(device_));
     std::memset(out, 0, sizeof(*out));
     if (!packed_) {
@@ -1252,6 +1268,7 @@ int Batch::poll(int32_t* slots, int cap, int* n_done) {
 // State access
 // ---------------------------------------------------------------------------
 int Batch::get_state(int slot, int which, double* x, double* y, double* z) {
+    st_fresh_ = false;  // device work follows: the host mirror is stale
     CK(cudaSetDevice(device_));
     if (!has(slot)) return fail(DMDGPU_ERR_INVALID, "no such slot");
     if (!packed_) {
@@ -1299,6 +1316,7 @@ int Batch::get_state(int slot, int which, double* x, double* y, double* z) {
 }
 
 int Batch::set_state(int slot, int which, const double* x, const double* y, const double* z) {
+    st_fresh_ = false;  // device work follows: the host mirror is stale
     CK(cudaSetDevice(device_));
     if (!has(slot)) return fail(DMDGPU_ERR_INVALID, "no such slot");
     if (!packed_) {
@@ -1338,8 +1356,10 @@ int Batch::get_scalars(int slot, dmdgpu_scalars* out) {
         if (rc) return rc;
     }
     const int k = replica_index(slot);
-    CK(cudaMemcpyAsync(h_st_ + k, d_st_ + k, sizeof(RepState), cudaMemcpyDeviceToHost, stream_));
-    CK(cudaStreamSynchronize(stream_));
+    if (!st_fresh_) {
+        CK(cudaMemcpyAsync(h_st_ + k, d_st_ + k, sizeof(RepState), cudaMemcpyDeviceToHost, stream_));
+        CK(cudaStreamSynchronize(stream_));
+    }
     const RepState& s = h_st_[k];
     const HostRep& h = *reps_[slot];
     const Rep& P = h.rep;
@@ -1377,6 +1397,7 @@ int Batch::get_scalars(int slot, dmdgpu_scalars* out) {
 }
 
 int Batch::compute_forces(int slot, double* fx, double* fy, double* fz, double* e_terms) {
+    st_fresh_ = false;  // device work follows: the host mirror is stale
     CK(cudaSetDevice(device_));
     if (!has(slot)) return fail(DMDGPU_ERR_INVALID, "no such slot");
     if (!packed_) {
@@ -1406,6 +1427,7 @@ int Batch::compute_forces(int slot, double* fx, double* fy, double* fz, double* 
 }
 
 int Batch::pair_list(int slot, int32_t* pi, int32_t* pj, long long cap, long long* count) {
+    st_fresh_ = false;  // device work follows: the host mirror is stale
     CK(cudaSetDevice(device_));
     if (!has(slot)) return fail(DMDGPU_ERR_INVALID, "no such slot");
     if (!packed_) {
@@ -1513,6 +1535,7 @@ int Batch::save_checkpoint(int slot, const char* path) {
 }
 
 int Batch::load_checkpoint(int slot, const char* path) {
+    st_fresh_ = false;  // device work follows: the host mirror is stale
     CK(cudaSetDevice(device_));
     if (!has(slot)) return fail(DMDGPU_ERR_INVALID, "no such slot");
     if (!packed_) {

@@ -132,6 +132,8 @@ class Batch {
     Rep* d_rep_ = nullptr;
     RepState* d_st_ = nullptr;
     RepState* h_st_ = nullptr;                      // pinned mirror of the state table
+    bool st_fresh_ = false;                         // h_st_ equals the device table (no work since)
+    long long* h_tgt_ = nullptr;                    // pinned step targets for extend_targets
     int* d_bin_rep_ = nullptr;
     long long n_fix_total_ = 0;
     int n_pme_blocks_ = 0;
