@@ -98,8 +98,10 @@ Batch::Batch(const dmdgpu_options& opt, long long budget) : opt_(opt), budget_(b
     if (cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi) != cudaSuccess ||
         cudaStreamCreateWithPriority(&stream_, cudaStreamNonBlocking, prio_hi) != cudaSuccess ||
         cudaStreamCreateWithPriority(&aux_stream_, cudaStreamNonBlocking, prio_lo) != cudaSuccess ||
+        cudaStreamCreateWithPriority(&bond_stream_, cudaStreamNonBlocking, prio_lo) != cudaSuccess ||
         cudaEventCreateWithFlags(&ev_fork_, cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&ev_join_, cudaEventDisableTiming) != cudaSuccess)
+        cudaEventCreateWithFlags(&ev_join_, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ev_join_b_, cudaEventDisableTiming) != cudaSuccess)
         throw std::runtime_error("cudaStreamCreate failed");
 }
 
@@ -110,6 +112,8 @@ Batch::~Batch() {
     for (cudaEvent_t e : ev_pool_) cudaEventDestroy(e);
     if (ev_fork_) cudaEventDestroy(ev_fork_);
     if (ev_join_) cudaEventDestroy(ev_join_);
+    if (ev_join_b_) cudaEventDestroy(ev_join_b_);
+    if (bond_stream_) cudaStreamDestroy(bond_stream_);
     if (aux_stream_) cudaStreamDestroy(aux_stream_);
     if (stream_) cudaStreamDestroy(stream_);
 }
@@ -875,12 +879,24 @@ void Batch::enqueue_eval(int pass) {
     // it returns at once on steps without a rebuild.
     enqueue_rebuild();
     // Bonded terms and PME depend on atom positions only (not on the sorted slots),
-    // so they run on aux_stream_ concurrently with the pair kernel; all force and
-    // energy sums are fixed-point atomics (order-free).
+    // so they run on two more streams concurrently with the pair kernel; all force
+    // and energy sums are fixed-point atomics (order-free).  The pair kernel (the
+    // longest branch, persistent) is issued first so its blocks take their SM
+    // slots before the short PME and bonded blocks fill the rest.
     cudaEventRecord(ev_fork_, stream_);
-    cudaStreamWaitEvent(aux_stream_, ev_fork_, 0);
     cudaEvent_t e0 = nullptr, e1 = nullptr;
-    launch_bonded(d, fp64_, phys_, aux_stream_, &launches_);
+    if (prof_nb_) {
+        e0 = next_event();
+        record(e0, stream_);
+    }
+    launch_nonbonded(d, fp64_, phys_, n_sm_, nb_blocks_per_sm_, stream_, &launches_);
+    if (prof_nb_) {
+        e1 = next_event();
+        record(e1, stream_);
+        prof_nb_->emplace_back(e0, e1);
+    }
+    cudaStreamWaitEvent(aux_stream_, ev_fork_, 0);
+    cudaStreamWaitEvent(bond_stream_, ev_fork_, 0);
     if (any_pme_) {
         if (prof_pme_) {
             e0 = next_event();
@@ -921,17 +937,10 @@ void Batch::enqueue_eval(int pass) {
         }
     }
     cudaEventRecord(ev_join_, aux_stream_);
-    if (prof_nb_) {
-        e0 = next_event();
-        record(e0, stream_);
-    }
-    launch_nonbonded(d, fp64_, phys_, n_sm_, nb_blocks_per_sm_, stream_, &launches_);
-    if (prof_nb_) {
-        e1 = next_event();
-        record(e1, stream_);
-        prof_nb_->emplace_back(e0, e1);
-    }
+    launch_bonded(d, fp64_, phys_, bond_stream_, &launches_);
+    cudaEventRecord(ev_join_b_, bond_stream_);
     cudaStreamWaitEvent(stream_, ev_join_, 0);
+    cudaStreamWaitEvent(stream_, ev_join_b_, 0);
     // the second pass of a step is closed by k_replica_update
     if (pass != PASS_SECOND) launch_eval_end(d, stream_, &launches_);
 }

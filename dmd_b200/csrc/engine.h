@@ -123,7 +123,9 @@ class Batch {
     cudaStream_t stream_ = nullptr;
     // bonded + PME run on aux_stream_, forked from and joined back to stream_
     cudaStream_t aux_stream_ = nullptr;
-    cudaEvent_t ev_fork_ = nullptr, ev_join_ = nullptr;
+    // bonded terms on a third stream, beside both
+    cudaStream_t bond_stream_ = nullptr;
+    cudaEvent_t ev_fork_ = nullptr, ev_join_ = nullptr, ev_join_b_ = nullptr;
     bool capture_error_ = false;
     std::vector<std::unique_ptr<HostRep>> reps_;   // indexed by slot (nullptr = free)
     std::vector<int> order_;                        // packed replica index -> slot

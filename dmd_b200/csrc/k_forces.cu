@@ -315,16 +315,19 @@ __global__ void k_pme_spread(Dev d) {
 // Fixed-point mesh -> real FFT input (K^3, natural layout); clears the fixed mesh.
 // REF: the FFT reads FFTW's padded in-place rows, i.e. element (z,y,x) of the real
 // array is fixed[(z*K + y)*P + x] with P = 2(K/2+1).
+// Four consecutive elements per thread (replica meshes start on 64-element
+// boundaries, so a group never straddles two replicas): 16-byte loads and
+// stores where the group lies inside one PHYS mesh.
 template <typename T>
 __global__ void k_pme_convert(Dev d, long long n_fix) {
-    const long long e = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (e >= n_fix) return;
-    // replica of fixed-mesh element e: linear scan over the (few) PME replicas;
-    // elements in the alignment gaps between replica meshes belong to none
+    const long long e0 = 4 * (static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x);
+    if (e0 >= n_fix) return;
+    // replica of the group: linear scan over the (few) PME replicas; groups in
+    // the alignment gaps between replica meshes belong to none
     int r = -1;
     for (int k = 0; k < d.n_rep; ++k) {
         const Rep& R = d.rep[k];
-        if ((R.flags & F_PME) && e >= R.mesh_fix_off && e < R.mesh_fix_off + R.mesh_fix_n) {
+        if ((R.flags & F_PME) && e0 >= R.mesh_fix_off && e0 < R.mesh_fix_off + R.mesh_fix_n) {
             r = k;
             break;
         }
@@ -332,19 +335,41 @@ __global__ void k_pme_convert(Dev d, long long n_fix) {
     if (r < 0) return;
     const Rep& R = d.rep[r];
     if (!d.st[r].eval) return;
-    const int loc = static_cast<int>(e - R.mesh_fix_off);  // meshes are < 2^31 points
-    const int K = R.pme_K;
-    const long long v = d.mesh_fix[e];
-    d.mesh_fix[e] = 0;
+    const long long end = R.mesh_fix_off + R.mesh_fix_n;
+    const int loc0 = static_cast<int>(e0 - R.mesh_fix_off);  // meshes are < 2^31 points
     T* real = reinterpret_cast<T*>(d.mesh_real) + R.mesh_real_off;
-    const T val = static_cast<T>(static_cast<double>(v) * (1.0 / MSCALE));
-    if (R.flags & F_PHYS) {
-        real[loc] = val;  // natural layout, same index
-    } else {
-        const int pitch = 2 * (K / 2 + 1);
-        const int row = loc / pitch;
-        const int col = loc - row * pitch;
-        if (col < K) real[static_cast<long long>(row) * K + col] = val;
+    if ((R.flags & F_PHYS) && e0 + 4 <= end) {
+        longlong2* src = reinterpret_cast<longlong2*>(d.mesh_fix + e0);
+        const longlong2 a = src[0], b = src[1];
+        src[0] = make_longlong2(0, 0);
+        src[1] = make_longlong2(0, 0);
+        const T v0 = static_cast<T>(static_cast<double>(a.x) * (1.0 / MSCALE));
+        const T v1 = static_cast<T>(static_cast<double>(a.y) * (1.0 / MSCALE));
+        const T v2 = static_cast<T>(static_cast<double>(b.x) * (1.0 / MSCALE));
+        const T v3 = static_cast<T>(static_cast<double>(b.y) * (1.0 / MSCALE));
+        if (sizeof(T) == 4) {
+            *reinterpret_cast<float4*>(real + loc0) = make_float4(v0, v1, v2, v3);
+        } else {
+            reinterpret_cast<double2*>(real + loc0)[0] = make_double2(v0, v1);
+            reinterpret_cast<double2*>(real + loc0)[1] = make_double2(v2, v3);
+        }
+        return;
+    }
+    const int K = R.pme_K;
+    for (int j = 0; j < 4 && e0 + j < end; ++j) {
+        const long long e = e0 + j;
+        const int loc = loc0 + j;
+        const long long v = d.mesh_fix[e];
+        d.mesh_fix[e] = 0;
+        const T val = static_cast<T>(static_cast<double>(v) * (1.0 / MSCALE));
+        if (R.flags & F_PHYS) {
+            real[loc] = val;  // natural layout, same index
+        } else {
+            const int pitch = 2 * (K / 2 + 1);
+            const int row = loc / pitch;
+            const int col = loc - row * pitch;
+            if (col < K) real[static_cast<long long>(row) * K + col] = val;
+        }
     }
 }
 
@@ -428,14 +453,14 @@ __global__ void k_pme_influence(Dev d) {
 // interpolate_forces (coulomb_pme.cpp:205-283).  REF reads the potential with
 // the unpadded index from FFTW's padded buffer (padding reads as zero) and
 // scales it by 1/N (:303-306); PHYS reads the natural layout, unscaled.
-// 16 threads per atom: thread (iz, iy) = (sub >> 2, sub & 3) sums its row of 4
-// points along x (adjacent addresses), then the atom's 16 lanes reduce in a
-// fixed butterfly order.
+// 4 threads per atom: thread iz sums its (y, x) slice of the 4x4x4 stencil,
+// rows of 4 adjacent x at a time, then the atom's 4 lanes reduce in a fixed
+// order.  The x and y weights are computed once per thread.
 template <typename T>
 __global__ void k_pme_gather(Dev d) {
     const long long t = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
-    const int a = static_cast<int>(t >> 4);
-    // every condition below is uniform over the atom's 16 lanes
+    const int a = static_cast<int>(t >> 2);
+    // every condition below is uniform over the atom's 4 lanes
     if (a >= d.n_atoms) return;
     const int r = d.atom_rep[a];
     RepState* s = d.st + r;
@@ -447,49 +472,62 @@ __global__ void k_pme_gather(Dev d) {
     const bool phys = (R.flags & F_PHYS) != 0;
     const int P = 2 * (K / 2 + 1);
     const double norm = 1.0 / (static_cast<double>(K) * K * K);
-    const int iz = (threadIdx.x >> 2) & 3, iy = threadIdx.x & 3;
+    const int iz = threadIdx.x & 3;
     int m0[3];
     double u[3];
     mesh_coord(d.x[a], s->invL, K, m0[0], u[0]);
     mesh_coord(d.y[a], s->invL, K, m0[1], u[1]);
     mesh_coord(d.z[a], s->invL, K, m0[2], u[2]);
-    T wx[4], dwx[4];
+    T wx[4], dwx[4], wy[4], dwy[4];
+    int xs[4];
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
-        const T tx = (T)(u[0] - (m0[0] + j));
+        const T tx = (T)(u[0] - (m0[0] + j)), ty = (T)(u[1] - (m0[1] + j));
         wx[j] = theta4<T>(tx);
         dwx[j] = dtheta4<T>(tx);
+        wy[j] = theta4<T>(ty);
+        dwy[j] = dtheta4<T>(ty);
+        xs[j] = wrap_mesh(m0[0] + j, K);
     }
-    const T ty = (T)(u[1] - (m0[1] + iy)), tz = (T)(u[2] - (m0[2] + iz));
-    const T wy = theta4<T>(ty), dwy = dtheta4<T>(ty);
+    const T tz = (T)(u[2] - (m0[2] + iz));
     const T wz = theta4<T>(tz), dwz = dtheta4<T>(tz);
     const T* real = reinterpret_cast<const T*>(d.mesh_real) + R.mesh_real_off;
-    const int z = wrap_mesh(m0[2] + iz, K), y = wrap_mesh(m0[1] + iy, K);
-    T sd = 0, sw = 0;  // the row's sums of phi * dtheta_x and phi * theta_x
+    const int z = wrap_mesh(m0[2] + iz, K);
+    T gx = 0, gy = 0, gz = 0;
 #pragma unroll
-    for (int ix = 0; ix < 4; ++ix) {
-        const int x = wrap_mesh(m0[0] + ix, K);
-        const int lin = (z * K + y) * K + x;
-        T phi;
-        if (phys) {
-            phi = real[lin];
-        } else {
-            const int row = lin / P;
-            const int col = lin - row * P;
-            phi = (col < K) ? (T)(static_cast<double>(real[row * K + col]) * norm) : T(0);
+    for (int iy = 0; iy < 4; ++iy) {
+        const int y = wrap_mesh(m0[1] + iy, K);
+        const int row = (z * K + y) * K;
+        T sd = 0, sw = 0;  // the row's sums of phi * dtheta_x and phi * theta_x
+#pragma unroll
+        for (int ix = 0; ix < 4; ++ix) {
+            const int lin = row + xs[ix];
+            T phi;
+            if (phys) {
+                phi = real[lin];
+            } else {
+                const int rr = lin / P;
+                const int col = lin - rr * P;
+                phi = (col < K) ? (T)(static_cast<double>(real[rr * K + col]) * norm) : T(0);
+            }
+            sd += phi * dwx[ix];
+            sw += phi * wx[ix];
         }
-        sd += phi * dwx[ix];
-        sw += phi * wx[ix];
+        gx += sd * wy[iy];
+        gy += sw * dwy[iy];
+        gz += sw * wy[iy];
     }
-    T gx = sd * wy * wz, gy = sw * dwy * wz, gz = sw * wy * dwz;
-    const unsigned grp = 0xFFFFu << (threadIdx.x & 16);
+    gx *= wz;
+    gy *= wz;
+    gz *= dwz;
+    const unsigned grp = 0xFu << (threadIdx.x & 28);
 #pragma unroll
-    for (int o = 8; o > 0; o >>= 1) {
+    for (int o = 2; o > 0; o >>= 1) {
         gx += __shfl_xor_sync(grp, gx, o);
         gy += __shfl_xor_sync(grp, gy, o);
         gz += __shfl_xor_sync(grp, gz, o);
     }
-    if ((threadIdx.x & 15) == 0) {
+    if (iz == 0) {
         const T fac = (T)(static_cast<double>(K) * s->invL);
         const T qt = (T)q;
         add_force(d, a, -qt * fac * gx, -qt * fac * gy, -qt * fac * gz, s);
@@ -541,7 +579,7 @@ void launch_pme_spread(const Dev& d, bool fp64, cudaStream_t st, long long* nlau
 void launch_pme_convert(const Dev& d, bool fp64, long long n_fix_total, cudaStream_t st,
                         long long* nlaunch) {
     const int T = 256;
-    const unsigned g = static_cast<unsigned>((n_fix_total + T - 1) / T);
+    const unsigned g = static_cast<unsigned>(((n_fix_total + 3) / 4 + T - 1) / T);
     if (fp64) k_pme_convert<double><<<g, T, 0, st>>>(d, n_fix_total);
     else k_pme_convert<float><<<g, T, 0, st>>>(d, n_fix_total);
     ++*nlaunch;
@@ -554,7 +592,7 @@ void launch_pme_influence(const Dev& d, bool fp64, int n_blocks, cudaStream_t st
 }
 
 void launch_pme_gather(const Dev& d, bool fp64, cudaStream_t st, long long* nlaunch) {
-    const int T = 256, g = static_cast<int>((16LL * d.n_atoms + T - 1) / T);
+    const int T = 256, g = static_cast<int>((4LL * d.n_atoms + T - 1) / T);
     if (fp64) k_pme_gather<double><<<g, T, 0, st>>>(d);
     else k_pme_gather<float><<<g, T, 0, st>>>(d);
     ++*nlaunch;
