@@ -486,7 +486,7 @@ int Batch::pack() {
     // offsets
     long long n_atoms = 0, n_tiles = 0, n_bins = 0, n_chunks = 0, n_lj = 0, n_bond = 0, n_ang = 0,
               n_dih = 0, n_imp = 0, n_excl = 0, mesh_fix = 0, mesh_real = 0, mesh_cplx = 0, n_bsp = 0;
-    int pme_blocks = 0;
+    int pme_blocks = 0, conv_blocks = 0;
     any_pme_ = any_baro_ = any_ref_lj_ = any_andersen_ref_ = any_andersen_phys_ = false;
     for (int k = 0; k < R; ++k) {
         HostRep& h = *reps_[order_[k]];
@@ -536,6 +536,9 @@ int Batch::pack() {
             P.pme_block_begin = pme_blocks;
             P.pme_blocks = static_cast<int>((static_cast<long long>(K) * K * (K / 2 + 1) + 255) / 256);
             pme_blocks += P.pme_blocks;
+            P.conv_block_begin = conv_blocks;
+            P.conv_blocks = static_cast<int>((P.mesh_fix_n + 1023) / 1024);
+            conv_blocks += P.conv_blocks;
             any_pme_ = true;
         }
         if (s.barostat) any_baro_ = true;
@@ -543,8 +546,8 @@ int Batch::pack() {
         if (s.thermostat == 3 && !phys_) any_andersen_ref_ = true;
         if (s.thermostat == 3 && phys_) any_andersen_phys_ = true;
     }
-    n_fix_total_ = mesh_fix;
     n_pme_blocks_ = pme_blocks;
+    n_conv_blocks_ = conv_blocks;
     try {
         arena_ = std::make_unique<DeviceArena>();
         DeviceArena& A = *arena_;
@@ -635,6 +638,7 @@ int Batch::pack() {
         std::vector<std::vector<int>> exl(n_atoms);
         std::vector<double> bsp(std::max<long long>(n_bsp, 1));
         std::vector<int> pbr(std::max(pme_blocks, 1));
+        std::vector<int> cbr(std::max(conv_blocks, 1));
         std::vector<Rep> hrep(R);
         for (int k = 0; k < R; ++k) {
             HostRep& h = *reps_[order_[k]];
@@ -723,6 +727,7 @@ int Batch::pack() {
                     bsp[P.bsp_off + kk] = b;
                 }
                 for (int b = 0; b < P.pme_blocks; ++b) pbr[P.pme_block_begin + b] = k;
+                for (int b = 0; b < P.conv_blocks; ++b) cbr[P.conv_block_begin + b] = k;
             }
             hrep[k] = P;
         }
@@ -817,6 +822,9 @@ int Batch::pack() {
             int* dpbr = A.alloc<int>(pbr.size());
             up(dpbr, pbr.data(), 4 * pbr.size());
             d.pme_block_rep = dpbr;
+            int* dcbr = A.alloc<int>(cbr.size());
+            up(dcbr, cbr.data(), 4 * cbr.size());
+            d.conv_block_rep = dcbr;
         }
         if (any_andersen_ref_) {
             d_and_flag_ = A.alloc<int>(n_atoms);
@@ -903,7 +911,7 @@ void Batch::enqueue_eval(int pass) {
             record(e0, aux_stream_);
         }
         launch_pme_spread(d, fp64_, aux_stream_, &launches_);
-        launch_pme_convert(d, fp64_, n_fix_total_, aux_stream_, &launches_);
+        launch_pme_convert(d, fp64_, n_conv_blocks_, aux_stream_, &launches_);
         for (int k : order_) {
             const Rep& P = reps_[k]->rep;
             if (!(P.flags & F_PME)) continue;

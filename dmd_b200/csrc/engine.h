@@ -137,8 +137,7 @@ class Batch {
     bool st_fresh_ = false;                         // h_st_ equals the device table (no work since)
     long long* h_tgt_ = nullptr;                    // pinned step targets for extend_targets
     int* d_bin_rep_ = nullptr;
-    long long n_fix_total_ = 0;
-    int n_pme_blocks_ = 0;
+    int n_pme_blocks_ = 0, n_conv_blocks_ = 0;
     bool any_pme_ = false, any_baro_ = false, any_ref_lj_ = false, any_andersen_ref_ = false,
          any_andersen_phys_ = false;
     std::map<int, std::pair<cufftHandle, cufftHandle>> plans_;

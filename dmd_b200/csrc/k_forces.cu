@@ -315,31 +315,21 @@ __global__ void k_pme_spread(Dev d) {
 // Fixed-point mesh -> real FFT input (K^3, natural layout); clears the fixed mesh.
 // REF: the FFT reads FFTW's padded in-place rows, i.e. element (z,y,x) of the real
 // array is fixed[(z*K + y)*P + x] with P = 2(K/2+1).
-// Four consecutive elements per thread (replica meshes start on 64-element
-// boundaries, so a group never straddles two replicas): 16-byte loads and
-// stores where the group lies inside one PHYS mesh.
+// Each block converts 1,024 points of one replica's mesh (the block -> replica
+// table is built at packing), four consecutive points per thread: 16-byte loads
+// and stores where the group lies inside a PHYS mesh.  Replicas that do not
+// evaluate this pass hold a zero mesh, so converting it is harmless and no
+// per-replica test delays the loads.
 template <typename T>
-__global__ void k_pme_convert(Dev d, long long n_fix) {
-    const long long e0 = 4 * (static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x);
-    if (e0 >= n_fix) return;
-    // replica of the group: linear scan over the (few) PME replicas; groups in
-    // the alignment gaps between replica meshes belong to none
-    int r = -1;
-    for (int k = 0; k < d.n_rep; ++k) {
-        const Rep& R = d.rep[k];
-        if ((R.flags & F_PME) && e0 >= R.mesh_fix_off && e0 < R.mesh_fix_off + R.mesh_fix_n) {
-            r = k;
-            break;
-        }
-    }
-    if (r < 0) return;
+__global__ void k_pme_convert(Dev d) {
+    const int r = d.conv_block_rep[blockIdx.x];
     const Rep& R = d.rep[r];
-    if (!d.st[r].eval) return;
-    const long long end = R.mesh_fix_off + R.mesh_fix_n;
-    const int loc0 = static_cast<int>(e0 - R.mesh_fix_off);  // meshes are < 2^31 points
+    const int loc0 = 1024 * (blockIdx.x - R.conv_block_begin) + 4 * threadIdx.x;
+    if (loc0 >= R.mesh_fix_n) return;
+    long long* fix = d.mesh_fix + R.mesh_fix_off;
     T* real = reinterpret_cast<T*>(d.mesh_real) + R.mesh_real_off;
-    if ((R.flags & F_PHYS) && e0 + 4 <= end) {
-        longlong2* src = reinterpret_cast<longlong2*>(d.mesh_fix + e0);
+    if ((R.flags & F_PHYS) && loc0 + 4 <= R.mesh_fix_n) {
+        longlong2* src = reinterpret_cast<longlong2*>(fix + loc0);
         const longlong2 a = src[0], b = src[1];
         src[0] = make_longlong2(0, 0);
         src[1] = make_longlong2(0, 0);
@@ -356,11 +346,10 @@ __global__ void k_pme_convert(Dev d, long long n_fix) {
         return;
     }
     const int K = R.pme_K;
-    for (int j = 0; j < 4 && e0 + j < end; ++j) {
-        const long long e = e0 + j;
-        const int loc = loc0 + j;
-        const long long v = d.mesh_fix[e];
-        d.mesh_fix[e] = 0;
+    for (int j = 0; j < 4 && loc0 + j < R.mesh_fix_n; ++j) {
+        const int loc = loc0 + j;  // meshes are < 2^31 points
+        const long long v = fix[loc];
+        fix[loc] = 0;
         const T val = static_cast<T>(static_cast<double>(v) * (1.0 / MSCALE));
         if (R.flags & F_PHYS) {
             real[loc] = val;  // natural layout, same index
@@ -576,12 +565,10 @@ void launch_pme_spread(const Dev& d, bool fp64, cudaStream_t st, long long* nlau
     ++*nlaunch;
 }
 
-void launch_pme_convert(const Dev& d, bool fp64, long long n_fix_total, cudaStream_t st,
-                        long long* nlaunch) {
-    const int T = 256;
-    const unsigned g = static_cast<unsigned>(((n_fix_total + 3) / 4 + T - 1) / T);
-    if (fp64) k_pme_convert<double><<<g, T, 0, st>>>(d, n_fix_total);
-    else k_pme_convert<float><<<g, T, 0, st>>>(d, n_fix_total);
+void launch_pme_convert(const Dev& d, bool fp64, int n_blocks, cudaStream_t st, long long* nlaunch) {
+    if (n_blocks <= 0) return;
+    if (fp64) k_pme_convert<double><<<n_blocks, 256, 0, st>>>(d);
+    else k_pme_convert<float><<<n_blocks, 256, 0, st>>>(d);
     ++*nlaunch;
 }
 

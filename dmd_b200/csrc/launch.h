@@ -23,8 +23,7 @@ void launch_nonbonded(const Dev& d, bool fp64, bool phys, int n_sm, int blocks_p
 // bonds, angles, dihedrals and the exclusion correction in one launch
 void launch_bonded(const Dev& d, bool fp64, bool phys, cudaStream_t st, long long* nlaunch);
 void launch_pme_spread(const Dev& d, bool fp64, cudaStream_t st, long long* nlaunch);
-void launch_pme_convert(const Dev& d, bool fp64, long long n_fix_total, cudaStream_t st,
-                        long long* nlaunch);
+void launch_pme_convert(const Dev& d, bool fp64, int n_blocks, cudaStream_t st, long long* nlaunch);
 void launch_pme_influence(const Dev& d, bool fp64, int n_blocks, cudaStream_t st,
                           long long* nlaunch);
 void launch_pme_gather(const Dev& d, bool fp64, cudaStream_t st, long long* nlaunch);

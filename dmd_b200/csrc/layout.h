@@ -57,6 +57,7 @@ struct Rep {
     long long mesh_cplx_off;             // K*K*(K/2+1) complex
     int bsp_off;                         // K doubles: B-spline factor per mesh index
     int pme_block_begin, pme_blocks;     // influence-kernel blocks
+    int conv_block_begin, conv_blocks;   // convert-kernel blocks (1,024 mesh points each)
     double rc_lj, rc_c, rc_list;
     double rc_lj2, rc_c2, rc_list2, half_skin2;
     double alpha;
@@ -164,6 +165,7 @@ struct Dev {
     const double* bsp;
     double* pme_part;                  // per influence block: energy, virial
     const int* pme_block_rep;
+    const int* conv_block_rep;         // replica of each convert-kernel block
     // Andersen (REF): host-generated overrides
     const int* and_flag;
     const double* and_v;
