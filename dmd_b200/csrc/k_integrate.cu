@@ -54,7 +54,9 @@ __global__ void k_eval_begin(Dev d, int pass) {
         if (s->active && !ev && ref_lj) s->lj_counter += 1;
     } else if (pass == PASS_SECOND) {
         ev = s->active;
-        s->vscale = 1.0;  // consumed by k_kick_drift
+        // consumed by k_kick_drift; a replica that has reached its target keeps
+        // its pending thermostat scale for the next read of its velocities
+        if (s->active) s->vscale = 1.0;
         if (s->active && (R.flags & F_PHYS) && s->pscale != 1.0) {
             // the box follows the positions k_kick_drift has just scaled
             s->L *= s->pscale;

@@ -129,8 +129,8 @@ def serve(jobs, budget_bytes=150 * 10**9, precision="mixed", profile="phys", chu
             j = running.pop(slot)
             j.done = now()
             s = b.scalars(slot)
-            j.result = {"positions": b.positions(slot), "potential_energy": s.potential_energy,
-                        "step": int(s.step)}
+            j.result = {"positions": b.positions(slot), "velocities": b.velocities(slot),
+                        "potential_energy": s.potential_energy, "step": int(s.step)}
             b.release(slot)
             dirty = True
     wall = time.perf_counter() - t0

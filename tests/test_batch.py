@@ -71,18 +71,22 @@ def test_serving_admit_and_release_midway():
     s_b = b.admit(b_cfg, 20)          # repack while A is mid-run (A at step 10)
     b.step(15)                        # A done at 25, B at 15
     assert b.poll() == [a]
-    pa, pe_a = b.positions(a), b.scalars(a).potential_energy
+    pa, va, pe_a = b.positions(a), b.velocities(a), b.scalars(a).potential_energy
     b.release(a)
     s_c = b.admit(c_cfg, 12)          # C takes the freed slot id and memory (B at step 15)
     assert s_c == a
     b.step(12)                        # B done at 20 (stops there), C at 12
     assert sorted(b.poll()) == sorted([s_b, s_c])
-    for cfg, n, reps, got, pe in ((a_cfg, 25, [10], pa, pe_a),
-                                  (b_cfg, 20, [15], b.positions(s_b), b.scalars(s_b).potential_energy),
-                                  (c_cfg, 12, [], b.positions(s_c), b.scalars(s_c).potential_energy)):
-        p, _, pe_alone = _alone(cfg, n, "mixed", reps)
+    # B (Nose-Hoover water) reaches its target while C keeps stepping: its last
+    # pending thermostat scale must survive the steps it sits out
+    for cfg, n, reps, got, vel, pe in (
+            (a_cfg, 25, [10], pa, va, pe_a),
+            (b_cfg, 20, [15], b.positions(s_b), b.velocities(s_b), b.scalars(s_b).potential_energy),
+            (c_cfg, 12, [], b.positions(s_c), b.velocities(s_c), b.scalars(s_c).potential_energy)):
+        p, v, pe_alone = _alone(cfg, n, "mixed", reps)
         assert got.shape == p.shape
         assert np.array_equal(got, p), (n, np.abs(got - p).max())
+        assert np.array_equal(vel, v), (n, np.abs(vel - v).max())
         assert pe == pe_alone
     assert b.active == 0
 
@@ -110,6 +114,7 @@ def test_serve_stream_results_equal_alone():
     assert any(j.repacks for j in jobs)       # the mix did overlap
     for j in jobs:
         assert j.result["step"] == j.n_steps
-        p, _, pe = run_alone(j, "mixed", "phys")
+        p, v, pe = run_alone(j, "mixed", "phys")
         assert np.array_equal(j.result["positions"], p), (j.jid, np.abs(j.result["positions"] - p).max())
+        assert np.array_equal(j.result["velocities"], v), (j.jid, np.abs(j.result["velocities"] - v).max())
         assert j.result["potential_energy"] == pe, j.jid
