@@ -301,9 +301,9 @@ class Engine:
 
     def repack(self):
         """Rebuild the device table with the state carried over bit for bit (pair
-        list rebuilt, forces evaluated again at the current positions): what a
-        running slot of a Batch goes through when another slot is admitted or
-        released."""
+        list rebuilt in the frame of its last build, forces evaluated again at
+        the current positions): what a running slot of a Batch goes through when
+        another slot is admitted or released.  The trajectory is unchanged."""
         self._check(self._lib.dmdgpu_repack(self._h))
 
     def step_timed(self, steps: int, l2_flush_bytes: int = 0) -> dict:

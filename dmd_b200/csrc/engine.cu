@@ -225,6 +225,7 @@ int Batch::build_host(HostRep& hr, unsigned mask) {
     st.pscale = 1.0;
     st.rebuild = 1;
     st.lj_counter = 10;  // LennardJones::step_since_rebuild_ initial value (lennard_jones.cpp:10)
+    st.L_build = s.box;
     return DMDGPU_OK;
 }
 
@@ -429,7 +430,8 @@ int Batch::release(int slot) {
 
 // What a running replica goes through when another slot is admitted or released:
 // the table is rebuilt with its state carried over bit for bit, its pair list is
-// rebuilt and its forces are evaluated again at the same positions.
+// rebuilt in the frame of its last build and its forces are evaluated again at
+// the same positions; the trajectory continues unchanged.
 int Batch::repack() {
     CK(cudaSetDevice(device_));
     packed_ = false;
@@ -466,9 +468,17 @@ int Batch::pack() {
             CK(cudaMemcpy(s.vx.data(), dev_.vx + a0, n * 8, cudaMemcpyDeviceToHost));
             CK(cudaMemcpy(s.vy.data(), dev_.vy + a0, n * 8, cudaMemcpyDeviceToHost));
             CK(cudaMemcpy(s.vz.data(), dev_.vz + a0, n * 8, cudaMemcpyDeviceToHost));
+            // the positions of the last list build: the list is rebuilt in that
+            // frame (rebuild_in_frame), so the carried replica continues exactly
+            // as it would have in the old table
+            s.xr.resize(n);
+            s.yr.resize(n);
+            s.zr.resize(n);
+            CK(cudaMemcpy(s.xr.data(), dev_.xr + a0, n * 8, cudaMemcpyDeviceToHost));
+            CK(cudaMemcpy(s.yr.data(), dev_.yr + a0, n * 8, cudaMemcpyDeviceToHost));
+            CK(cudaMemcpy(s.zr.data(), dev_.zr + a0, n * 8, cudaMemcpyDeviceToHost));
             RepState st = h_st_[k];
-            st.rebuild = 1;          // slots change: rebuild every list
-            st.have_forces = 0;      // forces are recomputed at the same positions
+            st.have_forces = 0;      // forces are evaluated again at the same positions
             st.n_chunks = 0;
             st.green_L = 0.0;        // the new arena holds no PME influence function yet
             o.init = st;
@@ -621,7 +631,7 @@ int Batch::pack() {
         d.grid_bar = A.alloc<unsigned>(2);
         // host-side staging
         std::vector<double> hm(n_atoms), hq(n_atoms), hx(n_atoms), hy(n_atoms), hz(n_atoms), hvx(n_atoms),
-            hvy(n_atoms), hvz(n_atoms);
+            hvy(n_atoms), hvz(n_atoms), hxr(n_atoms), hyr(n_atoms), hzr(n_atoms);
         std::vector<int> ht(n_atoms), har(n_atoms), htr(n_tiles), hvr(n_bins), hbr(n_bins);
         std::vector<double2> lj64(n_lj);
         std::vector<float4> lj32(n_lj);
@@ -651,6 +661,10 @@ int Batch::pack() {
                 hx[a0 + i] = s.x[i];
                 hy[a0 + i] = s.y[i];
                 hz[a0 + i] = s.z[i];
+                const bool framed = !s.xr.empty();
+                hxr[a0 + i] = framed ? s.xr[i] : s.x[i];
+                hyr[a0 + i] = framed ? s.yr[i] : s.y[i];
+                hzr[a0 + i] = framed ? s.zr[i] : s.z[i];
                 hvx[a0 + i] = s.vx[i];
                 hvy[a0 + i] = s.vy[i];
                 hvz[a0 + i] = s.vz[i];
@@ -749,6 +763,9 @@ int Batch::pack() {
         up(d.vx, hvx.data(), 8 * n_atoms);
         up(d.vy, hvy.data(), 8 * n_atoms);
         up(d.vz, hvz.data(), 8 * n_atoms);
+        up(d.xr, hxr.data(), 8 * n_atoms);
+        up(d.yr, hyr.data(), 8 * n_atoms);
+        up(d.zr, hzr.data(), 8 * n_atoms);
         up(mass, hm.data(), 8 * n_atoms);
         up(q, hq.data(), 8 * n_atoms);
         up(type, ht.data(), 4 * n_atoms);
@@ -865,6 +882,13 @@ int Batch::pack() {
         plans_[K] = {f, b};
     }
     for (int k : order_) reps_[k]->on_device = true;
+    {
+        // every replica's list, built in the frame of its last build (a new
+        // replica: its current positions and box)
+        std::vector<char> all(R, 1);
+        int rc = rebuild_in_frame(all);
+        if (rc) return rc;
+    }
     {
         std::lock_guard<std::mutex> lk(g_tune_mu);
         auto it = g_tune.find(tune_key(device_, fp64_, any_pme_, dev_.n_atoms));
@@ -1102,6 +1126,59 @@ int Batch::autotune(int max_steps, int* used) {
     tuned_ = true;
     std::lock_guard<std::mutex> lk(g_tune_mu);
     g_tune[tune_key(device_, fp64_, any_pme_, dev_.n_atoms)] = best;
+    return DMDGPU_OK;
+}
+
+// Pair lists of the selected replicas (packed indices) rebuilt in the frame of
+// their last build: positions xr/yr/zr (already on the device) and box L_build.
+// The slot order, tile centres, frozen images and chunk lists then equal the
+// ones the replica had, so a table rebuild or a checkpoint restart continues
+// bit for bit.  Afterwards the current box and counters are restored, forces
+// are marked for evaluation and the mirror is rewritten from the positions.
+int Batch::rebuild_in_frame(const std::vector<char>& sel) {
+    const int R = static_cast<int>(order_.size());
+    if (R == 0) return DMDGPU_OK;
+    std::vector<RepState> cur(R), tmp(R);
+    CK(cudaStreamSynchronize(stream_));
+    CK(cudaMemcpy(cur.data(), d_st_, sizeof(RepState) * R, cudaMemcpyDeviceToHost));
+    tmp = cur;
+    for (int k = 0; k < R; ++k) {
+        tmp[k].rebuild = sel[k] ? 1 : 0;
+        if (sel[k]) {
+            tmp[k].L = cur[k].L_build;
+            tmp[k].invL = 1.0 / cur[k].L_build;
+        }
+    }
+    CK(cudaMemcpy(d_st_, tmp.data(), sizeof(RepState) * R, cudaMemcpyHostToDevice));
+    Dev frame = dev_;
+    frame.x = dev_.xr;
+    frame.y = dev_.yr;
+    frame.z = dev_.zr;
+    launch_rebuild(frame, d_bin_rep_, n_sm_, stream_, &launches_);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(stream_));
+    CK(cudaMemcpy(tmp.data(), d_st_, sizeof(RepState) * R, cudaMemcpyDeviceToHost));
+    for (int k = 0; k < R; ++k) {
+        if (!sel[k]) {
+            tmp[k] = cur[k];
+            continue;
+        }
+        RepState& f = tmp[k];
+        f.L = cur[k].L;
+        f.invL = cur[k].invL;
+        f.L_build = cur[k].L_build;
+        f.lj_counter = cur[k].lj_counter;
+        // a replica that had built before keeps a pending rebuild request; a new
+        // one has just been built at its current positions
+        f.rebuild = cur[k].list_builds > 0 ? cur[k].rebuild : 0;
+        f.list_builds = std::max(cur[k].list_builds, 1LL);
+        f.have_forces = 0;
+    }
+    CK(cudaMemcpy(d_st_, tmp.data(), sizeof(RepState) * R, cudaMemcpyHostToDevice));
+    launch_write_mirror(dev_, fp64_, stream_, &launches_);
+    CK(cudaGetLastError());
+    st_fresh_ = false;
+    graph_dirty_ = true;
     return DMDGPU_OK;
 }
 
@@ -1531,9 +1608,11 @@ int Batch::save_checkpoint(int slot, const char* path) {
     os.write(reinterpret_cast<const char*>(h.sys.type.data()), 4 * n);
     int32_t ljc = sc.lj_step_since_rebuild;
     os.write(reinterpret_cast<const char*>(&ljc), 4);
-    // trailer: box, Nose-Hoover zeta, Andersen call counter, profile and (v3)
-    // the PHYS barostat scale still to be applied with the next drift
-    uint32_t tv = 3;
+    // trailer: box, Nose-Hoover zeta, Andersen call counter, profile, (v3) the
+    // PHYS barostat scale still to be applied with the next drift, (v4) the
+    // frame of the last list build (box edge, build count, positions) and the
+    // pending-rebuild flag, so a restart rebuilds the very same list
+    uint32_t tv = 4;
     double box = sc.box, zeta = sc.zeta;
     int k = replica_index(slot);
     int64_t acalls = h_st_[k].andersen_calls;
@@ -1548,6 +1627,21 @@ int Batch::save_checkpoint(int slot, const char* path) {
     os.write(reinterpret_cast<const char*>(&prof), 4);
     double pscale = phys_ ? h_st_[k].pscale : 1.0;
     os.write(reinterpret_cast<const char*>(&pscale), 8);
+    {
+        const RepState& st = h_st_[k];
+        const double lb = st.L_build;
+        const int64_t nb = st.list_builds;
+        const int32_t pending = st.rebuild;
+        os.write(reinterpret_cast<const char*>(&lb), 8);
+        os.write(reinterpret_cast<const char*>(&nb), 8);
+        os.write(reinterpret_cast<const char*>(&pending), 4);
+        std::vector<double> f(n);
+        const int a0 = h.rep.atom_begin;
+        for (double* src : {dev_.xr, dev_.yr, dev_.zr}) {
+            CK(cudaMemcpy(f.data(), src + a0, 8 * n, cudaMemcpyDeviceToHost));
+            os.write(reinterpret_cast<const char*>(f.data()), 8 * n);
+        }
+    }
     return os.good() ? DMDGPU_OK : fail(DMDGPU_ERR_PARM, "checkpoint write failed");
 }
 
@@ -1601,6 +1695,22 @@ int Batch::load_checkpoint(int slot, const char* path) {
         trailer = static_cast<bool>(is);
         if (trailer && tv >= 3 && !is.read(reinterpret_cast<char*>(&pscale), 8)) pscale = 1.0;
     }
+    // v4: the frame of the last list build
+    bool framed = false;
+    double lbuild = 0.0;
+    int64_t nbuilds = 0;
+    int32_t pending = 0;
+    std::vector<double> fr[3];
+    if (trailer && tv >= 4) {
+        is.read(reinterpret_cast<char*>(&lbuild), 8);
+        is.read(reinterpret_cast<char*>(&nbuilds), 8);
+        is.read(reinterpret_cast<char*>(&pending), 4);
+        for (auto& f : fr) {
+            f.resize(n);
+            is.read(reinterpret_cast<char*>(f.data()), 8 * n);
+        }
+        framed = static_cast<bool>(is) && lbuild > 0.0;
+    }
     const int k = replica_index(slot);
     const int a0 = h.rep.atom_begin;
     CK(cudaStreamSynchronize(stream_));
@@ -1627,7 +1737,21 @@ int Batch::load_checkpoint(int slot, const char* path) {
         h.andersen_seed = aseed;
         st.pscale = phys_ ? pscale : 1.0;
     }
+    if (framed) {
+        // the saved list frame: the list is rebuilt as it was, not at the loaded positions
+        st.L_build = lbuild;
+        st.list_builds = nbuilds;
+        st.rebuild = pending;
+        double* fdst[3] = {dev_.xr, dev_.yr, dev_.zr};
+        for (int i = 0; i < 3; ++i) CK(cudaMemcpy(fdst[i] + a0, fr[i].data(), 8 * n, cudaMemcpyHostToDevice));
+    }
     CK(cudaMemcpy(d_st_ + k, &st, sizeof(RepState), cudaMemcpyHostToDevice));
+    if (framed) {
+        std::vector<char> sel(order_.size(), 0);
+        sel[k] = 1;
+        int rc = rebuild_in_frame(sel);
+        if (rc) return rc;
+    }
     h.target = st.step;
     h.done = false;
     graph_dirty_ = true;  // the next step must evaluate forces first

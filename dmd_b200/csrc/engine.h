@@ -34,6 +34,7 @@ struct HostSystem {
     std::vector<double> akt, at0;
     std::vector<int> di, dj, dk, dl, dn;
     std::vector<double> dkp, dp0;
+    std::vector<double> xr, yr, zr;   // positions of the last list build (empty: never built)
     std::vector<int> ii, ij, ik, il;
     std::vector<double> ikp, ip0;
     std::vector<int> ei, ej;
@@ -111,6 +112,7 @@ class Batch {
     void enqueue_step();
     int run_steps(int n);
     int autotune(int max_steps, int* used);
+    int rebuild_in_frame(const std::vector<char>& sel);
     int sync_status();
     int replica_index(int slot) const;
     void free_device();

@@ -617,6 +617,7 @@ __device__ __forceinline__ void rebuild_finish(const Dev& d) {
             s->rebuild = 0;
             s->lj_counter = 0;
             s->list_builds += 1;
+            s->L_build = s->L;
         }
         d.chunk_prefix[r] = run;
         run += s->n_chunks;

@@ -99,6 +99,7 @@ struct RepState {
     int want_e;           // the current evaluation's pair energies / virial are read
     int green_ok;         // the cached PME influence function matches the box
     double green_L;       // box edge the cached influence function was made for
+    double L_build;       // box edge at the last list build (with xr/yr/zr: the list's frame)
 };
 
 // Kernel view of the whole batch (passed by value).

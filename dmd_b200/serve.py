@@ -150,19 +150,13 @@ def serve(jobs, budget_bytes=150 * 10**9, precision="mixed", profile="phys", chu
 
 
 def run_alone(job: Job, precision="mixed", profile="phys", device=None):
-    """The same job in an engine of its own, with its table rebuilt at the same
-    steps as in the stream (Engine.repack): positions, velocities, potential
-    energy.  Fixed-point force sums and per-replica reductions make this equal
-    to the job's result in the mix, bit for bit."""
+    """The same job in an engine of its own: positions, velocities, potential
+    energy.  Fixed-point force sums, per-replica reductions and pair lists
+    rebuilt in their own frame at table rebuilds make this equal to the job's
+    result in the mix, bit for bit."""
     from .core import Engine
     e = Engine(job.cfg, precision=precision, profile=profile, device=device)
-    done = 0
-    for at in job.repacks:
-        if at > done:
-            e.run_n(at - done)
-            done = at
-        e.repack()
-    e.run_n(job.n_steps - done)
+    e.run_n(job.n_steps)
     out = e.positions, e.velocities, e.potential_energy
     e.close()
     return out

@@ -178,8 +178,12 @@ int dmdgpu_component_compute(dmdgpu_ctx *ctx, int32_t component, const double *p
 int dmdgpu_pair_list(dmdgpu_ctx *ctx, int32_t *pi, int32_t *pj, int64_t cap, int64_t *count);
 
 /* Binary checkpoint v1 (src/sim/checkpoint.cpp:9-75) plus a trailer the v1
- * reader ignores (box, Nose-Hoover zeta, thermostat call counter, profile).
- * Replaces SimulationEngine::save_checkpoint / load_checkpoint (:108-137). */
+ * reader ignores (box, Nose-Hoover zeta, thermostat call counter, profile, the
+ * pending PHYS barostat scale, and the frame of the last pair-list build: its
+ * box edge and positions).  A restart rebuilds the list in that frame, so N
+ * steps equal N/2 + save/load + N/2 bit for bit in both profiles and both
+ * precisions.  Replaces SimulationEngine::save_checkpoint / load_checkpoint
+ * (:108-137). */
 int dmdgpu_save_checkpoint(dmdgpu_ctx *ctx, const char *path);
 int dmdgpu_load_checkpoint(dmdgpu_ctx *ctx, const char *path);
 
@@ -187,11 +191,11 @@ int dmdgpu_load_checkpoint(dmdgpu_ctx *ctx, const char *path);
 int64_t dmdgpu_footprint_bytes(const dmdgpu_system *sys, const dmdgpu_options *opt);
 
 /* Rebuild this context's device table with its state carried over bit for bit:
- * the pair list is rebuilt and forces are evaluated again at the current
- * positions before the next step.  This is what a running slot of a batch goes
- * through when another slot is admitted or released, so a system run alone with
- * dmdgpu_repack at the same steps reproduces its batched trajectory exactly.
- * No counterpart in the reference. */
+ * the pair list is rebuilt in the frame of its last build and forces are
+ * evaluated again at the current positions before the next step.  This is what
+ * a running slot of a batch goes through when another slot is admitted or
+ * released; the trajectory continues bit for bit, so a batched job equals the
+ * same job run alone.  No counterpart in the reference. */
 int dmdgpu_repack(dmdgpu_ctx *ctx);
 
 /* Kernel launches issued by this context so far (this library's own kernels). */

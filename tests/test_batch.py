@@ -4,10 +4,10 @@ A slot's result must be the same alone and in the mix.  The batch shares kernel
 launches, not arithmetic (fixed-point force sums, per-replica reductions in a
 fixed order), so results are compared bit for bit.  Admitting or releasing a
 job rebuilds the device table: every running replica carries its state over,
-rebuilds its pair list and evaluates its forces again at the same positions.
-In the mixed path the rebuilt list's FP32 tile frame rounds differently from
-the frame it replaces, so the reference run alone goes through the same
-rebuilds at the same steps (Engine.repack) -- and is then identical bit for bit.
+its pair list is rebuilt in the frame of its last build (same slots, tile
+centres and chunks) and its forces are evaluated again at the same positions,
+so a job is bit for bit the same as the same job run alone without any
+rebuilds.
 """
 import numpy as np
 import pytest
@@ -30,15 +30,10 @@ def _mix():
     return cfgs
 
 
-def _alone(cfg, steps, precision, repacks=()):
+def _alone(cfg, steps, precision):
     from dmd_b200.core import Engine
     e = Engine(cfg, precision=precision, profile="phys")
-    done = 0
-    for at in repacks:
-        e.run_n(at - done)
-        done = at
-        e.repack()
-    e.run_n(steps - done)
+    e.run_n(steps)
     return e.positions, e.velocities, e.potential_energy
 
 
@@ -61,7 +56,7 @@ def test_batch_matches_alone(precision):
 
 def test_serving_admit_and_release_midway():
     """Continuous batching: B arrives while A runs, C after A is released; every
-    result equals the same job run alone with its table rebuilt at the same steps."""
+    result equals the same job run alone."""
     from dmd_b200.batch import Batch
     cfgs = _mix()
     a_cfg, b_cfg, c_cfg = cfgs[1], cfgs[5], cfgs[3]
@@ -79,11 +74,11 @@ def test_serving_admit_and_release_midway():
     assert sorted(b.poll()) == sorted([s_b, s_c])
     # B (Nose-Hoover water) reaches its target while C keeps stepping: its last
     # pending thermostat scale must survive the steps it sits out
-    for cfg, n, reps, got, vel, pe in (
-            (a_cfg, 25, [10], pa, va, pe_a),
-            (b_cfg, 20, [15], b.positions(s_b), b.velocities(s_b), b.scalars(s_b).potential_energy),
-            (c_cfg, 12, [], b.positions(s_c), b.velocities(s_c), b.scalars(s_c).potential_energy)):
-        p, v, pe_alone = _alone(cfg, n, "mixed", reps)
+    for cfg, n, got, vel, pe in (
+            (a_cfg, 25, pa, va, pe_a),
+            (b_cfg, 20, b.positions(s_b), b.velocities(s_b), b.scalars(s_b).potential_energy),
+            (c_cfg, 12, b.positions(s_c), b.velocities(s_c), b.scalars(s_c).potential_energy)):
+        p, v, pe_alone = _alone(cfg, n, "mixed")
         assert got.shape == p.shape
         assert np.array_equal(got, p), (n, np.abs(got - p).max())
         assert np.array_equal(vel, v), (n, np.abs(vel - v).max())
@@ -104,8 +99,8 @@ def test_budget_admission():
 
 def test_serve_stream_results_equal_alone():
     """The request loop: jobs arriving over time (virtual clock in steps) are
-    admitted while others run; each result equals the same job run alone (with
-    its table rebuilt at the same steps), bit for bit."""
+    admitted while others run; each result equals the same job run alone, bit
+    for bit."""
     from dmd_b200.serve import job_mix, run_alone, serve
     jobs = job_mix(6, rate=0.05, seed=7, scale=0.02)
     out = serve(jobs, precision="mixed", profile="phys", chunk=10, virtual=True)

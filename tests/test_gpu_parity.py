@@ -183,26 +183,45 @@ def test_checkpoint_restart_bitwise(tmp_path):
     assert np.array_equal(full.velocities, fresh.velocities)
 
 
-def test_checkpoint_restart_bitwise_phys_npt(tmp_path):
-    """PHYS NPT: the barostat scale chosen at the end of the saved step is applied
-    with the next drift, so it travels in the checkpoint trailer; without it the
-    restarted run would drift from the continuous one by the scale (1e-6)."""
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_checkpoint_restart_bitwise_phys_npt(tmp_path, precision):
+    """PHYS NPT: N steps == N/2 + save/load + N/2, bit for bit.  The trailer
+    carries the barostat scale chosen at the end of the saved step (applied with
+    the next drift) and the frame of the last list build, which the restart
+    rebuilds the list in, so the mixed path's FP32 tile frame is the same too."""
     cfg = _water(300, seed=3)
     cfg.thermostat.type = "berendsen"
     cfg.barostat.type = "berendsen"
     cfg.barostat.tau = 0.5
-    full = _engine(cfg, "fp64", "phys")
+    full = _engine(cfg, precision, "phys")
     full.run_n(30)
-    half = _engine(cfg, "fp64", "phys")
+    half = _engine(cfg, precision, "phys")
     half.run_n(15)
     p = str(tmp_path / "ck_npt.bin")
     half.save_checkpoint(p)
-    fresh = _engine(cfg, "fp64", "phys")
+    fresh = _engine(cfg, precision, "phys")
     fresh.load_checkpoint(p)
     fresh.run_n(15)
     assert fresh.current_step == 30
-    # the restart rebuilds the pair list at the saved positions, which regroups
-    # the FP64 per-chunk partial sums: equal to round-off, not bit for bit
-    assert abs(fresh.box_size - full.box_size) <= 1e-12 * full.box_size
-    assert np.abs(full.positions - fresh.positions).max() < 1e-9
-    assert rel_rms(fresh.velocities, full.velocities) < 1e-8
+    assert fresh.box_size == full.box_size
+    assert np.array_equal(full.positions, fresh.positions)
+    assert np.array_equal(full.velocities, fresh.velocities)
+    assert fresh.potential_energy == full.potential_energy
+
+
+def test_repack_is_invisible():
+    """A table rebuild (what admission / release does to running replicas)
+    rebuilds each list in the frame of its last build: the trajectory continues
+    bit for bit."""
+    cfg = _water(400, seed=6)
+    a = _engine(cfg, "mixed", "phys")
+    a.run_n(24)
+    b = _engine(cfg, "mixed", "phys")
+    b.run_n(9)
+    b.repack()
+    b.run_n(8)
+    b.repack()
+    b.run_n(7)
+    assert np.array_equal(a.positions, b.positions)
+    assert np.array_equal(a.velocities, b.velocities)
+    assert a.potential_energy == b.potential_energy
