@@ -66,7 +66,8 @@ void sort_grid(int n, double L, int& nvx, int& nvz) {
 // Autotuner cache: the pair kernel's launch shape chosen for a kind of batch,
 // shared by every batch of the process (the serving loop repacks often).
 // Key: device, precision, whether a PME chain runs beside the pair kernel, and
-// the batch's atom count in powers of two.
+// the batch's atom count in powers of four (a served stream's table changes
+// size with every admission; nearby sizes share a shape).
 namespace {
 struct TuneKey {
     int device, fp64, pme, bucket;
@@ -81,7 +82,7 @@ constexpr int kTuneCand[] = {2, 3};         // pair-kernel blocks per SM
 
 TuneKey tune_key(int device, bool fp64, bool pme, long long n_atoms) {
     int b = 0;
-    while ((1LL << (b + 1)) <= n_atoms) ++b;
+    while ((1LL << (2 * b + 2)) <= n_atoms) ++b;
     return TuneKey{device, fp64 ? 1 : 0, pme ? 1 : 0, b};
 }
 }  // namespace
