@@ -682,10 +682,27 @@ __global__ void __launch_bounds__(NT_B, 4) k_rebuild(Dev d, const int* bin_rep) 
     const int gthreads = gridDim.x * NT_B;
     const int gtid = blockIdx.x * NT_B + tid;
     const int gwarp = gtid >> 5, nwarps = gthreads >> 5;
-    // R0: chunk counters of the replicas that rebuild, work counter of R6
+    // R0: chunk counters of the replicas that rebuild, work counter of R6 and
+    // the prefix of the rebuilding replicas' tiles (R6 visits only those)
     if (gtid == 0) *d.build_work = 0;
     for (int r = gtid; r < d.n_rep; r += gthreads)
         if (d.st[r].rebuild) d.st[r].n_chunks = 0;
+    if (blockIdx.x == 0 && tid < 32) {
+        int run = 0;
+        for (int base = 0; base < d.n_rep; base += 32) {
+            const int r = base + lane;
+            const int v = (r < d.n_rep && d.st[r].rebuild) ? d.rep[r].n_tiles : 0;
+            int incl = v;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int t = __shfl_up_sync(FULL, incl, o);
+                if (lane >= o) incl += t;
+            }
+            if (r < d.n_rep) d.build_prefix[r] = run + incl - v;
+            run += __shfl_sync(FULL, incl, 31);
+        }
+        if (lane == 0) d.build_prefix[d.n_rep] = run;
+    }
     for (int a = gtid; a < d.n_atoms; a += gthreads) bin_atom(d, a);
     if (!grid_barrier(d)) return;
     for (int r = blockIdx.x; r < d.n_rep; r += gridDim.x)
@@ -697,15 +714,18 @@ __global__ void __launch_bounds__(NT_B, 4) k_rebuild(Dev d, const int* bin_rep) 
     if (!grid_barrier(d)) return;
     for (int t = gwarp; t < d.n_tiles; t += nwarps) tile_warp(d, t, lane);
     if (!grid_barrier(d)) return;
-    // R6: i-tiles taken one at a time from a counter (their costs differ)
+    // R6: the rebuilding replicas' i-tiles taken one at a time from a counter
+    // (their costs differ)
     __shared__ int s_tile;
+    const int n_build = d.build_prefix[d.n_rep];
     for (;;) {
         if (tid == 0) s_tile = atomicAdd(d.build_work, 1);
         __syncthreads();
-        const int I = s_tile;
+        const int w = s_tile;
         __syncthreads();
-        if (I >= d.n_tiles) break;
-        build_tile(d, I);
+        if (w >= n_build) break;
+        const int r = chunk_replica(d.build_prefix, d.n_rep, w);
+        build_tile(d, d.rep[r].tile_begin + (w - d.build_prefix[r]));
     }
     if (!grid_barrier(d)) return;
     if (gtid == 0) rebuild_finish(d);
