@@ -630,7 +630,7 @@ int Batch::pack() {
         d.nb_work = d.chunk_prefix + R + 1;
         d.build_work = d.chunk_prefix + R + 2;
         d.grid_bar = A.alloc<unsigned>(2);
-        d.build_prefix = A.alloc<int>(R + 1);
+        d.build_prefix = A.alloc<int>(3 * (R + 1));
         // host-side staging
         std::vector<double> hm(n_atoms), hq(n_atoms), hx(n_atoms), hy(n_atoms), hz(n_atoms), hvx(n_atoms),
             hvy(n_atoms), hvz(n_atoms), hxr(n_atoms), hyr(n_atoms), hzr(n_atoms);

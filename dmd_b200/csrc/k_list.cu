@@ -683,49 +683,73 @@ __global__ void __launch_bounds__(NT_B, 4) k_rebuild(Dev d, const int* bin_rep) 
     const int gtid = blockIdx.x * NT_B + tid;
     const int gwarp = gtid >> 5, nwarps = gthreads >> 5;
     // R0: chunk counters of the replicas that rebuild, work counter of R6 and
-    // the prefix of the rebuilding replicas' tiles (R6 visits only those)
+    // the prefixes of the rebuilding replicas' atoms, sort cells and tiles (the
+    // later phases visit only those)
     if (gtid == 0) *d.build_work = 0;
     for (int r = gtid; r < d.n_rep; r += gthreads)
         if (d.st[r].rebuild) d.st[r].n_chunks = 0;
-    if (blockIdx.x == 0 && tid < 32) {
+    if (blockIdx.x == 0 && tid < 96) {  // warps 0, 1, 2: atoms, sort cells, tiles
+        const int kind = tid >> 5;
+        int* pre = d.build_prefix + kind * (d.n_rep + 1);
         int run = 0;
         for (int base = 0; base < d.n_rep; base += 32) {
             const int r = base + lane;
-            const int v = (r < d.n_rep && d.st[r].rebuild) ? d.rep[r].n_tiles : 0;
+            int v = 0;
+            if (r < d.n_rep && d.st[r].rebuild) {
+                const Rep& R = d.rep[r];
+                v = kind == 0 ? R.n_atoms : (kind == 1 ? R.nvx * R.nvx * R.nvz : R.n_tiles);
+            }
             int incl = v;
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
                 const int t = __shfl_up_sync(FULL, incl, o);
                 if (lane >= o) incl += t;
             }
-            if (r < d.n_rep) d.build_prefix[r] = run + incl - v;
+            if (r < d.n_rep) pre[r] = run + incl - v;
             run += __shfl_sync(FULL, incl, 31);
         }
-        if (lane == 0) d.build_prefix[d.n_rep] = run;
+        if (lane == 0) pre[d.n_rep] = run;
     }
-    for (int a = gtid; a < d.n_atoms; a += gthreads) bin_atom(d, a);
+    if (!grid_barrier(d)) return;
+    // the phases below visit only the rebuilding replicas' atoms, cells and tiles
+    const int* pa = d.build_prefix;
+    const int* pb = pa + d.n_rep + 1;
+    const int* pt = pb + d.n_rep + 1;
+    const int n_a = pa[d.n_rep], n_b = pb[d.n_rep], n_t = pt[d.n_rep];
+    for (int w = gtid; w < n_a; w += gthreads) {
+        const int r = chunk_replica(pa, d.n_rep, w);
+        bin_atom(d, d.rep[r].atom_begin + (w - pa[r]));
+    }
     if (!grid_barrier(d)) return;
     for (int r = blockIdx.x; r < d.n_rep; r += gridDim.x)
         if (d.st[r].rebuild) bin_scan_replica(d, r);
     if (!grid_barrier(d)) return;
-    for (int a = gtid; a < d.n_atoms; a += gthreads) bin_scatter_atom(d, a);
+    for (int w = gtid; w < n_a; w += gthreads) {
+        const int r = chunk_replica(pa, d.n_rep, w);
+        bin_scatter_atom(d, d.rep[r].atom_begin + (w - pa[r]));
+    }
     if (!grid_barrier(d)) return;
-    for (int b = gwarp; b < d.n_bins; b += nwarps) bin_sort_warp(d, bin_rep, b, lane);
+    for (int w = gwarp; w < n_b; w += nwarps) {
+        const int r = chunk_replica(pb, d.n_rep, w);
+        bin_sort_warp(d, bin_rep, d.rep[r].bin_begin + (w - pb[r]), lane);
+    }
     if (!grid_barrier(d)) return;
-    for (int t = gwarp; t < d.n_tiles; t += nwarps) tile_warp(d, t, lane);
+    for (int w = gwarp; w < n_t; w += nwarps) {
+        const int r = chunk_replica(pt, d.n_rep, w);
+        tile_warp(d, d.rep[r].tile_begin + (w - pt[r]), lane);
+    }
     if (!grid_barrier(d)) return;
     // R6: the rebuilding replicas' i-tiles taken one at a time from a counter
     // (their costs differ)
     __shared__ int s_tile;
-    const int n_build = d.build_prefix[d.n_rep];
     for (;;) {
         if (tid == 0) s_tile = atomicAdd(d.build_work, 1);
         __syncthreads();
         const int w = s_tile;
         __syncthreads();
-        if (w >= n_build) break;
-        const int r = chunk_replica(d.build_prefix, d.n_rep, w);
-        build_tile(d, d.rep[r].tile_begin + (w - d.build_prefix[r]));
+        if (w >= n_t) break;
+        const int r = chunk_replica(pt, d.n_rep, w);
+        build_tile(d, d.rep[r].tile_begin + (w - pt[r]));
     }
     if (!grid_barrier(d)) return;
     if (gtid == 0) rebuild_finish(d);

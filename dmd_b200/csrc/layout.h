@@ -143,7 +143,8 @@ struct Dev {
     void* pme_green;                   // cached PME influence function (mesh_cplx layout, T)
     int* nb_work;                      // pair-kernel chunk counter (reset per evaluation)
     int* build_work;                   // list-build i-tile counter (reset per rebuild)
-    int* build_prefix;                 // [n_rep + 1] prefix of the rebuilding replicas' tiles
+    int* build_prefix;                 // [3][n_rep + 1] prefixes of the rebuilding replicas'
+                                       // atoms, sort cells and tiles
     unsigned* grid_bar;                // [2] rebuild grid barrier: arrivals, generation
     // bonded terms (global atom indices)
     int n_bonds, n_angles, n_dih, n_imp;

@@ -168,7 +168,7 @@ extern "C" int dmdgpu_nonbonded_noalloc(const dmdgpu_nb_params* p, const double*
     Rep* d_rep = reinterpret_cast<Rep*>(at(sizeof(Rep)));
     RepState* d_st = reinterpret_cast<RepState*>(at(sizeof(RepState)));
     d.chunk_prefix = reinterpret_cast<int*>(at(8 * sizeof(int)));
-    d.build_prefix = d.chunk_prefix + 2;  // [2]: words 2, 3 (one replica)
+    d.build_prefix = d.chunk_prefix + 8;  // [3][2]: words 8..13 of the 256-byte block
     d.nb_work = d.chunk_prefix + 4;  // zeroed with the prefix below
     d.build_work = d.chunk_prefix + 5;
     d.grid_bar = reinterpret_cast<unsigned*>(d.chunk_prefix + 6);  // [2]: words 6, 7
