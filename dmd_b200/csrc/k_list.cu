@@ -604,10 +604,15 @@ __device__ __forceinline__ void build_tile(const Dev& d, int I) {
     }
 }
 
-// R7: close the rebuild -- capacity check, counters, flat chunk numbering.
-__device__ __forceinline__ void rebuild_finish(const Dev& d) {
-    int run = 0;
-    for (int r = 0; r < d.n_rep; ++r) {
+// R7: close the rebuild -- capacity check, counters, flat chunk numbering --
+// by one warp: each lane takes a contiguous run of replicas, a warp scan
+// places the runs.
+__device__ __forceinline__ void rebuild_finish(const Dev& d, int lane) {
+    const int n = d.n_rep;
+    const int per = (n + 31) >> 5;
+    const int r0 = min(lane * per, n), r1 = min(r0 + per, n);
+    int sum = 0;
+    for (int r = r0; r < r1; ++r) {
         RepState* s = d.st + r;
         if (s->rebuild) {
             if (s->n_chunks > d.rep[r].chunk_cap) {
@@ -619,10 +624,20 @@ __device__ __forceinline__ void rebuild_finish(const Dev& d) {
             s->list_builds += 1;
             s->L_build = s->L;
         }
-        d.chunk_prefix[r] = run;
-        run += s->n_chunks;
+        sum += s->n_chunks;
     }
-    d.chunk_prefix[d.n_rep] = run;
+    int incl = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(FULL, incl, o);
+        if (lane >= o) incl += v;
+    }
+    int run = incl - sum;
+    for (int r = r0; r < r1; ++r) {
+        d.chunk_prefix[r] = run;
+        run += d.st[r].n_chunks;
+    }
+    if (lane == 31) d.chunk_prefix[n] = incl;
 }
 
 __device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
@@ -752,7 +767,7 @@ __global__ void __launch_bounds__(NT_B, 4) k_rebuild(Dev d, const int* bin_rep) 
         build_tile(d, d.rep[r].tile_begin + (w - pt[r]));
     }
     if (!grid_barrier(d)) return;
-    if (gtid == 0) rebuild_finish(d);
+    if (gtid < 32) rebuild_finish(d, lane);
 }
 
 void launch_rebuild(const Dev& d, const int* bin_rep, int n_sm, cudaStream_t st, long long* nlaunch) {

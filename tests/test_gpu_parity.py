@@ -111,6 +111,45 @@ def test_pair_set_identical(oracle, system, profile):
     assert np.array_equal(pi, oi) and np.array_equal(pj, oj)
 
 
+def _big_water(shift_images):
+    cfg = W.water_box(n_mol=10_000, box=6.69, seed=9, spacing=0.1045).config()
+    if shift_images:
+        # atoms scattered over periodic images (unwrapped coordinates)
+        rng = np.random.default_rng(4)
+        n = len(cfg.masses)
+        L = cfg.box_size
+        cfg.pos_x = cfg.pos_x + L * rng.integers(-1, 3, n)
+        cfg.pos_y = cfg.pos_y + L * rng.integers(-2, 2, n)
+        cfg.pos_z = cfg.pos_z + L * rng.integers(-1, 2, n)
+    return cfg
+
+
+@pytest.mark.parametrize("profile", ["ref", "phys"])
+@pytest.mark.parametrize("shift_images", [False, True])
+def test_pair_set_identical_large_box(oracle, profile, shift_images):
+    """A box several cutoffs wide, so that each i-tile's candidate j-tiles are a
+    small part of the box: the pair set must still be the full O(N^2)
+    minimum-image set."""
+    cfg = _big_water(shift_images)
+    eng = _engine(cfg, "mixed", profile, skin=0.1)
+    eng.compute_forces()
+    pi, pj = eng.pair_list()
+    pos = np.stack([cfg.pos_x, cfg.pos_y, cfg.pos_z], 1)
+    rc = cfg.lj_cutoff
+    if profile == "phys":
+        rc = max(rc, cfg.coulomb_cutoff) + 0.1
+    oi, oj = oracle.pairs(pos, cfg.box_size, rc)
+    if profile == "phys":
+        n = len(cfg.masses)
+        ei = np.asarray(cfg.excl_i, np.int64)
+        ej = np.asarray(cfg.excl_j, np.int64)
+        ex = np.minimum(ei, ej) * n + np.maximum(ei, ej)
+        keep = ~np.isin(oi.astype(np.int64) * n + oj, ex)
+        oi, oj = oi[keep], oj[keep]
+    assert len(pi) == len(oi)
+    assert np.array_equal(pi, oi) and np.array_equal(pj, oj)
+
+
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_argon_trajectory_ref(oracle, precision):
     """REF profile argon NVE (the reference's LJ is correct): positions/velocities
