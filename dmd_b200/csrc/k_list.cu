@@ -161,9 +161,13 @@ __device__ __forceinline__ void tile_warp(const Dev& d, int t, int lane) {
 
 // Entry encoding: bits 0..25 j slot, 26..31 image shift (mx+1, my+1, mz+1), 2 bits each.
 //
-// R6: chunk list.  A block of BW warps per i-tile, in batches of up to MAXC
+// R6: chunk list, one block of BW warps per i-tile (lane = i atom), tiles taken
+// from a counter.  Two builders, chosen per replica by its tile count alone (so
+// a replica's chunks do not depend on what else is in the table):
+//
+// Plain scan (replicas below CELL_TILES tiles), in batches of up to MAXC
 // candidate j-tiles (J >= I, same replica, conservative bounding-box test,
-// enumerated in tile order):
+// enumerated in tile order over every later tile):
 //  1. enumerate the batch's candidates into shared memory;
 //  2. stage their j atoms in the i-tile's frame (all threads, independent loads);
 //  3. per candidate (round-robin over warps), lane = i atom: one ballot per j
@@ -171,13 +175,53 @@ __device__ __forceinline__ void tile_warp(const Dev& d, int t, int lane) {
 //     than one periodic image (small boxes) takes the general per-pair path;
 //  4. compact the non-empty entries in order and write whole chunks with one
 //     counter update per batch; fewer than 32 left over carry to the next batch.
+//
+// Cell ranges (larger replicas), where the scan over every later tile would
+// dominate:
+//  1. candidate j-tiles (J >= I, same replica): the tiles that hold the atoms
+//     of the sort grid's columns and z slabs within list-cutoff reach of the
+//     i-tile's bounding box, as ranges of tiles in slot order (every tile
+//     once); boxes too small for that scan every later tile.  Warp w takes
+//     the w-th quarter of the candidate indices; a conservative bounding-box
+//     test keeps the candidates;
+//  2. the j atoms of up to GRP candidates are loaded together, brought into
+//     the i-tile's frame (FP32) and those within the list cutoff of the
+//     i-tile's box are staged in order;
+//  3. per 32 staged j atoms, one ballot per j gives that j's 32-bit mask over
+//     the i lanes; a candidate whose two tiles need more than one periodic
+//     image (small boxes) takes the general per-pair path instead;
+//  4. each warp appends its non-empty entries in order and writes whole chunks
+//     (reserved OUTCAP / 32 at a time); the fewer than 32 left in each warp
+//     are then chained in warp order and written by warp 0.  The chunks of an
+//     i-tile (and their number, that of one stream) depend on the replica
+//     alone, not on the block or launch shape that built them.
 // Per pair: FP32 on tile-local coordinates, the reference's FP64 expression
 // within 1e-5 of the cutoff; PHYS drops excluded pairs.
 constexpr int BW = 4;
 constexpr int NT_B = 32 * BW;
-constexpr int MAXC = 48;
+constexpr int MAXC = 48;        // plain scan: candidates per batch
+constexpr int CELL_TILES = 2048;  // replicas with at least this many tiles use cell ranges
+constexpr int MAXR = 128;       // cell ranges: column z-runs per i-tile before the plain scan takes over
+constexpr int OUTCAP = 256;     // cell ranges: entries buffered per warp before chunks are reserved
+constexpr int GRP = 4;          // cell ranges: candidate j-tiles whose atoms are loaded together
+constexpr int STAGE = 32 * GRP + 64;  // staged j atoms: < 32 left over + one load group + padding
 constexpr float FAR = 1e18f;  // coordinate of padding atoms: r^2 overflows to +inf
 constexpr int ONE_IMAGE = 1 << 6;
+
+// Per-warp scratch of the cell-range builder.
+struct TileScratch {
+    float4 jx[STAGE];          // staged j atoms in the i-tile frame (w = atom index bits)
+    uint32_t je[STAGE];        // their entry words
+    uint32_t msk[32];          // masks of one group of 32 staged j atoms
+    uint32_t oe[OUTCAP + 32];  // entries waiting to be written as chunks
+    uint32_t om[OUTCAP + 32];
+    int r0[MAXR];              // candidate tile ranges: first tile
+    int rp[MAXR + 1];          // exclusive prefix of the range lengths
+    int ia[32];                // i atoms and their tile-local coordinates (general path)
+    float ilx[32], ily[32], ilz[32];
+    int nr, total;             // ranges and candidate indices (warp 0's copy is used)
+    int nleft;                 // entries left after this warp's whole chunks
+};
 
 // The reference's minimum-image r^2 < rc2 test in FP64 (src/core/pbc.h semantics).
 __device__ __forceinline__ bool ref_member(const Dev& d, int ai, int aj, double L, double invL, double rc2) {
@@ -188,23 +232,44 @@ __device__ __forceinline__ bool ref_member(const Dev& d, int ai, int aj, double 
     return r2_ref(ex, ey, ez) < rc2;
 }
 
-__device__ __forceinline__ void build_tile(const Dev& d, int I) {
+// Block scratch of the plain-scan builder.
+struct ScanScratch {
+    float lx[32], ly[32], lz[32];
+    int a[32];
+    uint32_t e[BW][64], m[BW][64];  // general path: per-warp entry buffers
+    int left[BW];
+    int cand[MAXC], cinfo[MAXC];
+    float4 coff[MAXC];              // j-tile frame -> i-tile frame (FP32)
+    float4 jx[MAXC * 32];           // staged j atoms (w = atom index bits); reused for compaction
+    uint32_t je[MAXC * 32];         // staged j entry words
+    uint32_t msk[MAXC * 32];
+    uint32_t carry_e[32], carry_m[32];
+    int wcnt[4][BW];
+    int jnext, c0;
+};
+
+__device__ __forceinline__ void build_tile_scan(const Dev& d, int I, ScanScratch& O) {
     const int tid = threadIdx.x;
     const int lane = tid & 31;
     const int wib = tid >> 5;
-    __shared__ float s_lx[32], s_ly[32], s_lz[32];
-    __shared__ int s_a[32];
-    __shared__ uint32_t s_e[BW][64], s_m[BW][64];   // general path: per-warp entry buffers
-    __shared__ int s_left[BW];
-    __shared__ int s_cand[MAXC], s_cinfo[MAXC];
-    __shared__ float4 s_coff[MAXC];                  // j-tile frame -> i-tile frame (FP32)
-    __shared__ float4 s_jx[MAXC * 32];               // staged j atoms (w = atom index bits);
-                                                     // reused for compaction
-    __shared__ uint32_t s_je[MAXC * 32];             // staged j entry words
-    __shared__ uint32_t s_msk[MAXC * 32];
-    __shared__ uint32_t s_carry_e[32], s_carry_m[32];
-    __shared__ int s_wcnt[4][BW];
-    __shared__ int s_jnext, s_c0;
+    float(&s_lx)[32] = O.lx;
+    float(&s_ly)[32] = O.ly;
+    float(&s_lz)[32] = O.lz;
+    int(&s_a)[32] = O.a;
+    uint32_t(&s_e)[BW][64] = O.e;
+    uint32_t(&s_m)[BW][64] = O.m;
+    int(&s_left)[BW] = O.left;
+    int(&s_cand)[MAXC] = O.cand;
+    int(&s_cinfo)[MAXC] = O.cinfo;
+    float4(&s_coff)[MAXC] = O.coff;
+    float4(&s_jx)[MAXC * 32] = O.jx;
+    uint32_t(&s_je)[MAXC * 32] = O.je;
+    uint32_t(&s_msk)[MAXC * 32] = O.msk;
+    uint32_t(&s_carry_e)[32] = O.carry_e;
+    uint32_t(&s_carry_m)[32] = O.carry_m;
+    int(&s_wcnt)[4][BW] = O.wcnt;
+    int& s_jnext = O.jnext;
+    int& s_c0 = O.c0;
     const int r = d.tile_rep[I];
     RepState* s = d.st + r;
     if (!s->rebuild) return;
@@ -604,6 +669,521 @@ __device__ __forceinline__ void build_tile(const Dev& d, int I) {
     }
 }
 
+__device__ __forceinline__ int mod_n(int a, int n) {
+    const int m = a % n;
+    return m < 0 ? m + n : m;
+}
+
+// Sort-grid cells [lo, lo + cnt) (modulo n) along one axis that hold every
+// wrapped coordinate within `span` of c; cnt == n: all of them.  The cell
+// index is R1's expression (w / L * n), which is monotonic in w.
+__device__ __forceinline__ void cell_reach(double c, double span, double L, int n, int& lo, int& cnt) {
+    const double fa = floor((c - span) / L * n), fb = floor((c + span) / L * n);
+    lo = 0;
+    cnt = n;
+    // every cell when the reach covers the axis (or the coordinates are not finite)
+    if (!(fb - fa + 3.0 < n) || !(fabs(fa) < 1e8) || !(fabs(fb) < 1e8)) return;
+    int a = static_cast<int>(fa), b = static_cast<int>(fb);
+    // R1 clamps a wrapped coordinate that rounds up to L into the last cell and
+    // one just below 0 into the first
+    if (mod_n(a, n) == 0) a -= 1;
+    if (mod_n(b, n) == n - 1) b += 1;
+    if (b - a + 1 < n) {
+        lo = mod_n(a, n);
+        cnt = b - a + 1;
+    }
+}
+
+// k-th smallest value of the cyclic interval [lo, lo + cnt) modulo n.
+__device__ __forceinline__ int nth_ascending(int lo, int cnt, int n, int k) {
+    const int w = lo + cnt - n;  // values that wrapped to 0 .. w-1
+    return (w > 0) ? (k < w ? k : lo + (k - w)) : lo + k;
+}
+
+__device__ __forceinline__ void build_tile_cells(const Dev& d, int I, TileScratch* SS) {
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    TileScratch& S = SS[wib];
+    TileScratch& S0 = SS[0];
+    const uint32_t lt = (1u << lane) - 1u;
+    const int r = d.tile_rep[I];
+    RepState* s = d.st + r;
+    const Rep& R = d.rep[r];
+    const double L = s->L, invL = s->invL;
+    const float Lf = static_cast<float>(L), hLf = 0.5f * Lf;
+    const bool phys = (R.flags & F_PHYS) != 0;
+    const double rc2 = R.rc_list2;
+    const float rc2_lo = static_cast<float>(rc2 * (1.0 - 1e-5));
+    const float rc2_hi = static_cast<float>(rc2 * (1.0 + 1e-5));
+    const double bb_rc2 = rc2 * (1.0 + 1e-6) + 1e-9;
+    const double cIx = d.tcx[I], cIy = d.tcy[I], cIz = d.tcz[I];
+    const float hIx = d.thx[I], hIy = d.thy[I], hIz = d.thz[I];
+    const int t_end = R.tile_begin + R.n_tiles;
+
+    // this lane's i atom; a padding i lane sits far away (+FAR), padding j atoms at -FAR
+    const int ai = d.atom_of_slot[32 * I + lane];
+    const float4 pi = d.xl32[32 * I + lane];
+    const float lix = ai >= 0 ? pi.x : FAR, liy = ai >= 0 ? pi.y : FAR, liz = ai >= 0 ? pi.z : FAR;
+    S.ia[lane] = ai;
+    S.ilx[lane] = pi.x;
+    S.ily[lane] = pi.y;
+    S.ilz[lane] = pi.z;
+    // (PHYS) exclusion partners, sorted ascending, spanning [i_lo, i_lo + i_span];
+    // an empty set never matches
+    int i_e0 = 0, i_e1 = 0, i_lo = 0x7fffffff, i_span = 0;
+    if (phys && ai >= 0) {
+        i_e0 = d.ex_start[ai];
+        i_e1 = d.ex_start[ai + 1];
+        if (i_e1 > i_e0) {
+            i_lo = d.ex_list[i_e0];
+            i_span = d.ex_list[i_e1 - 1] - i_lo;
+        }
+    }
+
+    // ---- 1a. candidate tile ranges (warp 0) ---------------------------------
+    if (wib == 0) {
+        int nr, total;
+        const double rc_m = sqrt(rc2) * (1.0 + 1e-4) + 1e-6 * L;
+        const int nvx = R.nvx, nvz = R.nvz;
+        int xlo, xc, ylo, yc, zlo, zc;
+        cell_reach(cIx, static_cast<double>(hIx) + rc_m, L, nvx, xlo, xc);
+        cell_reach(cIy, static_cast<double>(hIy) + rc_m, L, nvx, ylo, yc);
+        cell_reach(cIz, static_cast<double>(hIz) + rc_m, L, nvz, zlo, zc);
+        const int ncol = xc * yc;
+        if ((xc == nvx && yc == nvx && zc == nvz) || 2 * ncol > MAXR) {
+            nr = 1;
+            total = t_end - I;
+            if (lane == 0) {
+                S.r0[0] = I;
+                S.rp[0] = 0;
+                S.rp[1] = total;
+            }
+        } else {
+            // range q = 2 * (column k) + run: columns in ascending column index
+            // (x-major, y in the snake direction of its x row), the one or two z
+            // runs of each column in ascending bin order
+            nr = 2 * ncol;
+            const int B = R.bin_begin;
+            const int nb = nvx * nvx * nvz;
+            const int slot_end = 32 * R.tile_begin + R.n_atoms;
+            const int wz = zlo + zc - nvz;  // > 0: the z interval wraps
+            int t0[4], t1[4];
+            int lmax = I - 1;
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int q = 4 * lane + u;
+                t0[u] = I;  // empty: [I, I - 1]
+                t1[u] = I - 1;
+                if (q >= nr) continue;
+                const int kcol = q >> 1, run = q & 1;
+                const int ix = nth_ascending(xlo, xc, nvx, kcol / yc);
+                const int ky = kcol % yc;
+                const int iy = nth_ascending(ylo, yc, nvx, (ix & 1) ? yc - 1 - ky : ky);
+                const int col = ix * nvx + ((ix & 1) ? nvx - 1 - iy : iy);
+                // z runs as cell intervals [a0, a1], [b0, b1] (b empty unless wrapped)
+                int a0, a1, b0 = 1, b1 = 0;
+                if (wz > 0) {
+                    a0 = 0;
+                    a1 = wz - 1;
+                    b0 = zlo;
+                    b1 = nvz - 1;
+                } else {
+                    a0 = zlo;
+                    a1 = zlo + zc - 1;
+                }
+                // bin offsets within the column (odd columns run top-down)
+                if (col & 1) {
+                    const int na0 = nvz - 1 - a1, na1 = nvz - 1 - a0;
+                    const int nb0 = nvz - 1 - b1, nb1 = nvz - 1 - b0;
+                    a0 = na0;
+                    a1 = na1;
+                    b0 = nb0;
+                    b1 = nb1;
+                    if (wz > 0) {  // ascending: b's offsets come first
+                        int t = a0;
+                        a0 = b0;
+                        b0 = t;
+                        t = a1;
+                        a1 = b1;
+                        b1 = t;
+                    }
+                }
+                const int o0 = run ? b0 : a0, o1 = run ? b1 : a1;
+                if (o1 < o0) continue;
+                const int g0 = B + col * nvz + o0, g1 = B + col * nvz + o1;
+                const int s_lo = d.bin_start[g0];
+                const int s_hi = (g1 + 1 < B + nb) ? d.bin_start[g1 + 1] : slot_end;
+                if (s_hi <= s_lo) continue;
+                t0[u] = max(s_lo >> 5, I);
+                t1[u] = (s_hi - 1) >> 5;
+                lmax = max(lmax, t1[u]);
+            }
+            // ranges are disjoint in slots and ascending, so consecutive ones share at
+            // most an end tile: start each after the largest tile of those before it
+            int prev = lmax;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int v = __shfl_up_sync(FULL, prev, o);
+                if (lane >= o) prev = max(prev, v);
+            }
+            prev = __shfl_up_sync(FULL, prev, 1);
+            if (lane == 0) prev = I - 1;
+            int len[4], lsum = 0;
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                t0[u] = max(t0[u], prev + 1);
+                len[u] = max(t1[u] - t0[u] + 1, 0);
+                prev = max(prev, t1[u]);
+                lsum += len[u];
+            }
+            int incl = lsum;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int v = __shfl_up_sync(FULL, incl, o);
+                if (lane >= o) incl += v;
+            }
+            int run_v = incl - lsum;
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int q = 4 * lane + u;
+                if (q < nr) {
+                    S.r0[q] = t0[u];
+                    S.rp[q] = run_v;
+                }
+                run_v += len[u];
+            }
+            total = __shfl_sync(FULL, incl, 31);
+            if (lane == 0) S.rp[nr] = total;
+        }
+        if (lane == 0) {
+            S.nr = nr;
+            S.total = total;
+        }
+    }
+    __syncthreads();
+    const int nr = S0.nr, total = S0.total;
+    // this warp's quarter of the candidate indices
+    const int v_beg = static_cast<int>(static_cast<long long>(total) * wib / BW);
+    const int v_end = static_cast<int>(static_cast<long long>(total) * (wib + 1) / BW);
+
+    // ---- output: ordered entries, written as whole chunks reserved in bulk ---
+    int no = 0;  // entries waiting in S.oe / S.om (warp-uniform)
+    auto write_chunks = [&](int count) {
+        const int k = (count + 31) >> 5;
+        int c0 = 0;
+        if (lane == 0) c0 = atomicAdd(&s->n_chunks, k);
+        c0 = __shfl_sync(FULL, c0, 0);
+        if (c0 + k > R.chunk_cap && lane == 0) set_status(s, ST_CAPACITY);
+        for (int q = 0; q < k && c0 + q < R.chunk_cap; ++q) {
+            const int g = R.chunk_begin + c0 + q;
+            const int idx = 32 * q + lane;
+            if (lane == 0) d.chunk_itile[g] = I;
+            d.chunk_j[32 * g + lane] = idx < count ? S.oe[idx] : 0u;
+            d.chunk_mask[32 * g + lane] = idx < count ? S.om[idx] : 0u;
+        }
+    };
+    auto emit = [&](uint32_t e, uint32_t m) {
+        const uint32_t has = __ballot_sync(FULL, m != 0u);
+        const int pos = no + __popc(has & lt);
+        if (m) {
+            S.oe[pos] = e;
+            S.om[pos] = m;
+        }
+        no += __popc(has);
+        __syncwarp();
+        if (no >= OUTCAP) {
+            write_chunks(OUTCAP);
+            __syncwarp();
+            if (lane < no - OUTCAP) {
+                S.oe[lane] = S.oe[lane + OUTCAP];
+                S.om[lane] = S.om[lane + OUTCAP];
+            }
+            no -= OUTCAP;
+            __syncwarp();
+        }
+    };
+
+    // ---- 3. masks of `count` (<= 32) staged j atoms from `base` (lane = i atom)
+    int ns = 0, s0 = 0;  // staged j atoms S.jx[s0, s0 + ns) (warp-uniform)
+    auto mask_group = [&](int base, int count) {
+        if (lane >= count) {
+            S.jx[base + lane] = make_float4(-FAR, -FAR, -FAR, __int_as_float(-1));
+            S.je[base + lane] = 0u;
+        }
+        __syncwarp();
+        const float4* pjs = S.jx + base;
+        uint32_t rare = 0;
+#pragma unroll
+        for (int j = 0; j < 32; ++j) {
+            const float4 pj = pjs[j];
+            const int a2 = __float_as_int(pj.w);
+            const float dx = pj.x - lix, dy = pj.y - liy, dz = pj.z - liz;
+            const float r2 = dx * dx + dy * dy + dz * dz;
+            const bool exr = static_cast<unsigned>(a2 - i_lo) <= static_cast<unsigned>(i_span);
+            const bool in = (r2 < rc2_lo) & !exr;
+            rare |= static_cast<uint32_t>((r2 < rc2_hi) & ((r2 >= rc2_lo) | exr)) << j;
+            const uint32_t m = __ballot_sync(FULL, in);
+            if (lane == 0) S.msk[j] = m;
+        }
+        __syncwarp();
+        // pairs at the cutoff band or among the i atom's exclusion partners (rare):
+        // the FP64 reference test, then the exclusions
+        while (rare) {
+            const int j = __ffs(rare) - 1;
+            rare &= rare - 1;
+            const float4 pj = pjs[j];
+            const int a2 = __float_as_int(pj.w);
+            const float dx = pj.x - lix, dy = pj.y - liy, dz = pj.z - liz;
+            const float r2 = dx * dx + dy * dy + dz * dz;
+            bool in = (r2 < rc2_lo) || ref_member(d, ai, a2, L, invL, rc2);
+            if (in && static_cast<unsigned>(a2 - i_lo) <= static_cast<unsigned>(i_span))
+                for (int e = i_e0; e < i_e1; ++e) in &= (d.ex_list[e] != a2);
+            if (in) atomicOr(&S.msk[j], 1u << lane);
+        }
+        __syncwarp();
+        // lane = staged j: within the i-tile itself only pairs i < j
+        uint32_t m = S.msk[lane];
+        const uint32_t e = S.je[base + lane];
+        const int js = static_cast<int>(e & 0x03FFFFFFu);
+        if (lane >= count) m = 0u;
+        if ((js >> 5) == I) m &= (1u << (js & 31)) - 1u;
+        __syncwarp();
+        emit(e, m);
+    };
+
+    // ---- general path: one candidate with several periodic images, lane = j --
+    auto general_candidate = [&](int J) {
+        const int js = 32 * J + lane;
+        const int aj = d.atom_of_slot[js];
+        const double ddx = d.tcx[J] - cIx, ddy = d.tcy[J] - cIy, ddz = d.tcz[J] - cIz;
+        const double rx0 = round(ddx * invL), ry0 = round(ddy * invL), rz0 = round(ddz * invL);
+        float jx = 0.f, jy = 0.f, jz = 0.f;
+        int ex[8];
+        int nex = 0, e0 = 0, e1 = 0;
+        if (aj >= 0) {
+            jx = static_cast<float>((d.x[aj] - d.imgx[aj] * L) - cIx - rx0 * L);
+            jy = static_cast<float>((d.y[aj] - d.imgy[aj] * L) - cIy - ry0 * L);
+            jz = static_cast<float>((d.z[aj] - d.imgz[aj] * L) - cIz - rz0 * L);
+            e0 = d.ex_start[aj];
+            e1 = d.ex_start[aj + 1];
+            if (phys) nex = e1 - e0;
+        }
+#pragma unroll
+        for (int k = 0; k < 8; ++k) ex[k] = (k < nex) ? d.ex_list[e0 + k] : -1;
+        uint32_t todo = 0;
+        if (aj >= 0) todo = (J == I) ? lt : 0xffffffffu;
+        while (__any_sync(FULL, todo != 0)) {
+            uint32_t bits = 0, rest = 0, code0 = 0xffffffffu;
+            for (uint32_t t = todo; t; t &= t - 1) {
+                const int i = __ffs(t) - 1;
+                const int a_i = S.ia[i];
+                if (a_i < 0) continue;
+                float dx = jx - S.ilx[i], dy = jy - S.ily[i], dz = jz - S.ilz[i];
+                int sx = 0, sy = 0, sz = 0;
+                if (dx > hLf) { dx -= Lf; sx = 1; } else if (dx < -hLf) { dx += Lf; sx = -1; }
+                if (dy > hLf) { dy -= Lf; sy = 1; } else if (dy < -hLf) { dy += Lf; sy = -1; }
+                if (dz > hLf) { dz -= Lf; sz = 1; } else if (dz < -hLf) { dz += Lf; sz = -1; }
+                const float r2 = dx * dx + dy * dy + dz * dz;
+                if (r2 >= rc2_hi) continue;
+                int mx, my, mz;
+                if (r2 > rc2_lo) {
+                    // borderline: the reference's FP64 expression decides
+                    double ex_ = __dsub_rn(d.x[aj], d.x[a_i]), ey = __dsub_rn(d.y[aj], d.y[a_i]),
+                           ez = __dsub_rn(d.z[aj], d.z[a_i]);
+                    const double qx = round(__dmul_rn(ex_, invL)), qy = round(__dmul_rn(ey, invL)),
+                                 qz = round(__dmul_rn(ez, invL));
+                    ex_ = __dsub_rn(ex_, __dmul_rn(qx, L));
+                    ey = __dsub_rn(ey, __dmul_rn(qy, L));
+                    ez = __dsub_rn(ez, __dmul_rn(qz, L));
+                    if (!(r2_ref(ex_, ey, ez) < rc2)) continue;
+                    mx = d.imgx[aj] - d.imgx[a_i] - static_cast<int>(qx);
+                    my = d.imgy[aj] - d.imgy[a_i] - static_cast<int>(qy);
+                    mz = d.imgz[aj] - d.imgz[a_i] - static_cast<int>(qz);
+                } else {
+                    // displacement = w_j - w_i - (r0 + s) L
+                    mx = -static_cast<int>(rx0) - sx;
+                    my = -static_cast<int>(ry0) - sy;
+                    mz = -static_cast<int>(rz0) - sz;
+                }
+                if (phys) {
+                    bool excluded = false;
+                    if (nex <= 8) {
+#pragma unroll
+                        for (int k = 0; k < 8; ++k) excluded |= (ex[k] == a_i);
+                    } else {
+                        for (int e = e0; e < e1; ++e) excluded |= (d.ex_list[e] == a_i);
+                    }
+                    if (excluded) continue;
+                }
+                const uint32_t code = static_cast<uint32_t>((mx + 1) | ((my + 1) << 2) | ((mz + 1) << 4));
+                if (code0 == 0xffffffffu) code0 = code;
+                if (code == code0) bits |= 1u << i;
+                else rest |= 1u << i;
+            }
+            emit(static_cast<uint32_t>(js) | ((bits ? code0 : 0u) << 26), bits);
+            todo = rest;
+        }
+    };
+
+    // ---- 1b/2. candidates in tile order --------------------------------------
+    // One step per pass, each kind of work at one place in the code: a mask
+    // group when 32 atoms are staged (or fewer before a general candidate and at
+    // the end), the next 32 candidate indices, a general candidate, or the
+    // atoms of up to GRP one-image candidates.
+    const double hL = 0.5 * L;
+    int v0 = v_beg;
+    uint32_t cm = 0, gm = 0;  // candidates of the current 32 indices not yet taken; general ones
+    int J = 0, info = 0;      // this lane's candidate among them
+    float4 off = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (;;) {
+        const bool at_end = cm == 0u && v0 >= v_end;
+        const bool next_general = cm != 0u && ((gm >> (__ffs(cm) - 1)) & 1u);
+        if (ns >= 32 || (ns > 0 && (at_end || next_general))) {
+            const int cnt = min(ns, 32);
+            mask_group(s0, cnt);
+            s0 += cnt;
+            ns -= cnt;
+            continue;
+        }
+        if (at_end) break;
+        if (cm == 0u) {
+            const int v = v0 + lane;
+            v0 += 32;
+            bool cand = false;
+            if (v < v_end) {
+                // the range holding v: the last one whose prefix is <= v
+                int lo = 0, hi = nr - 1;
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (S0.rp[mid] <= v) lo = mid;
+                    else hi = mid - 1;
+                }
+                J = S0.r0[lo] + (v - S0.rp[lo]);
+                double dx = d.tcx[J] - cIx, dy = d.tcy[J] - cIy, dz = d.tcz[J] - cIz;
+                const double rx0 = round(dx * invL), ry0 = round(dy * invL), rz0 = round(dz * invL);
+                dx -= L * rx0;
+                dy -= L * ry0;
+                dz -= L * rz0;
+                const double ex = (double)(hIx + d.thx[J]), ey = (double)(hIy + d.thy[J]),
+                             ez = (double)(hIz + d.thz[J]);
+                const double gx = fmax(fabs(dx) - ex, 0.0), gy = fmax(fabs(dy) - ey, 0.0),
+                             gz = fmax(fabs(dz) - ez, 0.0);
+                cand = gx * gx + gy * gy + gz * gz <= bb_rc2;
+                // one periodic image serves every pair of the two tiles when their
+                // extents around the centre displacement stay inside half a box
+                const bool one = fabs(dx) + ex < hL && fabs(dy) + ey < hL && fabs(dz) + ez < hL;
+                info = (static_cast<int>(rx0) + 1) | ((static_cast<int>(ry0) + 1) << 2) |
+                       ((static_cast<int>(rz0) + 1) << 4) | (one ? ONE_IMAGE : 0);
+                off = make_float4(static_cast<float>(dx), static_cast<float>(dy), static_cast<float>(dz), 0.f);
+            }
+            cm = __ballot_sync(FULL, cand);
+            gm = __ballot_sync(FULL, cand && !(info & ONE_IMAGE));
+            continue;
+        }
+        if (next_general) {
+            const int k = __ffs(cm) - 1;
+            cm &= cm - 1;
+            general_candidate(__shfl_sync(FULL, J, k));
+            continue;
+        }
+        // up to GRP one-image candidates before the next general one, in order;
+        // the fewer than 32 atoms left staged move to the front first
+        if (s0 > 0) {
+            float4 pk = make_float4(0.f, 0.f, 0.f, 0.f);
+            uint32_t ek = 0u;
+            if (lane < ns) {
+                pk = S.jx[s0 + lane];
+                ek = S.je[s0 + lane];
+            }
+            __syncwarp();
+            if (lane < ns) {
+                S.jx[lane] = pk;
+                S.je[lane] = ek;
+            }
+            s0 = 0;
+            __syncwarp();
+        }
+        const uint32_t gpend = gm & cm;  // general candidates not yet taken (none is lowest)
+        const uint32_t avail = gpend ? (cm & ((gpend & (0u - gpend)) - 1u)) : cm;
+        uint32_t take = avail;
+        int kk[GRP], aj[GRP];
+        float4 pg[GRP];
+#pragma unroll
+        for (int u = 0; u < GRP; ++u) {
+            kk[u] = take ? __ffs(take) - 1 : -1;
+            take &= take - 1;
+            const int Jk = __shfl_sync(FULL, J, kk[u] & 31);
+            aj[u] = -1;
+            pg[u] = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (kk[u] >= 0) {
+                aj[u] = d.atom_of_slot[32 * Jk + lane];
+                pg[u] = d.xl32[32 * Jk + lane];
+            }
+        }
+        cm &= ~(avail & ~take);  // the candidates taken
+#pragma unroll
+        for (int u = 0; u < GRP; ++u) {
+            const int k = kk[u] & 31;
+            const int Jk = __shfl_sync(FULL, J, k);
+            const int ik = __shfl_sync(FULL, info, k);
+            const float ox = __shfl_sync(FULL, off.x, k), oy = __shfl_sync(FULL, off.y, k),
+                        oz = __shfl_sync(FULL, off.z, k);
+            bool keep = false;
+            float4 pj = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (kk[u] >= 0 && aj[u] >= 0) {
+                pj = make_float4(pg[u].x + ox, pg[u].y + oy, pg[u].z + oz, __int_as_float(aj[u]));
+                const float gx = fmaxf(fabsf(pj.x) - hIx, 0.f), gy = fmaxf(fabsf(pj.y) - hIy, 0.f),
+                            gz = fmaxf(fabsf(pj.z) - hIz, 0.f);
+                keep = gx * gx + gy * gy + gz * gz <= rc2_hi * 1.0001f + 1e-6f;
+            }
+            const uint32_t code = static_cast<uint32_t>((2 - (ik & 3)) | ((2 - ((ik >> 2) & 3)) << 2) |
+                                                        ((2 - ((ik >> 4) & 3)) << 4));
+            const uint32_t kb = __ballot_sync(FULL, keep);
+            if (keep) {
+                const int pos = ns + __popc(kb & lt);
+                S.jx[pos] = pj;
+                S.je[pos] = static_cast<uint32_t>(32 * Jk + lane) | (code << 26);
+            }
+            ns += __popc(kb);
+        }
+        __syncwarp();
+    }
+    // whole chunks of this warp; the rest (< 32) moves to the front
+    const int whole = no & ~31;
+    if (whole > 0) {
+        write_chunks(whole);
+        __syncwarp();
+        uint32_t e = 0u, m = 0u;
+        if (lane < no - whole) {
+            e = S.oe[whole + lane];
+            m = S.om[whole + lane];
+        }
+        __syncwarp();
+        if (lane < no - whole) {
+            S.oe[lane] = e;
+            S.om[lane] = m;
+        }
+        no -= whole;
+    }
+    if (lane == 0) S.nleft = no;
+    __syncthreads();
+    if (wib == 0) {
+        // the leftovers of the other warps, in warp order, after warp 0's own
+        for (int w = 1; w < BW; ++w) {
+            const int nl = SS[w].nleft;
+            emit(lane < nl ? SS[w].oe[lane] : 0u, lane < nl ? SS[w].om[lane] : 0u);
+        }
+        if (no > 0) write_chunks(no);
+    }
+    __syncthreads();
+}
+
+// R6 block scratch: one builder runs at a time.
+union BuildScratch {
+    ScanScratch scan;
+    TileScratch cells[BW];
+};
+
 // R7: close the rebuild -- capacity check, counters, flat chunk numbering --
 // by one warp: each lane takes a contiguous run of replicas, a warp scan
 // places the runs.
@@ -754,8 +1334,9 @@ __global__ void __launch_bounds__(NT_B, 4) k_rebuild(Dev d, const int* bin_rep) 
         tile_warp(d, d.rep[r].tile_begin + (w - pt[r]), lane);
     }
     if (!grid_barrier(d)) return;
-    // R6: the rebuilding replicas' i-tiles taken one at a time from a counter
+    // R6: the rebuilding replicas' i-tiles, one per block, taken from a counter
     // (their costs differ)
+    __shared__ BuildScratch s_scr;
     __shared__ int s_tile;
     for (;;) {
         if (tid == 0) s_tile = atomicAdd(d.build_work, 1);
@@ -764,7 +1345,9 @@ __global__ void __launch_bounds__(NT_B, 4) k_rebuild(Dev d, const int* bin_rep) 
         __syncthreads();
         if (w >= n_t) break;
         const int r = chunk_replica(pt, d.n_rep, w);
-        build_tile(d, d.rep[r].tile_begin + (w - pt[r]));
+        const int I = d.rep[r].tile_begin + (w - pt[r]);
+        if (d.rep[r].n_tiles >= CELL_TILES) build_tile_cells(d, I, s_scr.cells);
+        else build_tile_scan(d, I, s_scr.scan);
     }
     if (!grid_barrier(d)) return;
     if (gtid < 32) rebuild_finish(d, lane);

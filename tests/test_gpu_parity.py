@@ -111,8 +111,13 @@ def test_pair_set_identical(oracle, system, profile):
     assert np.array_equal(pi, oi) and np.array_equal(pj, oj)
 
 
-def _big_water(shift_images):
-    cfg = W.water_box(n_mol=10_000, box=6.69, seed=9, spacing=0.1045).config()
+# (molecules, box): 938 tiles (plain-scan list build) and 2063 tiles (cell ranges)
+BIG_WATER = {"30k": (10_000, 6.69), "66k": (22_000, 8.70)}
+
+
+def _big_water(size, shift_images):
+    n_mol, box = BIG_WATER[size]
+    cfg = W.water_box(n_mol=n_mol, box=box, seed=9, spacing=box / round(box / 0.1045)).config()
     if shift_images:
         # atoms scattered over periodic images (unwrapped coordinates)
         rng = np.random.default_rng(4)
@@ -126,11 +131,12 @@ def _big_water(shift_images):
 
 @pytest.mark.parametrize("profile", ["ref", "phys"])
 @pytest.mark.parametrize("shift_images", [False, True])
-def test_pair_set_identical_large_box(oracle, profile, shift_images):
-    """A box several cutoffs wide, so that each i-tile's candidate j-tiles are a
-    small part of the box: the pair set must still be the full O(N^2)
-    minimum-image set."""
-    cfg = _big_water(shift_images)
+@pytest.mark.parametrize("size", ["30k", "66k"])
+def test_pair_set_identical_large_box(oracle, size, profile, shift_images):
+    """Boxes several cutoffs wide, below and above the tile count at which the
+    list build takes its candidates from the sort grid's nearby columns and
+    slabs: the pair set must still be the full O(N^2) minimum-image set."""
+    cfg = _big_water(size, shift_images)
     eng = _engine(cfg, "mixed", profile, skin=0.1)
     eng.compute_forces()
     pi, pj = eng.pair_list()
@@ -198,6 +204,20 @@ def test_run_to_run_bitwise():
     b = _engine(cfg, "mixed", "phys")
     a.run_n(25)
     b.run_n(25)
+    assert np.array_equal(a.positions, b.positions)
+    assert np.array_equal(a.velocities, b.velocities)
+    assert a.potential_energy == b.potential_energy
+
+
+def test_run_to_run_bitwise_cell_list_build():
+    """A box large enough for the cell-range list build: its chunks, and with
+    them the trajectory through several list rebuilds, repeat bit for bit."""
+    cfg = _big_water("66k", False)
+    a = _engine(cfg, "mixed", "phys")
+    b = _engine(cfg, "mixed", "phys")
+    a.run_n(40)
+    b.run_n(40)
+    assert a.scalars().list_builds > 1
     assert np.array_equal(a.positions, b.positions)
     assert np.array_equal(a.velocities, b.velocities)
     assert a.potential_energy == b.potential_energy
