@@ -587,6 +587,9 @@ int Batch::pack() {
         d.q = q;
         d.type = type;
         d.atom_rep = atom_rep;
+        d.fbx = A.alloc<long long>(n_atoms);
+        d.fby = A.alloc<long long>(n_atoms);
+        d.fbz = A.alloc<long long>(n_atoms);
         d.slot_of_atom = A.alloc<int>(n_atoms);
         d.xr = A.alloc<double>(n_atoms);
         d.yr = A.alloc<double>(n_atoms);
@@ -909,9 +912,8 @@ void Batch::enqueue_eval(int pass) {
     // The list rebuild (a cooperative launch: it needs the whole GPU) goes first;
     // it returns at once on steps without a rebuild.
     enqueue_rebuild();
-    // Bonded terms and PME read atom positions (they add their forces into the
-    // slots of the list just built), so they run on two more streams concurrently
-    // with the pair kernel; all force
+    // Bonded terms and PME depend on atom positions only (not on the sorted slots),
+    // so they run on two more streams concurrently with the pair kernel; all force
     // and energy sums are fixed-point atomics (order-free).  The pair kernel (the
     // longest branch, persistent) is issued first so its blocks take their SM
     // slots before the short PME and bonded blocks fill the rest.
@@ -1387,17 +1389,20 @@ int Batch::get_state(int slot, int which, double* x, double* y, double* z) {
         CK(cudaStreamSynchronize(stream_));
         const Rep& P = h.rep;
         const int s0 = 32 * P.tile_begin, ns = 32 * P.n_tiles;
-        std::vector<long long> fn(3 * ns);
+        std::vector<long long> fb(3 * n), fn(3 * ns);
         std::vector<int> sl(n);
+        CK(cudaMemcpy(fb.data(), dev_.fbx + a0, 8 * n, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(fb.data() + n, dev_.fby + a0, 8 * n, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(fb.data() + 2 * n, dev_.fbz + a0, 8 * n, cudaMemcpyDeviceToHost));
         CK(cudaMemcpy(fn.data(), dev_.fnx + s0, 8 * ns, cudaMemcpyDeviceToHost));
         CK(cudaMemcpy(fn.data() + ns, dev_.fny + s0, 8 * ns, cudaMemcpyDeviceToHost));
         CK(cudaMemcpy(fn.data() + 2 * ns, dev_.fnz + s0, 8 * ns, cudaMemcpyDeviceToHost));
         CK(cudaMemcpy(sl.data(), dev_.slot_of_atom + a0, 4 * n, cudaMemcpyDeviceToHost));
         for (int i = 0; i < n; ++i) {
             const int s = sl[i] - s0;
-            x[i] = static_cast<double>(fn[s]) * (1.0 / FSCALE);
-            y[i] = static_cast<double>(fn[ns + s]) * (1.0 / FSCALE);
-            z[i] = static_cast<double>(fn[2 * ns + s]) * (1.0 / FSCALE);
+            x[i] = static_cast<double>(fb[i] + fn[s]) * (1.0 / FSCALE);
+            y[i] = static_cast<double>(fb[n + i] + fn[ns + s]) * (1.0 / FSCALE);
+            z[i] = static_cast<double>(fb[2 * n + i] + fn[2 * ns + s]) * (1.0 / FSCALE);
         }
     } else {
         return fail(DMDGPU_ERR_PARM, "which must be 0, 1 or 2");

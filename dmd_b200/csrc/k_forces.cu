@@ -38,10 +38,9 @@ __device__ __forceinline__ void add_energy(const Dev& d, int r, int term, long l
 
 template <typename T>
 __device__ __forceinline__ void add_force(const Dev& d, int a, T fx, T fy, T fz, RepState* s) {
-    const int sl = d.slot_of_atom[a];  // forces live in slot order with the pair forces
-    fix_add(d.fnx + sl, to_fix(fx, FSCALE, s));
-    fix_add(d.fny + sl, to_fix(fy, FSCALE, s));
-    fix_add(d.fnz + sl, to_fix(fz, FSCALE, s));
+    fix_add(d.fbx + a, to_fix(fx, FSCALE, s));
+    fix_add(d.fby + a, to_fix(fy, FSCALE, s));
+    fix_add(d.fbz + a, to_fix(fz, FSCALE, s));
 }
 
 template <typename T, bool PHYS>

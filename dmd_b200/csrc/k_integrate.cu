@@ -103,6 +103,14 @@ __global__ void k_clear_forces(Dev d) {
             d.fnz[i] = 0;
         }
     }
+    if (i < d.n_atoms) {
+        int r = d.atom_rep[i];
+        if (d.st[r].eval) {
+            d.fbx[i] = 0;
+            d.fby[i] = 0;
+            d.fbz[i] = 0;
+        }
+    }
 }
 
 __device__ __forceinline__ void write_mirror(const Dev& d, int slot, int a, double x, double y, double z,
@@ -129,9 +137,9 @@ __device__ __forceinline__ void skin_check(const Dev& d, RepState* s, const Rep&
 // the pending position scale s (1 otherwise, an exact multiply) is applied
 // before the drift, x <- s x + v dt, and the mirror is written for the box
 // s L that k_eval_begin stores next.
-// One thread per atom in reference order: the FP64 state and masses are read
-// and written coalesced; the forces (all terms, one fixed-point sum per slot)
-// and the mirror are addressed through the atom's slot.
+// One thread per atom in reference order: the FP64 state, masses and bonded
+// forces are read and written coalesced; only the pair forces and the mirror
+// are addressed through the atom's slot.
 __global__ void k_kick_drift(Dev d) {
     const int a = blockIdx.x * blockDim.x + threadIdx.x;
     if (a >= d.n_atoms) return;
@@ -143,9 +151,9 @@ __global__ void k_kick_drift(Dev d) {
     const double dt = R.dt, half_dt = 0.5 * dt;
     const double inv_mass = 1.0 / d.mass[a];
     const double lam = s->vscale;
-    const double fx = from_fix(d.fnx[slot], FSCALE);
-    const double fy = from_fix(d.fny[slot], FSCALE);
-    const double fz = from_fix(d.fnz[slot], FSCALE);
+    const double fx = from_fix(d.fnx[slot] + d.fbx[a], FSCALE);
+    const double fy = from_fix(d.fny[slot] + d.fby[a], FSCALE);
+    const double fz = from_fix(d.fnz[slot] + d.fbz[a], FSCALE);
     double vx = __dmul_rn(d.vx[a], lam), vy = __dmul_rn(d.vy[a], lam), vz = __dmul_rn(d.vz[a], lam);
     vx = __dadd_rn(vx, __dmul_rn(__dmul_rn(fx, inv_mass), half_dt));
     vy = __dadd_rn(vy, __dmul_rn(__dmul_rn(fy, inv_mass), half_dt));
@@ -163,6 +171,9 @@ __global__ void k_kick_drift(Dev d) {
     d.fnx[slot] = 0;
     d.fny[slot] = 0;
     d.fnz[slot] = 0;
+    d.fbx[a] = 0;
+    d.fby[a] = 0;
+    d.fbz[a] = 0;
     write_mirror(d, slot, a, x, y, z, s->L * sc);
     skin_check(d, s, R, a, x, y, z);
 }
@@ -198,9 +209,9 @@ __global__ void k_kick2(Dev d, int andersen_ref, int andersen_phys) {
             const double half_dt = 0.5 * R.dt;
             const double m = d.mass[a];
             const double inv_mass = 1.0 / m;
-            const double fx = from_fix(d.fnx[slot], FSCALE);
-            const double fy = from_fix(d.fny[slot], FSCALE);
-            const double fz = from_fix(d.fnz[slot], FSCALE);
+            const double fx = from_fix(d.fnx[slot] + d.fbx[a], FSCALE);
+            const double fy = from_fix(d.fny[slot] + d.fby[a], FSCALE);
+            const double fz = from_fix(d.fnz[slot] + d.fbz[a], FSCALE);
             double vx = __dadd_rn(d.vx[a], __dmul_rn(__dmul_rn(fx, inv_mass), half_dt));
             double vy = __dadd_rn(d.vy[a], __dmul_rn(__dmul_rn(fy, inv_mass), half_dt));
             double vz = __dadd_rn(d.vz[a], __dmul_rn(__dmul_rn(fz, inv_mass), half_dt));

@@ -111,6 +111,7 @@ struct Dev {
     double *x, *y, *z, *vx, *vy, *vz;
     const double *mass, *q;
     const int *type, *atom_rep;
+    long long *fbx, *fby, *fbz;        // bonded + PME + exclusion forces (fixed point)
     int* slot_of_atom;
     double *xr, *yr, *zr;              // positions at the last list build
     int *imgx, *imgy, *imgz;           // periodic image frozen at the last build
@@ -121,7 +122,7 @@ struct Dev {
     float4* xl32;                      // the same at the last list build (aliases xq32 when mixed)
     double4* xq64;                     // unwrapped FP64 coordinates + charge
     int* type_s;
-    long long *fnx, *fny, *fnz;        // all forces (fixed point, slot order)
+    long long *fnx, *fny, *fnz;        // non-bonded forces (fixed point, slot order)
     // tiles
     double *tcx, *tcy, *tcz;
     float *thx, *thy, *thz;
