@@ -179,16 +179,23 @@ def rel_rms(a, b):
 
 
 class Ranks:
-    """Process-group plumbing: barrier and max over ranks (no-ops at N = 1)."""
+    """Process-group plumbing: barrier and max over ranks (no-ops at N = 1).
+
+    One process per GPU over NCCL; without a GPU (host-side tests) the same
+    calls run over gloo with CPU tensors.
+    """
 
     def __init__(self, local: int):
         import torch
         self.ws, self.rank, self.local = _dist()
-        torch.cuda.set_device(local)
+        self.cuda = torch.cuda.is_available()
+        if self.cuda:
+            torch.cuda.set_device(local)
         if self.ws > 1:
             import datetime
             import torch.distributed as dist
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+            dist.init_process_group("nccl" if self.cuda else "gloo",
+                                    timeout=datetime.timedelta(seconds=120))
 
     def barrier(self):
         if self.ws > 1:
@@ -200,7 +207,8 @@ class Ranks:
             return v
         import torch
         import torch.distributed as dist
-        t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{self.local}")
+        t = torch.tensor([v], dtype=torch.float64,
+                         device=f"cuda:{self.local}" if self.cuda else "cpu")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
