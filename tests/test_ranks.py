@@ -74,3 +74,29 @@ def test_single_rank_is_a_no_op(monkeypatch):
     R.barrier()
     assert R.max(3.5) == 3.5
     R.close()
+
+
+def _bench_reference(rank, ws):
+    env = dict(os.environ, RANK=str(rank), LOCAL_RANK=str(rank), WORLD_SIZE=str(ws),
+               CUDA_VISIBLE_DEVICES="")
+    return subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference",
+                           "--workload", "argon4k", "--steps", "2", "--warmup", "1", "--gpus", str(ws)],
+                          env=env, capture_output=True, text=True, timeout=600, cwd=ROOT)
+
+
+def test_reference_arm_rank0_reports_other_ranks_exit_quietly():
+    """The reference arm under torchrun: rank 0 alone times the reference's CPU
+    implementation and prints the line; every other rank exits 0 without work."""
+    r1 = _bench_reference(1, 2)
+    assert r1.returncode == 0, r1.stderr[-2000:]
+    assert r1.stdout.strip() == ""
+    r0 = _bench_reference(0, 2)
+    assert r0.returncode == 0, r0.stderr[-2000:]
+    line = json.loads(r0.stdout.strip().splitlines()[-1])
+    assert line["impl"] == "reference" and line["metric"] == "atom-steps/s"
+    assert line["n_gpus"] == 2 and line["value"] > 0
+    assert line["config"]["workload"] == "argon4k"
+    assert line["cpu_baseline"]["kind"] in ("reference", "port")
+    assert line["cpu_baseline"]["value"] == line["value"]
+    assert line["e2e"] == {"value": line["value"], "unit": "atom-steps/s",
+                           "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
