@@ -222,6 +222,75 @@ double orc_self_energy(double alpha, const double* q, int n, double k_e) {
 }
 void orc_philox(uint32_t* c, uint32_t k0, uint32_t k1) { philox(c, k0, k1); }
 
+// ---- distance constraints (src/integrate/constraints.cpp) ------------------
+// Constraints::apply (constraints.cpp:9-47): SHAKE as Gauss-Seidel sweeps over
+// the constraints in their order; each constraint whose |r^2 - d^2| exceeds
+// the tolerance moves both atoms along the current (minimum-image) bond
+// vector by lambda = (r^2 - d^2) / (2 d^2 (1/m_i + 1/m_j)), weighted by the
+// inverse masses; at most 100 sweeps, stopping after the first sweep whose
+// largest error (measured before each correction) is below the tolerance.
+// Positions in place; returns the number of sweeps.
+int orc_shake(int nc, const int* ci, const int* cj, const double* dist, double tol, double L,
+              const double* m, double* x, double* y, double* z) {
+    int it = 0;
+    while (it < 100) {
+        ++it;
+        double worst = 0.0;
+        for (int c = 0; c < nc; ++c) {
+            const int a = ci[c], b = cj[c];
+            double dx = x[b] - x[a], dy = y[b] - y[a], dz = z[b] - z[a];
+            min_image(L, dx, dy, dz);
+            const double r2 = dx * dx + dy * dy + dz * dz;
+            const double d2 = dist[c] * dist[c];
+            const double err = r2 - d2;
+            worst = std::max(worst, std::abs(err));
+            if (!(std::abs(err) > tol)) continue;
+            const double wa = 1.0 / m[a], wb = 1.0 / m[b];
+            const double lam = err / (2.0 * d2 * (wa + wb));
+            x[a] += lam * dx * wa;
+            y[a] += lam * dy * wa;
+            z[a] += lam * dz * wa;
+            x[b] -= lam * dx * wb;
+            y[b] -= lam * dy * wb;
+            z[b] -= lam * dz * wb;
+        }
+        if (worst < tol) break;
+    }
+    return it;
+}
+
+// Constraints::apply_rattle (constraints.cpp:49-91): the velocity half, the
+// same sweeps on r.v (relative velocity along the bond), lambda = r.v / (r^2
+// (1/m_i + 1/m_j)).  Velocities in place; returns the number of sweeps.
+int orc_rattle(int nc, const int* ci, const int* cj, double tol, double L, const double* m,
+               const double* x, const double* y, const double* z, double* vx, double* vy,
+               double* vz) {
+    int it = 0;
+    while (it < 100) {
+        ++it;
+        double worst = 0.0;
+        for (int c = 0; c < nc; ++c) {
+            const int a = ci[c], b = cj[c];
+            double dx = x[b] - x[a], dy = y[b] - y[a], dz = z[b] - z[a];
+            min_image(L, dx, dy, dz);
+            const double rv = dx * (vx[b] - vx[a]) + dy * (vy[b] - vy[a]) + dz * (vz[b] - vz[a]);
+            const double r2 = dx * dx + dy * dy + dz * dz;
+            worst = std::max(worst, std::abs(rv));
+            if (!(std::abs(rv) > tol)) continue;
+            const double wa = 1.0 / m[a], wb = 1.0 / m[b];
+            const double lam = rv / (r2 * (wa + wb));
+            vx[a] += lam * dx * wa;
+            vy[a] += lam * dy * wa;
+            vz[a] += lam * dz * wa;
+            vx[b] -= lam * dx * wb;
+            vy[b] -= lam * dy * wb;
+            vz[b] -= lam * dz * wb;
+        }
+        if (worst < tol) break;
+    }
+    return it;
+}
+
 // 3-D r2c of a K^3 real array (natural layout) -> K*K*(K/2+1) complex (interleaved)
 void orc_rfft3(int K, const double* in, double* out) {
     const int P = 2 * (K / 2 + 1);

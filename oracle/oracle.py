@@ -159,6 +159,10 @@ class Oracle:
             ("orc_dtheta4", C.c_double, [C.c_double]),
             ("orc_self_energy", C.c_double, [C.c_double, _dp, C.c_int, C.c_double]),
             ("orc_philox", None, [C.POINTER(C.c_uint32), C.c_uint32, C.c_uint32]),
+            ("orc_shake", C.c_int, [C.c_int, _ip, _ip, _dp, C.c_double, C.c_double, _dp, _dp, _dp,
+                                    _dp]),
+            ("orc_rattle", C.c_int, [C.c_int, _ip, _ip, C.c_double, C.c_double, _dp, _dp, _dp, _dp,
+                                     _dp, _dp, _dp]),
             ("orc_rfft3", None, [C.c_int, _dp, _dp]),
             ("orc_pairs_build", vp, [C.c_int, _dp, _dp, _dp, C.c_double, C.c_double]),
             ("orc_pairs_count", C.c_long, [vp]),
@@ -177,6 +181,29 @@ class Oracle:
             f.restype = res
             f.argtypes = args
         self.L = L
+
+    # -- distance constraints ------------------------------------------------
+    def shake(self, pos, masses, ci, cj, dist, box, tol=1e-8):
+        """Constraints::apply on a copy of pos; returns (positions, sweeps)."""
+        x, y, z = (np.ascontiguousarray(pos[:, k], dtype=np.float64).copy() for k in range(3))
+        i, pi = _i(ci)
+        j, pj = _i(cj)
+        d, pd = _d(dist)
+        m, pm = _d(masses)
+        it = self.L.orc_shake(len(i), pi, pj, pd, float(tol), float(box), pm, x.ctypes.data_as(_dp),
+                              y.ctypes.data_as(_dp), z.ctypes.data_as(_dp))
+        return np.stack([x, y, z], 1), it
+
+    def rattle(self, pos, vel, masses, ci, cj, box, tol=1e-8):
+        """Constraints::apply_rattle on a copy of vel; returns (velocities, sweeps)."""
+        (x, y, z), (px, py, pz) = Ref._xyz(pos)
+        vx, vy, vz = (np.ascontiguousarray(vel[:, k], dtype=np.float64).copy() for k in range(3))
+        i, pi = _i(ci)
+        j, pj = _i(cj)
+        m, pm = _d(masses)
+        it = self.L.orc_rattle(len(i), pi, pj, float(tol), float(box), pm, px, py, pz,
+                               vx.ctypes.data_as(_dp), vy.ctypes.data_as(_dp), vz.ctypes.data_as(_dp))
+        return np.stack([vx, vy, vz], 1), it
 
     # -- small functions ----------------------------------------------------
     def min_image(self, L, d):
@@ -370,6 +397,9 @@ class Ref:
             "ref_improper": (None, [C.c_int, _dp, _dp, _dp, D, C.c_int, _ip, _ip, _ip, _ip, _dp, _dp,
                                     _dp, _dp, _dp, _dp]),
             "ref_kinetic_energy": (D, [C.c_int, _dp, _dp, _dp, _dp]),
+            "ref_shake": (None, [C.c_int, C.c_int, _ip, _ip, _dp, D, D, _dp, _dp, _dp, _dp]),
+            "ref_rattle": (None, [C.c_int, C.c_int, _ip, _ip, _dp, D, D, _dp, _dp, _dp, _dp, _dp, _dp,
+                                  _dp]),
             "ref_temperature": (D, [D, C.c_int]),
             "ref_engine_create": (vp, [C.POINTER(ref_run_desc)]),
             "ref_engine_step": (None, [vp, C.c_int]),
@@ -410,6 +440,29 @@ class Ref:
                             pj.ctypes.data_as(_ip), cap)
         assert np_ <= cap
         return f.T.copy(), e.value, (pi[:np_].copy(), pj[:np_].copy())
+
+    def shake(self, pos, masses, ci, cj, dist, box, tol=1e-8):
+        """The reference's Constraints::apply on a copy of pos."""
+        x, y, z = (np.ascontiguousarray(pos[:, k], dtype=np.float64).copy() for k in range(3))
+        i, pi = _i(ci)
+        j, pj = _i(cj)
+        d, pd = _d(dist)
+        m, pm = _d(masses)
+        self.L.ref_shake(len(x), len(i), pi, pj, pd, float(tol), float(box), pm,
+                         x.ctypes.data_as(_dp), y.ctypes.data_as(_dp), z.ctypes.data_as(_dp))
+        return np.stack([x, y, z], 1)
+
+    def rattle(self, pos, vel, masses, ci, cj, dist, box, tol=1e-8):
+        """The reference's Constraints::apply_rattle on a copy of vel."""
+        (x, y, z), (px, py, pz) = self._xyz(pos)
+        vx, vy, vz = (np.ascontiguousarray(vel[:, k], dtype=np.float64).copy() for k in range(3))
+        i, pi = _i(ci)
+        j, pj = _i(cj)
+        d, pd = _d(dist)
+        m, pm = _d(masses)
+        self.L.ref_rattle(len(x), len(i), pi, pj, pd, float(tol), float(box), pm, px, py, pz,
+                          vx.ctypes.data_as(_dp), vy.ctypes.data_as(_dp), vz.ctypes.data_as(_dp))
+        return np.stack([vx, vy, vz], 1)
 
     def _bonded(self, fn, pos, box, n, *args):
         keep, (px, py, pz) = self._xyz(pos)

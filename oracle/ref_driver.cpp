@@ -46,6 +46,7 @@
 #include "force/periodic_dihedral.h"
 #include "force/harmonic_improper.h"
 #include "integrate/integrator.h"
+#include "integrate/constraints.h"
 #include "thermostat/thermostat.h"
 #include "thermostat/berendsen.h"
 #include "thermostat/nose_hoover.h"
@@ -63,6 +64,51 @@ std::vector<int> veci(const int* p, int n) { return std::vector<int>(p, p + n); 
 }  // namespace
 
 extern "C" {
+
+// ---- integrate/constraints: the reference's SHAKE / RATTLE on arrays --------
+void ref_shake(int n, int nc, const int* ci, const int* cj, const double* dist, double tol,
+               double L, const double* m, double* x, double* y, double* z) {
+    SystemData sys(static_cast<size_t>(n));
+    sys.masses = vec(m, n);
+    sys.pos_x = vec(x, n);
+    sys.pos_y = vec(y, n);
+    sys.pos_z = vec(z, n);
+    ConstraintsParams p;
+    p.i = veci(ci, nc);
+    p.j = veci(cj, nc);
+    p.distance_target = vec(dist, nc);
+    p.tolerance = tol;
+    Constraints c(std::move(p));
+    Cell cell(L, L, L);
+    c.apply(sys, cell);
+    std::copy(sys.pos_x.begin(), sys.pos_x.end(), x);
+    std::copy(sys.pos_y.begin(), sys.pos_y.end(), y);
+    std::copy(sys.pos_z.begin(), sys.pos_z.end(), z);
+}
+
+void ref_rattle(int n, int nc, const int* ci, const int* cj, const double* dist, double tol,
+                double L, const double* m, const double* x, const double* y, const double* z,
+                double* vx, double* vy, double* vz) {
+    SystemData sys(static_cast<size_t>(n));
+    sys.masses = vec(m, n);
+    sys.pos_x = vec(x, n);
+    sys.pos_y = vec(y, n);
+    sys.pos_z = vec(z, n);
+    sys.vel_x = vec(vx, n);
+    sys.vel_y = vec(vy, n);
+    sys.vel_z = vec(vz, n);
+    ConstraintsParams p;
+    p.i = veci(ci, nc);
+    p.j = veci(cj, nc);
+    p.distance_target = vec(dist, nc);
+    p.tolerance = tol;
+    Constraints c(std::move(p));
+    Cell cell(L, L, L);
+    c.apply_rattle(sys, cell);
+    std::copy(sys.vel_x.begin(), sys.vel_x.end(), vx);
+    std::copy(sys.vel_y.begin(), sys.vel_y.end(), vy);
+    std::copy(sys.vel_z.begin(), sys.vel_z.end(), vz);
+}
 
 // ---- core/cell ----------------------------------------------------------
 void ref_min_image(double L, double dx, double dy, double dz, double* out) {

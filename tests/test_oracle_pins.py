@@ -301,3 +301,52 @@ def test_phys_pme_vs_direct_ewald(oracle):
 def test_philox_known_answer(oracle):
     # Philox4x32-10 test vector from the Random123 distribution (counter 0, key 0)
     assert oracle.philox([0, 0, 0, 0], 0) == [0x6627e8d5, 0xe169c58d, 0xbc57ac4c, 0x9b00dbd8]
+
+
+# ---- distance constraints: SHAKE / RATTLE (src/integrate/constraints.cpp) ----
+def test_shake_rattle_kat(oracle):
+    # tests/unit/integrate/test_constraints.cpp:11-92 (box 100 nm: no wrapping)
+    m2, m3 = np.ones(2), np.ones(3)
+    p, _ = oracle.shake(np.array([[0.0, 0.0, 0.0], [1.1, 0.1, 0.05]]), m2, [0], [1], [1.0], 100.0)
+    assert abs(np.linalg.norm(p[1] - p[0]) - 1.0) < 1e-6
+    p, _ = oracle.shake(np.array([[0.0, 0.0, 0.0], [1.05, 0.1, 0.0], [2.1, -0.1, 0.0]]), m3,
+                        [0, 1], [1, 2], [1.0, 1.0], 100.0)
+    assert abs(np.linalg.norm(p[1] - p[0]) - 1.0) < 1e-6
+    assert abs(np.linalg.norm(p[2] - p[1]) - 1.0) < 1e-6
+    pos = np.array([[0.0, 0.0, 0.0], [1.0, 0.0, 0.0]])
+    v, _ = oracle.rattle(pos, np.array([[0.1, 0.0, 0.0], [0.3, 0.0, 0.0]]), m2, [0], [1], 100.0)
+    assert abs((pos[1, 0] - pos[0, 0]) * (v[1, 0] - v[0, 0])) < 1e-8
+
+
+def _constrained_water(n_mol, seed, jitter):
+    """Rigid-water constraints (O-H1, O-H2, H1-H2) on a perturbed water box
+    shifted so that molecules straddle the periodic boundary."""
+    w = W.water_box(n_mol=n_mol, box=(n_mol / 33.43) ** (1 / 3), seed=seed, spacing=0.1)
+    rng = np.random.default_rng(seed)
+    L = w.box
+    pos = w.pos + rng.normal(0.0, jitter, w.pos.shape) + 0.5 * L
+    mol = np.arange(n_mol) * 3
+    ci = np.stack([mol, mol, mol + 1], 1).reshape(-1).astype(np.int32)
+    cj = np.stack([mol + 1, mol + 2, mol + 2], 1).reshape(-1).astype(np.int32)
+    r0, th = 0.09572, math.radians(104.52)
+    dist = np.tile([r0, r0, 2 * r0 * math.sin(th / 2)], n_mol)
+    vel = rng.normal(0.0, 0.5, pos.shape)
+    return pos, vel, w.mass, ci, cj, dist, L
+
+
+@pytest.mark.parametrize("jitter,tol", [(0.002, 1e-8), (0.01, 1e-10)])
+def test_shake_rattle_bitwise_vs_reference(oracle, ref, jitter, tol):
+    pos, vel, m, ci, cj, dist, L = _constrained_water(300, 11, jitter)
+    p_o, sweeps = oracle.shake(pos, m, ci, cj, dist, L, tol)
+    p_r = ref.shake(pos, m, ci, cj, dist, L, tol)
+    assert sweeps > 1
+    assert np.array_equal(p_o, p_r)
+    v_o, _ = oracle.rattle(p_o, vel, m, ci, cj, L, tol)
+    v_r = ref.rattle(p_r, vel, m, ci, cj, dist, L, tol)
+    assert np.array_equal(v_o, v_r)
+    # converged: bond lengths and relative velocities along the bonds
+    d = p_o[cj] - p_o[ci]
+    d -= np.round(d / L) * L
+    r2 = (d ** 2).sum(1)
+    assert np.abs(r2 - dist ** 2).max() < 10 * tol
+    assert np.abs((d * (v_o[cj] - v_o[ci])).sum(1)).max() < 10 * tol
