@@ -890,6 +890,10 @@ struct orc_run {
     double b_pressure, b_tau, b_compress;
     uint64_t rng_seed;  // phys Andersen (Philox key)
     int brute_list;     // ref profile: rebuild the LJ list with the reference's O(N^2) loop
+    int n_cons;         // SHAKE / RATTLE distance constraints (0: none)
+    const int *cons_i, *cons_j;
+    const double* cons_dist;
+    double cons_tol;
 };
 
 struct OrcEngine {
@@ -911,6 +915,9 @@ struct OrcEngine {
     orc_energy e{};
     bool have_forces{false};
     double pscale{1.0};  // phys: barostat scale chosen at the end of a step, applied with the next drift
+    std::vector<int> cons_i, cons_j;  // distance constraints, in the order they are swept
+    std::vector<double> cons_d;
+    double cons_tol{1e-6};
 };
 
 void* orc_engine_create(const orc_system* s, const orc_run* r) {
@@ -981,6 +988,12 @@ void* orc_engine_create(const orc_system* s, const orc_run* r) {
             double lam = std::sqrt(r->init_temperature / ta);
             for (int i = 0; i < n; ++i) { E->vx[i] *= lam; E->vy[i] *= lam; E->vz[i] *= lam; }
         }
+    }
+    if (r->n_cons > 0) {  // constraint_type "shake" with pairs (simulation_engine.cpp:294-300)
+        cpi(E->cons_i, r->cons_i, r->n_cons);
+        cpi(E->cons_j, r->cons_j, r->n_cons);
+        cpd(E->cons_d, r->cons_dist, r->n_cons);
+        E->cons_tol = r->cons_tol;
     }
     return E;
 }
@@ -1170,6 +1183,37 @@ void eng_apply_pending_scale(OrcEngine* E) {
     E->pscale = 1.0;
 }
 
+// After the drift (simulation_engine.cpp:67): SHAKE on the new positions.
+// phys: the displacement SHAKE makes is also given to the half-step velocities
+// (v += dx / dt), so that positions and velocities stay consistent.
+void eng_shake(OrcEngine* E) {
+    if (E->cons_i.empty()) return;
+    const int n = static_cast<int>(E->x.size());
+    const bool phys = E->s.profile == 1;
+    std::vector<double> x0, y0, z0;
+    if (phys) {
+        x0 = E->x;
+        y0 = E->y;
+        z0 = E->z;
+    }
+    orc_shake(static_cast<int>(E->cons_i.size()), E->cons_i.data(), E->cons_j.data(), E->cons_d.data(),
+              E->cons_tol, E->L, E->m.data(), E->x.data(), E->y.data(), E->z.data());
+    if (phys)
+        for (int i = 0; i < n; ++i) {
+            E->vx[i] += (E->x[i] - x0[i]) / E->dt;
+            E->vy[i] += (E->y[i] - y0[i]) / E->dt;
+            E->vz[i] += (E->z[i] - z0[i]) / E->dt;
+        }
+}
+
+// After the second half kick (simulation_engine.cpp:78): RATTLE on the velocities.
+void eng_rattle(OrcEngine* E) {
+    if (E->cons_i.empty()) return;
+    orc_rattle(static_cast<int>(E->cons_i.size()), E->cons_i.data(), E->cons_j.data(), E->cons_tol,
+               E->L, E->m.data(), E->x.data(), E->y.data(), E->z.data(), E->vx.data(), E->vy.data(),
+               E->vz.data());
+}
+
 }  // namespace
 
 extern "C" {
@@ -1186,8 +1230,10 @@ void orc_engine_step(void* h, int nsteps) {
         eng_half_kick(E);
         if (E->s.profile == 1) eng_apply_pending_scale(E);
         eng_advance(E);
+        eng_shake(E);
         eng_compute(E);
         eng_half_kick(E);
+        eng_rattle(E);
         eng_thermostat(E);
         eng_barostat(E);
         ++E->step;

@@ -74,7 +74,9 @@ class orc_run(C.Structure):
                 ("init_temperature", C.c_double), ("thermostat", C.c_int),
                 ("t_temp", C.c_double), ("t_tau", C.c_double), ("t_freq", C.c_double),
                 ("barostat", C.c_int), ("b_pressure", C.c_double), ("b_tau", C.c_double),
-                ("b_compress", C.c_double), ("rng_seed", C.c_uint64), ("brute_list", C.c_int)]
+                ("b_compress", C.c_double), ("rng_seed", C.c_uint64), ("brute_list", C.c_int),
+                ("n_cons", C.c_int), ("cons_i", _ip), ("cons_j", _ip), ("cons_dist", _dp),
+                ("cons_tol", C.c_double)]
 
 
 THERMO = {"none": 0, "berendsen": 1, "nose-hoover": 2, "andersen": 3}
@@ -314,6 +316,12 @@ class OracleEngine:
         r.b_pressure, r.b_tau, r.b_compress = cfg.barostat.pressure, cfg.barostat.tau, cfg.barostat.compressibility
         r.rng_seed = rng_seed
         r.brute_list = int(bool(brute_list))
+        if cfg.constraint_type == "shake" and len(cfg.constraint_i):
+            ci, pi = _i(cfg.constraint_i)
+            cj, pj = _i(cfg.constraint_j)
+            k.extend([ci, cj])
+            r.n_cons, r.cons_i, r.cons_j = len(ci), pi, pj
+            r.cons_dist, r.cons_tol = d(cfg.constraint_dist), float(cfg.constraint_tolerance)
         self.n = len(cfg.masses)
         self.h = o.L.orc_engine_create(C.byref(self.S.s), C.byref(r))
         self._k = k
@@ -365,6 +373,8 @@ class ref_run_desc(C.Structure):
         ("t_freq", C.c_double), ("barostat", C.c_int), ("b_pressure", C.c_double),
         ("b_tau", C.c_double), ("b_compress", C.c_double), ("gen_vel", C.c_int), ("seed", C.c_int),
         ("init_temperature", C.c_double),
+        ("n_cons", C.c_int), ("cons_i", _ip), ("cons_j", _ip), ("cons_dist", _dp),
+        ("cons_tol", C.c_double),
     ]
 
 
@@ -586,6 +596,9 @@ class RefEngine:
         s.barostat = BARO[cfg.barostat.type]
         s.b_pressure, s.b_tau, s.b_compress = cfg.barostat.pressure, cfg.barostat.tau, cfg.barostat.compressibility
         s.gen_vel, s.seed, s.init_temperature = int(bool(cfg.gen_vel)), int(cfg.seed), cfg.init_temperature
+        if cfg.constraint_type == "shake" and len(cfg.constraint_i):
+            s.n_cons, s.cons_i, s.cons_j = len(cfg.constraint_i), i(cfg.constraint_i), i(cfg.constraint_j)
+            s.cons_dist, s.cons_tol = d(cfg.constraint_dist), float(cfg.constraint_tolerance)
         self.n = n
         self.h = r.L.ref_engine_create(C.byref(s))
         self._k = k

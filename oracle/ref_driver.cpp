@@ -278,6 +278,7 @@ struct RefEngine {
     std::unique_ptr<ForceEngine> fe;
     std::unique_ptr<Thermostat> thermo;
     std::unique_ptr<Barostat> baro;
+    std::unique_ptr<Constraints> cons;
     LennardJones* lj{nullptr};
     Integrator integ;
     Cell cell;
@@ -320,6 +321,10 @@ struct ref_run_desc {
     double b_pressure, b_tau, b_compress;
     int gen_vel, seed;
     double init_temperature;
+    int n_cons;  // SHAKE / RATTLE distance constraints (0: none)
+    const int *cons_i, *cons_j;
+    const double* cons_dist;
+    double cons_tol;
 };
 
 void* ref_engine_create(const ref_run_desc* d) {
@@ -493,6 +498,14 @@ void* ref_engine_create(const ref_run_desc* d) {
             }
         }
     }
+    if (d->n_cons > 0) {  // build_simulation (simulation_engine.cpp:293-300)
+        ConstraintsParams cp;
+        cp.i = veci(d->cons_i, d->n_cons);
+        cp.j = veci(d->cons_j, d->n_cons);
+        cp.distance_target = vec(d->cons_dist, d->n_cons);
+        cp.tolerance = d->cons_tol;
+        e->cons = std::make_unique<Constraints>(std::move(cp));
+    }
     return e;
 }
 
@@ -510,12 +523,14 @@ void ref_engine_step(void* h, int nsteps) {
         e->fe->compute(s, e->cell);
         e->integ.half_kick(s, e->dt);
         e->integ.advance(s, e->dt);
+        if (e->cons) e->cons->apply(s, e->cell);
         s.forces_x.assign(s.n_atoms, 0.0);
         s.forces_y.assign(s.n_atoms, 0.0);
         s.forces_z.assign(s.n_atoms, 0.0);
         s.potential_energy = 0.0;
         e->fe->compute(s, e->cell);
         e->integ.half_kick(s, e->dt);
+        if (e->cons) e->cons->apply_rattle(s, e->cell);
         if (e->thermo) e->thermo->apply(s, e->dt);
         if (e->baro) e->baro->apply(s, e->cell, e->dt);
         ++e->step;

@@ -350,3 +350,53 @@ def test_shake_rattle_bitwise_vs_reference(oracle, ref, jitter, tol):
     r2 = (d ** 2).sum(1)
     assert np.abs(r2 - dist ** 2).max() < 10 * tol
     assert np.abs((d * (v_o[cj] - v_o[ci])).sum(1)).max() < 10 * tol
+
+
+def _rigid(c, tol):
+    """Rigid-water constraints (O-H1, O-H2, H1-H2) on a water config."""
+    n_mol = len(c.masses) // 3
+    mol = np.arange(n_mol) * 3
+    r0, th = 0.09572, math.radians(104.52)
+    c.constraint_type = "shake"
+    c.constraint_tolerance = tol
+    c.constraint_i = np.stack([mol, mol, mol + 1], 1).reshape(-1).astype(np.int32)
+    c.constraint_j = np.stack([mol + 1, mol + 2, mol + 2], 1).reshape(-1).astype(np.int32)
+    c.constraint_dist = np.tile([r0, r0, 2 * r0 * math.sin(th / 2)], n_mol)
+    return c
+
+
+def test_trajectory_shake_bitwise_vs_reference(oracle, ref):
+    """SimulationEngine::step with constraints (SHAKE after the drift, RATTLE
+    after the second half kick): the oracle engine's REF profile against the
+    reference's own classes, bit for bit."""
+    c = _rigid(_small_water(n_mol=100), 1e-8)
+    c.coulomb_type = "cutoff"
+    c.thermostat.type = "berendsen"
+    c.dt = 0.001
+    re_ = ref.engine(c)
+    oe = oracle.engine(c, "ref")
+    for _ in range(3):
+        re_.step(4)
+        oe.step(4)
+        for w in (0, 1, 2):
+            assert np.array_equal(re_.get(w), oe.get(w)), w
+        assert re_.scalars()["pe"] == oe.scalars()["pe"]
+
+
+def test_phys_shake_keeps_constraints(oracle):
+    """PHYS profile: after every step the constrained distances hold to the
+    tolerance and the relative velocities along them vanish (RATTLE)."""
+    tol = 1e-10
+    c = _rigid(_small_water(n_mol=100), tol)
+    c.coulomb_type = "cutoff"
+    c.dt = 0.002
+    oe = oracle.engine(c, "phys")
+    ci, cj, d0 = np.asarray(c.constraint_i), np.asarray(c.constraint_j), np.asarray(c.constraint_dist)
+    L = c.box_size
+    for _ in range(5):
+        oe.step(2)
+        x, v = oe.get(0), oe.get(1)
+        d = x[cj] - x[ci]
+        d -= np.round(d / L) * L
+        assert np.abs((d ** 2).sum(1) - d0 ** 2).max() < 10 * tol
+        assert np.abs((d * (v[cj] - v[ci])).sum(1)).max() < 10 * tol
