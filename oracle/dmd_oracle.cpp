@@ -915,6 +915,8 @@ struct OrcEngine {
     orc_energy e{};
     bool have_forces{false};
     double pscale{1.0};  // phys: barostat scale chosen at the end of a step, applied with the next drift
+    double eps_dot{0.0};   // Andersen barostat: piston velocity (strain rate)
+    double piston_W{1.0};  // and piston mass
     std::vector<int> cons_i, cons_j;  // distance constraints, in the order they are swept
     std::vector<double> cons_d;
     double cons_tol{1e-6};
@@ -988,6 +990,11 @@ void* orc_engine_create(const orc_system* s, const orc_run* r) {
             double lam = std::sqrt(r->init_temperature / ta);
             for (int i = 0; i < n; ++i) { E->vx[i] *= lam; E->vy[i] *= lam; E->vz[i] *= lam; }
         }
+    }
+    {  // AndersenBarostat's piston mass (andersen_barostat.cpp:8-14)
+        double dof = 3.0 * static_cast<double>(n) - 3.0;
+        if (dof < 1.0) dof = 1.0;
+        E->piston_W = dof * KB * r->b_pressure * r->b_tau * r->b_tau;
     }
     if (r->n_cons > 0) {  // constraint_type "shake" with pairs (simulation_engine.cpp:294-300)
         cpi(E->cons_i, r->cons_i, r->n_cons);
@@ -1136,8 +1143,35 @@ void eng_thermostat(OrcEngine* E) {
     }
 }
 
+// AndersenBarostat::apply (andersen_barostat.cpp:20-45), REF profile: the
+// piston velocity takes half a step of 3V (P - P0) / W (P from the reference's
+// virial and kinetic energy, P0 as given: the reference's units), positions and
+// box scale by exp(eps_dot dt), then the second half step with the same forcing.
+void eng_andersen_barostat(OrcEngine* E) {
+    const orc_run& r = E->run;
+    const size_t n = E->m.size();
+    const double L = E->L;
+    const double volume = L * (L * L);
+    if (volume <= 0.0) return;
+    const double ek = kinetic(E);
+    double w = 0.0;
+    for (size_t i = 0; i < n; ++i)  // barostat.cpp:6-14
+        w += E->x[i] * E->fx[i] + E->y[i] * E->fy[i] + E->z[i] * E->fz[i];
+    const double P = (2.0 * ek + w) / (3.0 * volume);
+    const double forcing = 3.0 * volume * (P - r.b_pressure) / E->piston_W;
+    E->eps_dot = E->eps_dot + 0.5 * E->dt * forcing;
+    const double sc = std::exp(E->eps_dot * E->dt);
+    for (size_t i = 0; i < n; ++i) { E->x[i] *= sc; E->y[i] *= sc; E->z[i] *= sc; }
+    E->L *= sc;
+    E->eps_dot = E->eps_dot + 0.5 * E->dt * forcing;
+}
+
 void eng_barostat(OrcEngine* E) {  // berendsen_barostat.cpp:14-66
     const orc_run& r = E->run;
+    if (r.barostat == 2 && E->s.profile == 0) {
+        eng_andersen_barostat(E);
+        return;
+    }
     if (r.barostat != 1) return;
     if (r.b_tau <= 0.0) return;
     const size_t n = E->m.size();

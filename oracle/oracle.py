@@ -80,7 +80,7 @@ class orc_run(C.Structure):
 
 
 THERMO = {"none": 0, "berendsen": 1, "nose-hoover": 2, "andersen": 3}
-BARO = {"none": 0, "berendsen": 1}
+BARO = {"none": 0, "berendsen": 1, "andersen": 2}
 
 
 def pme_mesh(cfg) -> int:
@@ -313,6 +313,8 @@ class OracleEngine:
         r.thermostat = THERMO[cfg.thermostat.type]
         r.t_temp, r.t_tau, r.t_freq = cfg.thermostat.temperature, cfg.thermostat.tau, cfg.thermostat.frequency
         r.barostat = BARO[cfg.barostat.type]
+        if r.barostat == 2 and profile != "ref":
+            raise ValueError("the Andersen barostat is restated for the ref profile only")
         r.b_pressure, r.b_tau, r.b_compress = cfg.barostat.pressure, cfg.barostat.tau, cfg.barostat.compressibility
         r.rng_seed = rng_seed
         r.brute_list = int(bool(brute_list))

@@ -53,6 +53,7 @@
 #include "thermostat/andersen.h"
 #include "barostat/barostat.h"
 #include "barostat/berendsen_barostat.h"
+#include "barostat/andersen_barostat.h"
 #include "sim/checkpoint.h"
 #undef private
 
@@ -437,6 +438,11 @@ void* ref_engine_create(const ref_run_desc* d) {
         p.tau = d->b_tau;
         p.compressibility = d->b_compress;
         e->baro = std::make_unique<BerendsenBarostat>(p);
+    } else if (d->barostat == 2) {  // build_barostat (simulation_engine.cpp:239-243)
+        AndersenBarostatParams p;
+        p.pressure = d->b_pressure;
+        p.tau = d->b_tau;
+        e->baro = std::make_unique<AndersenBarostat>(p, static_cast<size_t>(n));
     }
     e->cell = Cell(d->box, d->box, d->box);
     e->dt = d->dt;

@@ -400,3 +400,28 @@ def test_phys_shake_keeps_constraints(oracle):
         d -= np.round(d / L) * L
         assert np.abs((d ** 2).sum(1) - d0 ** 2).max() < 10 * tol
         assert np.abs((d * (v[cj] - v[ci])).sum(1)).max() < 10 * tol
+
+
+@pytest.mark.parametrize("pressure", [1.0, 300.0])
+def test_trajectory_andersen_barostat_bitwise_vs_reference(oracle, ref, pressure):
+    """AndersenBarostat (piston velocity, exp(eps_dot dt) scaling of positions
+    and box) in the engine step: the oracle's REF restatement against the
+    reference's own class, bit for bit, box included."""
+    c = W.argon_fcc(n_cells=3, a=0.575, T=120.0, seed=11).config()
+    c.lj_cutoff = 0.8
+    c.thermostat.type = "berendsen"
+    c.thermostat.temperature = 100.0
+    c.barostat.type = "andersen"
+    c.barostat.pressure = pressure
+    c.barostat.tau = 0.5
+    re_ = ref.engine(c)
+    oe = oracle.engine(c, "ref")
+    box0 = c.box_size
+    for _ in range(3):
+        re_.step(7)
+        oe.step(7)
+        for w in (0, 1, 2):
+            assert np.array_equal(re_.get(w), oe.get(w)), w
+        rs, os_ = re_.scalars(), oe.scalars()
+        assert rs["box"] == os_["box"] and rs["pe"] == os_["pe"]
+    assert oe.scalars()["box"] != box0
