@@ -27,7 +27,7 @@ PROFILES = {"ref": 0, "phys": 1}
 PRECISIONS = {"mixed": 0, "fp64": 1}
 COULOMB = {"cutoff": 0, "direct": 0, "pme": 1}
 THERMO = {"none": 0, "berendsen": 1, "nose-hoover": 2, "andersen": 3}
-BARO = {"none": 0, "berendsen": 1}
+BARO = {"none": 0, "berendsen": 1, "andersen": 2}
 E_TERMS = ("lj", "coul_real", "coul_recip", "coul_self", "coul_excl", "bond", "angle", "dihedral",
            "improper")
 

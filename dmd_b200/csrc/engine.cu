@@ -205,6 +205,7 @@ int Batch::build_host(HostRep& hr, unsigned mask) {
     R.b_pressure = s.b_pressure;
     R.b_tau = s.b_tau;
     R.b_compress = s.b_compress;
+    R.piston_W = dof * KB * s.b_pressure * s.b_tau * s.b_tau;  // andersen_barostat.cpp:8-14
     R.n_types = std::max(s.n_types, 1);
     sort_grid(n, s.box, R.nvx, R.nvz);
     if (s.coulomb_type == 1) {
@@ -255,8 +256,10 @@ int Batch::add(const dmdgpu_system& in, long long n_steps, unsigned comp_mask, i
         return fail(DMDGPU_ERR_PARM, "SHAKE/RATTLE constraints are not supported on this path");
     if (in.thermostat_type < 0 || in.thermostat_type > 3)
         return fail(DMDGPU_ERR_PARM, "Unknown thermostat type");
-    if (in.barostat_type < 0 || in.barostat_type > 1)
+    if (in.barostat_type < 0 || in.barostat_type > 2)
         return fail(DMDGPU_ERR_PARM, "Unknown barostat type");
+    if (in.barostat_type == DMDGPU_BARO_ANDERSEN && phys_)
+        return fail(DMDGPU_ERR_PARM, "the Andersen barostat runs in the ref profile only");
     if (in.n_atoms >= (1 << 26)) return fail(DMDGPU_ERR_PARM, "more than 2^26 atoms in one system");
     auto hr = std::make_unique<HostRep>();
     HostSystem& s = hr->sys;
@@ -1613,8 +1616,9 @@ int Batch::save_checkpoint(int slot, const char* path) {
     // trailer: box, Nose-Hoover zeta, Andersen call counter, profile, (v3) the
     // PHYS barostat scale still to be applied with the next drift, (v4) the
     // frame of the last list build (box edge, build count, positions) and the
-    // pending-rebuild flag, so a restart rebuilds the very same list
-    uint32_t tv = 4;
+    // pending-rebuild flag, so a restart rebuilds the very same list, (v5) the
+    // Andersen barostat's piston velocity
+    uint32_t tv = 5;
     double box = sc.box, zeta = sc.zeta;
     int k = replica_index(slot);
     int64_t acalls = h_st_[k].andersen_calls;
@@ -1643,6 +1647,8 @@ int Batch::save_checkpoint(int slot, const char* path) {
             CK(cudaMemcpy(f.data(), src + a0, 8 * n, cudaMemcpyDeviceToHost));
             os.write(reinterpret_cast<const char*>(f.data()), 8 * n);
         }
+        const double ed = st.eps_dot;
+        os.write(reinterpret_cast<const char*>(&ed), 8);
     }
     return os.good() ? DMDGPU_OK : fail(DMDGPU_ERR_PARM, "checkpoint write failed");
 }
@@ -1713,6 +1719,8 @@ int Batch::load_checkpoint(int slot, const char* path) {
         }
         framed = static_cast<bool>(is) && lbuild > 0.0;
     }
+    double eps_dot = 0.0;  // v5
+    if (trailer && tv >= 5 && !is.read(reinterpret_cast<char*>(&eps_dot), 8)) eps_dot = 0.0;
     const int k = replica_index(slot);
     const int a0 = h.rep.atom_begin;
     CK(cudaStreamSynchronize(stream_));
@@ -1738,6 +1746,7 @@ int Batch::load_checkpoint(int slot, const char* path) {
         st.andersen_calls = acalls;
         h.andersen_seed = aseed;
         st.pscale = phys_ ? pscale : 1.0;
+        st.eps_dot = eps_dot;
     }
     if (framed) {
         // the saved list frame: the list is rebuilt as it was, not at the loaded positions

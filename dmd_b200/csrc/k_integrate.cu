@@ -374,6 +374,19 @@ __global__ void k_replica_update(Dev d) {
     else W = w;
     s->virial = W;
     s->pressure = (V <= 0.0) ? 0.0 : (2.0 * ke_after + W) / (3.0 * V);
+    if (R.barostat == 2 && V > 0.0) {
+        // AndersenBarostat::apply (andersen_barostat.cpp:20-45), ref profile: half a
+        // step of piston velocity from 3V (P - P0) / W (P0 in the reference's units),
+        // positions and box scale by exp(eps_dot dt) (positions in k_apply_scale),
+        // then the second half step with the same forcing
+        const double forcing = 3.0 * V * (s->pressure - R.b_pressure) / R.piston_W;
+        s->eps_dot = s->eps_dot + 0.5 * dt * forcing;
+        const double sc = exp(s->eps_dot * dt);
+        s->pscale = sc;
+        s->L = L * sc;
+        s->invL = 1.0 / s->L;
+        s->eps_dot = s->eps_dot + 0.5 * dt * forcing;
+    }
     if (R.barostat == 1 && R.b_tau > 0.0 && V > 0.0) {
         double mu;
         if (R.flags & F_PHYS) mu = 1.0 - (dt / R.b_tau) * R.b_compress * (R.b_pressure - s->pressure / BAR);

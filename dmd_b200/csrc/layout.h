@@ -64,6 +64,7 @@ struct Rep {
     double dt;
     double t_temp, t_tau, t_freq, nh_Q;
     double b_pressure, b_tau, b_compress;
+    double piston_W;                     // Andersen barostat piston mass
     double e_self;
     uint32_t key0, key1;                 // Andersen (phys) Philox key
 };
@@ -82,6 +83,7 @@ struct RepState {
     double zeta;
     double vscale;        // pending thermostat velocity scale (applied in the next kick)
     double pscale;        // pending barostat position scale
+    double eps_dot;       // Andersen barostat piston velocity (strain rate)
     double ke, pressure, virial;
     double e_recip, vir_recip;
     double time;

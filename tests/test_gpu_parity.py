@@ -242,6 +242,58 @@ def test_checkpoint_restart_bitwise(tmp_path):
     assert np.array_equal(full.velocities, fresh.velocities)
 
 
+def _argon_andersen_npt(nc=4, seed=5):
+    cfg = W.argon_fcc(n_cells=nc, a=0.575, T=120.0, seed=seed).config()
+    cfg.thermostat.type = "berendsen"
+    cfg.thermostat.temperature = 100.0
+    cfg.barostat.type = "andersen"
+    cfg.barostat.pressure = 300.0
+    cfg.barostat.tau = 0.5
+    return cfg
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_argon_andersen_barostat_ref(oracle, precision):
+    """REF NPT with the Andersen barostat: positions, velocities and the box
+    follow the FP64 oracle, whose restatement is pinned bit for bit to the
+    reference's AndersenBarostat."""
+    cfg = _argon_andersen_npt()
+    oe = oracle.engine(cfg, "ref")
+    eng = _engine(cfg, precision, "ref")
+    tol = {"fp64": 1e-9, "mixed": 2e-5}[precision]
+    for k in range(4):
+        oe.step(6)
+        eng.run_n(6)
+        L = oe.scalars()["box"]
+        assert abs(eng.scalars().box - L) <= tol * L, (k, eng.scalars().box, L)
+        assert np.abs(eng.positions - oe.get(0)).max() / L < tol, k
+        assert rel_rms(eng.velocities, oe.get(1)) < tol, k
+    assert oe.scalars()["box"] != cfg.box_size
+
+
+def test_andersen_barostat_phys_rejected():
+    cfg = _argon_andersen_npt(nc=2)
+    with pytest.raises(Exception, match="Andersen barostat"):
+        _engine(cfg, "fp64", "phys")
+
+
+def test_checkpoint_restart_bitwise_andersen_barostat(tmp_path):
+    """The piston velocity travels in the checkpoint: N steps == N/2 + save/load + N/2."""
+    cfg = _argon_andersen_npt(nc=3, seed=8)
+    full = _engine(cfg, "fp64", "ref")
+    full.run_n(40)
+    half = _engine(cfg, "fp64", "ref")
+    half.run_n(20)
+    p = str(tmp_path / "ck.bin")
+    half.save_checkpoint(p)
+    fresh = _engine(cfg, "fp64", "ref")
+    fresh.load_checkpoint(p)
+    fresh.run_n(20)
+    assert np.array_equal(full.positions, fresh.positions)
+    assert np.array_equal(full.velocities, fresh.velocities)
+    assert full.scalars().box == fresh.scalars().box
+
+
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_checkpoint_restart_bitwise_phys_npt(tmp_path, precision):
     """PHYS NPT: N steps == N/2 + save/load + N/2, bit for bit.  The trailer
