@@ -180,8 +180,8 @@ int dmdgpu_pair_list(dmdgpu_ctx *ctx, int32_t *pi, int32_t *pj, int64_t cap, int
 
 /* Binary checkpoint v1 (src/sim/checkpoint.cpp:9-75) plus a trailer the v1
  * reader ignores (box, Nose-Hoover zeta, thermostat call counter, profile, the
- * pending PHYS barostat scale, and the frame of the last pair-list build: its
- * box edge and positions).  A restart rebuilds the list in that frame, so N
+ * pending PHYS barostat scale, the frame of the last pair-list build: its
+ * box edge and positions, and the Andersen barostat's piston velocity).  A restart rebuilds the list in that frame, so N
  * steps equal N/2 + save/load + N/2 bit for bit in both profiles and both
  * precisions.  Replaces SimulationEngine::save_checkpoint / load_checkpoint
  * (:108-137). */
