@@ -60,6 +60,8 @@ class dmdgpu_system(C.Structure):
         ("baro_compressibility", C.c_double),
         ("constraint_type", C.c_int32), ("checkpoint_interval", C.c_int32),
         ("checkpoint_path", C.c_char_p),
+        ("n_constraints", C.c_int32), ("constraint_i", _ip), ("constraint_j", _ip),
+        ("constraint_dist", _dp), ("constraint_tolerance", C.c_double),
     ]
 
 
@@ -239,6 +241,12 @@ class SystemDesc:
         s.barostat_type = BARO[b.type]
         s.baro_pressure, s.baro_tau, s.baro_compressibility = b.pressure, b.tau, b.compressibility
         s.constraint_type = 0 if cfg.constraint_type == "none" or not len(cfg.constraint_i) else 1
+        if s.constraint_type:
+            nc = len(cfg.constraint_i)
+            s.n_constraints = nc
+            s.constraint_i, s.constraint_j = i(cfg.constraint_i, nc), i(cfg.constraint_j, nc)
+            s.constraint_dist = d(cfg.constraint_dist, nc)
+            s.constraint_tolerance = float(cfg.constraint_tolerance)
         s.checkpoint_interval = int(cfg.checkpoint_interval)
         p = (cfg.checkpoint_path or "").encode()
         keep.append(p)

@@ -206,6 +206,7 @@ int Batch::build_host(HostRep& hr, unsigned mask) {
     R.b_tau = s.b_tau;
     R.b_compress = s.b_compress;
     R.piston_W = dof * KB * s.b_pressure * s.b_tau * s.b_tau;  // andersen_barostat.cpp:8-14
+    R.cons_tol = s.ctol;
     R.n_types = std::max(s.n_types, 1);
     sort_grid(n, s.box, R.nvx, R.nvz);
     if (s.coulomb_type == 1) {
@@ -239,6 +240,7 @@ long long Batch::footprint(const HostSystem& s) const {
     long long chunks = tiles * 64;
     (void)rho;
     long long b = n * per_atom + tiles * 32 * per_slot + chunks * (4 + 32 * 8) + tiles * 64;
+    b += static_cast<long long>(s.ci.size()) * (8 + 8 + 8);  // constraints and their groups
     if (s.coulomb_type == 1) {
         long long K = std::max(8, static_cast<int>(s.box / s.spacing + 0.5));
         b += K * K * (K + 2) * 8 + K * K * K * 8 + K * K * (K / 2 + 1) * 16 + 3 * K * K * K * 8;
@@ -252,8 +254,12 @@ int Batch::add(const dmdgpu_system& in, long long n_steps, unsigned comp_mask, i
     if (!(in.box_size > 0)) return fail(DMDGPU_ERR_PARM, "box_size must be positive");
     if (!in.masses || !in.pos_x || !in.pos_y || !in.pos_z)
         return fail(DMDGPU_ERR_PARM, "masses and positions are required");
-    if (in.constraint_type != 0)
-        return fail(DMDGPU_ERR_PARM, "SHAKE/RATTLE constraints are not supported on this path");
+    if (in.constraint_type < 0 || in.constraint_type > 1)
+        return fail(DMDGPU_ERR_PARM, "Unknown constraint type");
+    if (in.constraint_type == 1 && phys_)
+        return fail(DMDGPU_ERR_PARM, "SHAKE/RATTLE constraints run in the ref profile only");
+    if (in.constraint_type == 1 && in.thermostat_type == DMDGPU_THERMO_ANDERSEN)
+        return fail(DMDGPU_ERR_PARM, "SHAKE/RATTLE constraints with the Andersen thermostat are not supported");
     if (in.thermostat_type < 0 || in.thermostat_type > 3)
         return fail(DMDGPU_ERR_PARM, "Unknown thermostat type");
     if (in.barostat_type < 0 || in.barostat_type > 2)
@@ -342,6 +348,17 @@ int Batch::add(const dmdgpu_system& in, long long n_steps, unsigned comp_mask, i
             return fail(DMDGPU_ERR_PARM, "exclusion index out of range");
         s.ei = vec_of(in.excl_i, in.n_excl);
         s.ej = vec_of(in.excl_j, in.n_excl);
+    }
+    if (in.constraint_type == 1 && in.n_constraints > 0) {
+        const int m = in.n_constraints;
+        if (!in.constraint_i || !in.constraint_j || !in.constraint_dist)
+            return fail(DMDGPU_ERR_PARM, "constraint arrays missing");
+        if (!check_idx(in.constraint_i, m) || !check_idx(in.constraint_j, m))
+            return fail(DMDGPU_ERR_PARM, "constraint index out of range");
+        s.ci = vec_of(in.constraint_i, m);
+        s.cj = vec_of(in.constraint_j, m);
+        s.cd = vec_of(in.constraint_dist, m);
+        s.ctol = in.constraint_tolerance;
     }
     s.coulomb_type = in.coulomb_type;
     s.coul_cutoff = in.coulomb_cutoff;
@@ -651,6 +668,9 @@ int Batch::pack() {
         std::vector<double2> ikp;
         std::vector<int2> ex;
         std::vector<std::vector<int>> exl(n_atoms);
+        std::vector<int2> cij;              // constraints grouped by connected atom set
+        std::vector<double> cdist;
+        std::vector<int> cgb(1, 0), cgr;    // group begin offsets, group replica
         std::vector<double> bsp(std::max<long long>(n_bsp, 1));
         std::vector<int> pbr(std::max(pme_blocks, 1));
         std::vector<int> cbr(std::max(conv_blocks, 1));
@@ -719,6 +739,41 @@ int Batch::pack() {
             for (size_t t = 0; t < s.ii.size(); ++t) {
                 iijkl.push_back(make_int4(a0 + s.ii[t], a0 + s.ij[t], a0 + s.ik[t], a0 + s.il[t]));
                 ikp.push_back(make_double2(s.ikp[t], s.ip0[t]));
+            }
+            if (!s.ci.empty()) {
+                // connected atom sets of the constraint graph (union-find); groups in
+                // order of their first constraint, each group's constraints in the
+                // order given: sweeping every group on its own reproduces the
+                // reference's Gauss-Seidel sweeps over all constraints, which never
+                // couple two groups
+                std::vector<int> root(s.n);
+                for (int i = 0; i < s.n; ++i) root[i] = i;
+                auto find = [&](int v) {
+                    while (root[v] != v) v = root[v] = root[root[v]];
+                    return v;
+                };
+                for (size_t t = 0; t < s.ci.size(); ++t) {
+                    const int ra = find(s.ci[t]), rb = find(s.cj[t]);
+                    if (ra != rb) root[std::max(ra, rb)] = std::min(ra, rb);
+                }
+                std::vector<int> gid(s.n, -1);
+                std::vector<std::vector<int>> members;
+                for (size_t t = 0; t < s.ci.size(); ++t) {
+                    const int g0 = find(s.ci[t]);
+                    if (gid[g0] < 0) {
+                        gid[g0] = static_cast<int>(members.size());
+                        members.emplace_back();
+                    }
+                    members[gid[g0]].push_back(static_cast<int>(t));
+                }
+                for (const auto& mem : members) {
+                    for (int t : mem) {
+                        cij.push_back(make_int2(a0 + s.ci[t], a0 + s.cj[t]));
+                        cdist.push_back(s.cd[t]);
+                    }
+                    cgb.push_back(static_cast<int>(cij.size()));
+                    cgr.push_back(k);
+                }
             }
             for (size_t t = 0; t < s.ei.size(); ++t) {
                 const int gi = a0 + s.ei[t], gj = a0 + s.ej[t];
@@ -826,6 +881,22 @@ int Batch::pack() {
         d.excl = dex;
         d.ex_start = dexs;
         d.ex_list = dexl;
+        d.n_cgroups = static_cast<int>(cgr.size());
+        any_cons_ = d.n_cgroups > 0;
+        if (any_cons_) {
+            int* dcgb = A.alloc<int>(cgb.size());
+            int* dcgr = A.alloc<int>(cgr.size());
+            int2* dcij = A.alloc<int2>(cij.size());
+            double* dcd = A.alloc<double>(cdist.size());
+            up(dcgb, cgb.data(), sizeof(int) * cgb.size());
+            up(dcgr, cgr.data(), sizeof(int) * cgr.size());
+            up(dcij, cij.data(), sizeof(int2) * cij.size());
+            up(dcd, cdist.data(), sizeof(double) * cdist.size());
+            d.cgroup_begin = dcgb;
+            d.cgroup_rep = dcgr;
+            d.cons_ij = dcij;
+            d.cons_d = dcd;
+        }
         if (any_pme_) {
             d.mesh_fix = A.alloc<long long>(mesh_fix);
             if (fp64_) {
@@ -992,8 +1063,10 @@ void Batch::enqueue_step() {
     // exist yet; only then is it issued (its kernels skip replicas that do not need it).
     if (need_eval1_) enqueue_eval(PASS_FIRST);
     launch_kick_drift(dev_, fp64_, stream_, &launches_);
+    if (any_cons_) launch_shake(dev_, stream_, &launches_);
     enqueue_eval(PASS_SECOND);
     launch_kick2(dev_, any_andersen_ref_, any_andersen_phys_, stream_, &launches_);
+    if (any_cons_) launch_rattle(dev_, stream_, &launches_);
     launch_replica_update(dev_, stream_, &launches_);
     if (any_baro_ && !phys_) launch_apply_scale(dev_, fp64_, stream_, &launches_);
 }

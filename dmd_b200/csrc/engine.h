@@ -38,6 +38,9 @@ struct HostSystem {
     std::vector<int> ii, ij, ik, il;
     std::vector<double> ikp, ip0;
     std::vector<int> ei, ej;
+    std::vector<int> ci, cj;              // distance constraints (SHAKE / RATTLE), in sweep order
+    std::vector<double> cd;
+    double ctol = 1e-6;
     int coulomb_type = 0;
     double coul_cutoff = 1.2, ewald = 0.34, spacing = 0.12;
     int pme_order = 4, pme_K = 0;
@@ -140,6 +143,7 @@ class Batch {
     long long* h_tgt_ = nullptr;                    // pinned step targets for extend_targets
     int* d_bin_rep_ = nullptr;
     int n_pme_blocks_ = 0, n_conv_blocks_ = 0;
+    bool any_cons_ = false;  // some replica has distance constraints
     bool any_pme_ = false, any_baro_ = false, any_ref_lj_ = false, any_andersen_ref_ = false,
          any_andersen_phys_ = false;
     std::map<int, std::pair<cufftHandle, cufftHandle>> plans_;

@@ -259,6 +259,117 @@ __global__ void k_kick2(Dev d, int andersen_ref, int andersen_phys) {
     }
 }
 
+// Constraints::apply (src/integrate/constraints.cpp:9-47), REF profile, after
+// the drift: one thread per group of constraints that share atoms (a
+// molecule), its constraints swept in their given order until the group's
+// largest |r^2 - d^2| (measured before each correction) is below the
+// tolerance, at most 100 sweeps.  Groups share no atoms, so this is the
+// reference's Gauss-Seidel sweep over all constraints, group by group.  The
+// FP64 operations follow the reference's order; the moved atoms' mirror
+// entries are written again.
+__global__ void k_shake(Dev d) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= d.n_cgroups) return;
+    const int r = d.cgroup_rep[g];
+    RepState* s = d.st + r;
+    if (!(s->step < s->target_step)) return;  // the replicas k_kick_drift moved
+    const Rep& R = d.rep[r];
+    const double L = s->L, inv = 1.0 / L, tol = R.cons_tol;
+    const int c0 = d.cgroup_begin[g], c1 = d.cgroup_begin[g + 1];
+    for (int it = 0; it < 100; ++it) {
+        double worst = 0.0;
+        for (int c = c0; c < c1; ++c) {
+            const int a = d.cons_ij[c].x, b = d.cons_ij[c].y;
+            double dx = __dsub_rn(d.x[b], d.x[a]), dy = __dsub_rn(d.y[b], d.y[a]), dz = __dsub_rn(d.z[b], d.z[a]);
+            dx = __dsub_rn(dx, __dmul_rn(round(__dmul_rn(dx, inv)), L));
+            dy = __dsub_rn(dy, __dmul_rn(round(__dmul_rn(dy, inv)), L));
+            dz = __dsub_rn(dz, __dmul_rn(round(__dmul_rn(dz, inv)), L));
+            const double r2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+            const double d2 = __dmul_rn(d.cons_d[c], d.cons_d[c]);
+            const double err = __dsub_rn(r2, d2);
+            if (fabs(err) > worst) worst = fabs(err);
+            if (fabs(err) > tol) {
+                const double wa = 1.0 / d.mass[a], wb = 1.0 / d.mass[b];
+                const double lam = err / __dmul_rn(__dmul_rn(2.0, d2), __dadd_rn(wa, wb));
+                d.x[a] = __dadd_rn(d.x[a], __dmul_rn(__dmul_rn(lam, dx), wa));
+                d.y[a] = __dadd_rn(d.y[a], __dmul_rn(__dmul_rn(lam, dy), wa));
+                d.z[a] = __dadd_rn(d.z[a], __dmul_rn(__dmul_rn(lam, dz), wa));
+                d.x[b] = __dsub_rn(d.x[b], __dmul_rn(__dmul_rn(lam, dx), wb));
+                d.y[b] = __dsub_rn(d.y[b], __dmul_rn(__dmul_rn(lam, dy), wb));
+                d.z[b] = __dsub_rn(d.z[b], __dmul_rn(__dmul_rn(lam, dz), wb));
+            }
+        }
+        if (worst < tol) break;
+    }
+    for (int c = c0; c < c1; ++c) {
+        const int ab[2] = {d.cons_ij[c].x, d.cons_ij[c].y};
+        for (int a : ab) {
+            write_mirror(d, d.slot_of_atom[a], a, d.x[a], d.y[a], d.z[a], L);
+            skin_check(d, s, R, a, d.x[a], d.y[a], d.z[a]);
+        }
+    }
+}
+
+// Constraints::apply_rattle (constraints.cpp:49-91), after the second half
+// kick: the same group sweeps on r.v, lambda = r.v / (r^2 (1/m_i + 1/m_j)).
+__global__ void k_rattle(Dev d) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= d.n_cgroups) return;
+    const int r = d.cgroup_rep[g];
+    RepState* s = d.st + r;
+    if (!s->active) return;
+    const Rep& R = d.rep[r];
+    const double L = s->L, inv = 1.0 / L, tol = R.cons_tol;
+    const int c0 = d.cgroup_begin[g], c1 = d.cgroup_begin[g + 1];
+    for (int it = 0; it < 100; ++it) {
+        double worst = 0.0;
+        for (int c = c0; c < c1; ++c) {
+            const int a = d.cons_ij[c].x, b = d.cons_ij[c].y;
+            double dx = __dsub_rn(d.x[b], d.x[a]), dy = __dsub_rn(d.y[b], d.y[a]), dz = __dsub_rn(d.z[b], d.z[a]);
+            dx = __dsub_rn(dx, __dmul_rn(round(__dmul_rn(dx, inv)), L));
+            dy = __dsub_rn(dy, __dmul_rn(round(__dmul_rn(dy, inv)), L));
+            dz = __dsub_rn(dz, __dmul_rn(round(__dmul_rn(dz, inv)), L));
+            const double dvx = __dsub_rn(d.vx[b], d.vx[a]), dvy = __dsub_rn(d.vy[b], d.vy[a]),
+                         dvz = __dsub_rn(d.vz[b], d.vz[a]);
+            const double rv = __dadd_rn(__dadd_rn(__dmul_rn(dx, dvx), __dmul_rn(dy, dvy)), __dmul_rn(dz, dvz));
+            const double r2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+            const double e = fabs(rv);
+            if (e > worst) worst = e;
+            if (e > tol) {
+                const double wa = 1.0 / d.mass[a], wb = 1.0 / d.mass[b];
+                const double lam = rv / __dmul_rn(r2, __dadd_rn(wa, wb));
+                d.vx[a] = __dadd_rn(d.vx[a], __dmul_rn(__dmul_rn(lam, dx), wa));
+                d.vy[a] = __dadd_rn(d.vy[a], __dmul_rn(__dmul_rn(lam, dy), wa));
+                d.vz[a] = __dadd_rn(d.vz[a], __dmul_rn(__dmul_rn(lam, dz), wa));
+                d.vx[b] = __dsub_rn(d.vx[b], __dmul_rn(__dmul_rn(lam, dx), wb));
+                d.vy[b] = __dsub_rn(d.vy[b], __dmul_rn(__dmul_rn(lam, dy), wb));
+                d.vz[b] = __dsub_rn(d.vz[b], __dmul_rn(__dmul_rn(lam, dz), wb));
+            }
+        }
+        if (worst < tol) break;
+    }
+}
+
+// Per-tile kinetic-energy partials again after RATTLE (the thermostat reads the
+// constrained velocities; same expression and order as k_kick2's).
+__global__ void k_tile_ke(Dev d) {
+    const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    const int t = slot >> 5;
+    const int r = (t < d.n_tiles) ? d.tile_rep[t] : 0;
+    double ke = 0.0;
+    if (slot < d.n_slots && d.st[r].active) {
+        const int a = d.atom_of_slot[slot];
+        if (a >= 0) {
+            const double m = d.mass[a], vx = d.vx[a], vy = d.vy[a], vz = d.vz[a];
+            ke = __dmul_rn(__dmul_rn(0.5, m),
+                           __dadd_rn(__dadd_rn(__dmul_rn(vx, vx), __dmul_rn(vy, vy)), __dmul_rn(vz, vz)));
+        }
+    }
+    ke = warp_sum_d(ke);
+    if (lane == 0 && t < d.n_tiles) d.tile_ke[t] = ke;
+}
+
 __device__ double block_sum(double v, double* sh) {
     sh[threadIdx.x] = v;
     __syncthreads();
@@ -467,6 +578,15 @@ void launch_kick_drift(const Dev& d, bool, cudaStream_t st, long long* n) {
 void launch_kick2(const Dev& d, bool andersen_ref, bool andersen_phys, cudaStream_t st, long long* n) {
     k_kick2<<<(d.n_slots + 255) / 256, 256, 0, st>>>(d, andersen_ref ? 1 : 0, andersen_phys ? 1 : 0);
     ++*n;
+}
+void launch_shake(const Dev& d, cudaStream_t st, long long* n) {
+    k_shake<<<(d.n_cgroups + 127) / 128, 128, 0, st>>>(d);
+    ++*n;
+}
+void launch_rattle(const Dev& d, cudaStream_t st, long long* n) {
+    k_rattle<<<(d.n_cgroups + 127) / 128, 128, 0, st>>>(d);
+    k_tile_ke<<<(d.n_slots + 255) / 256, 256, 0, st>>>(d);
+    *n += 2;
 }
 void launch_replica_update(const Dev& d, cudaStream_t st, long long* n) {
     k_replica_update<<<d.n_rep, 256, 0, st>>>(d);

@@ -36,6 +36,8 @@ void launch_eval_end(const Dev& d, cudaStream_t st, long long* nlaunch);
 void launch_kick_drift(const Dev& d, bool fp64, cudaStream_t st, long long* nlaunch);
 void launch_kick2(const Dev& d, bool andersen_ref, bool andersen_phys, cudaStream_t st,
                   long long* nlaunch);
+void launch_shake(const Dev& d, cudaStream_t st, long long* nlaunch);
+void launch_rattle(const Dev& d, cudaStream_t st, long long* nlaunch);
 void launch_replica_update(const Dev& d, cudaStream_t st, long long* nlaunch);
 void launch_apply_scale(const Dev& d, bool fp64, cudaStream_t st, long long* nlaunch);
 void launch_finalize_velocities(const Dev& d, cudaStream_t st, long long* nlaunch);

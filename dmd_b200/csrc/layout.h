@@ -65,6 +65,7 @@ struct Rep {
     double t_temp, t_tau, t_freq, nh_Q;
     double b_pressure, b_tau, b_compress;
     double piston_W;                     // Andersen barostat piston mass
+    double cons_tol;                     // constraint tolerance (SHAKE on r^2 - d^2, RATTLE on r.v)
     double e_self;
     uint32_t key0, key1;                 // Andersen (phys) Philox key
 };
@@ -159,6 +160,13 @@ struct Dev {
     const double2* dih_kp;
     const int4* imp_ijkl;
     const double2* imp_kp;             // (k, chi0)
+    // distance constraints, grouped by connected atom set (a molecule), each
+    // group's constraints in their sweep order (global atom indices)
+    int n_cgroups;
+    const int* cgroup_begin;           // [n_cgroups + 1] into cons_ij / cons_d
+    const int* cgroup_rep;
+    const int2* cons_ij;
+    const double* cons_d;              // target distance
     // LJ tables per type pair
     const double2* lj64;               // (eps, sig^6)
     const float4* lj32;                // (c6, c12, 6 c6, 12 c12), c6 = 4 eps sig^6, c12 = 4 eps sig^12

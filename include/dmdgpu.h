@@ -41,7 +41,9 @@ enum { DMDGPU_COULOMB_CUTOFF = 0, /* "cutoff" / "direct" */ DMDGPU_COULOMB_PME =
 /* ThermostatConfig::type (src/sim/simulation_config.h:11-16) */
 enum { DMDGPU_THERMO_NONE = 0, DMDGPU_THERMO_BERENDSEN = 1, DMDGPU_THERMO_NOSE_HOOVER = 2,
        DMDGPU_THERMO_ANDERSEN = 3 };
-/* BarostatConfig::type (src/sim/simulation_config.h:18-23); "andersen"
+/* Constraints (src/integrate/constraints.cpp:9-91): SHAKE after the drift,
+ * RATTLE after the second half kick, REF profile, not with the Andersen
+ * thermostat.  BarostatConfig::type (src/sim/simulation_config.h:18-23); "andersen"
  * (src/barostat/andersen_barostat.cpp:8-45) runs in the REF profile only */
 enum { DMDGPU_BARO_NONE = 0, DMDGPU_BARO_BERENDSEN = 1, DMDGPU_BARO_ANDERSEN = 2 };
 /* Semantic profile: REF reproduces the reference's formulas (quirks included);
@@ -99,9 +101,15 @@ typedef struct dmdgpu_system {
     double thermo_temperature, thermo_tau, thermo_frequency;
     int32_t barostat_type;
     double baro_pressure, baro_tau, baro_compressibility;
-    int32_t constraint_type; /* must be 0 ("none"): SHAKE/RATTLE are not on this path */
+    int32_t constraint_type; /* 0 "none", 1 "shake" (SHAKE + RATTLE, REF profile only) */
     int32_t checkpoint_interval;
     const char *checkpoint_path; /* may be NULL */
+    /* distance constraints (ConstraintsParams, src/integrate/constraints.h:8-12),
+     * used when constraint_type is 1 */
+    int32_t n_constraints;
+    const int32_t *constraint_i, *constraint_j;
+    const double *constraint_dist;
+    double constraint_tolerance;
 } dmdgpu_system;
 
 typedef struct dmdgpu_options {

@@ -242,6 +242,53 @@ def test_checkpoint_restart_bitwise(tmp_path):
     assert np.array_equal(full.velocities, fresh.velocities)
 
 
+def _rigid_water(n_mol=100, tol=1e-8):
+    """Rigid 3-site water: O-H1, O-H2 and H1-H2 distance constraints."""
+    c = W.water_box(n_mol=n_mol, box=(n_mol / 33.4) ** (1 / 3), seed=3, spacing=0.1).config()
+    mol = np.arange(n_mol) * 3
+    r0, th = 0.09572, math.radians(104.52)
+    c.constraint_type = "shake"
+    c.constraint_tolerance = tol
+    c.constraint_i = np.stack([mol, mol, mol + 1], 1).reshape(-1).astype(np.int32)
+    c.constraint_j = np.stack([mol + 1, mol + 2, mol + 2], 1).reshape(-1).astype(np.int32)
+    c.constraint_dist = np.tile([r0, r0, 2 * r0 * math.sin(th / 2)], n_mol)
+    c.coulomb_type = "cutoff"
+    c.thermostat.type = "berendsen"
+    c.dt = 0.001
+    return c
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_water_shake_rattle_trajectory_ref(oracle, precision):
+    """REF rigid water: SHAKE after the drift and RATTLE after the second half
+    kick on the GPU (one thread per molecule) follow the FP64 oracle, whose
+    engine is pinned bit for bit to the reference's Constraints."""
+    c = _rigid_water()
+    oe = oracle.engine(c, "ref")
+    eng = _engine(c, precision, "ref")
+    tol = {"fp64": 1e-8, "mixed": 1e-4}[precision]
+    ci, cj, d0 = np.asarray(c.constraint_i), np.asarray(c.constraint_j), np.asarray(c.constraint_dist)
+    L = c.box_size
+    for k in range(3):
+        oe.step(4)
+        eng.run_n(4)
+        x, v = eng.positions, eng.velocities
+        assert np.abs(x - oe.get(0)).max() / L < tol, k
+        assert rel_rms(v, oe.get(1)) < tol, k
+        d = x[cj] - x[ci]
+        d -= np.round(d / L) * L
+        assert np.abs((d ** 2).sum(1) - d0 ** 2).max() < 1e-7, k
+
+
+def test_constraints_rejected_where_not_supported():
+    c = _rigid_water(n_mol=20)
+    with pytest.raises(Exception, match="ref profile only"):
+        _engine(c, "fp64", "phys")
+    c.thermostat.type = "andersen"
+    with pytest.raises(Exception, match="Andersen thermostat"):
+        _engine(c, "fp64", "ref")
+
+
 def _argon_andersen_npt(nc=4, seed=5):
     cfg = W.argon_fcc(n_cells=nc, a=0.575, T=120.0, seed=seed).config()
     cfg.thermostat.type = "berendsen"
