@@ -41,10 +41,11 @@ enum { DMDGPU_COULOMB_CUTOFF = 0, /* "cutoff" / "direct" */ DMDGPU_COULOMB_PME =
 /* ThermostatConfig::type (src/sim/simulation_config.h:11-16) */
 enum { DMDGPU_THERMO_NONE = 0, DMDGPU_THERMO_BERENDSEN = 1, DMDGPU_THERMO_NOSE_HOOVER = 2,
        DMDGPU_THERMO_ANDERSEN = 3 };
-/* Constraints (src/integrate/constraints.cpp:9-91): SHAKE after the drift,
- * RATTLE after the second half kick, REF profile, not with the Andersen
- * thermostat.  BarostatConfig::type (src/sim/simulation_config.h:18-23); "andersen"
- * (src/barostat/andersen_barostat.cpp:8-45) runs in the REF profile only */
+/* BarostatConfig::type (src/sim/simulation_config.h:18-23); "andersen"
+ * (src/barostat/andersen_barostat.cpp:8-45) runs in the REF profile only.
+ * Constraints (constraint_type 1, src/integrate/constraints.cpp:9-91): SHAKE
+ * after the drift, RATTLE after the second half kick; REF profile, not with the
+ * Andersen thermostat. */
 enum { DMDGPU_BARO_NONE = 0, DMDGPU_BARO_BERENDSEN = 1, DMDGPU_BARO_ANDERSEN = 2 };
 /* Semantic profile: REF reproduces the reference's formulas (quirks included);
  * PHYS uses gradient-consistent forces (skin list, erfc real space with
