@@ -256,8 +256,6 @@ int Batch::add(const dmdgpu_system& in, long long n_steps, unsigned comp_mask, i
         return fail(DMDGPU_ERR_PARM, "masses and positions are required");
     if (in.constraint_type < 0 || in.constraint_type > 1)
         return fail(DMDGPU_ERR_PARM, "Unknown constraint type");
-    if (in.constraint_type == 1 && phys_)
-        return fail(DMDGPU_ERR_PARM, "SHAKE/RATTLE constraints run in the ref profile only");
     if (in.constraint_type == 1 && in.thermostat_type == DMDGPU_THERMO_ANDERSEN)
         return fail(DMDGPU_ERR_PARM, "SHAKE/RATTLE constraints with the Andersen thermostat are not supported");
     if (in.thermostat_type < 0 || in.thermostat_type > 3)
@@ -671,6 +669,7 @@ int Batch::pack() {
         std::vector<int2> cij;              // constraints grouped by connected atom set
         std::vector<double> cdist;
         std::vector<int> cgb(1, 0), cgr;    // group begin offsets, group replica
+        std::vector<int> cgab(1, 0), cga;   // each group's distinct atoms
         std::vector<double> bsp(std::max<long long>(n_bsp, 1));
         std::vector<int> pbr(std::max(pme_blocks, 1));
         std::vector<int> cbr(std::max(conv_blocks, 1));
@@ -766,12 +765,19 @@ int Batch::pack() {
                     }
                     members[gid[g0]].push_back(static_cast<int>(t));
                 }
+                std::vector<char> seen(s.n, 0);
                 for (const auto& mem : members) {
                     for (int t : mem) {
                         cij.push_back(make_int2(a0 + s.ci[t], a0 + s.cj[t]));
                         cdist.push_back(s.cd[t]);
+                        for (int a : {s.ci[t], s.cj[t]})
+                            if (!seen[a]) {
+                                seen[a] = 1;
+                                cga.push_back(a0 + a);
+                            }
                     }
                     cgb.push_back(static_cast<int>(cij.size()));
+                    cgab.push_back(static_cast<int>(cga.size()));
                     cgr.push_back(k);
                 }
             }
@@ -892,10 +898,17 @@ int Batch::pack() {
             up(dcgr, cgr.data(), sizeof(int) * cgr.size());
             up(dcij, cij.data(), sizeof(int2) * cij.size());
             up(dcd, cdist.data(), sizeof(double) * cdist.size());
+            int* dcgab = A.alloc<int>(cgab.size());
+            int* dcga = A.alloc<int>(cga.size());
+            up(dcgab, cgab.data(), sizeof(int) * cgab.size());
+            up(dcga, cga.data(), sizeof(int) * cga.size());
             d.cgroup_begin = dcgb;
             d.cgroup_rep = dcgr;
             d.cons_ij = dcij;
             d.cons_d = dcd;
+            d.cgroup_atom_begin = dcgab;
+            d.cgroup_atoms = dcga;
+            d.cons_x0 = A.alloc<double>(3 * static_cast<size_t>(n_atoms));
         }
         if (any_pme_) {
             d.mesh_fix = A.alloc<long long>(mesh_fix);

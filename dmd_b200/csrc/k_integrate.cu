@@ -259,14 +259,16 @@ __global__ void k_kick2(Dev d, int andersen_ref, int andersen_phys) {
     }
 }
 
-// Constraints::apply (src/integrate/constraints.cpp:9-47), REF profile, after
-// the drift: one thread per group of constraints that share atoms (a
-// molecule), its constraints swept in their given order until the group's
-// largest |r^2 - d^2| (measured before each correction) is below the
-// tolerance, at most 100 sweeps.  Groups share no atoms, so this is the
-// reference's Gauss-Seidel sweep over all constraints, group by group.  The
-// FP64 operations follow the reference's order; the moved atoms' mirror
-// entries are written again.
+// Constraints::apply (src/integrate/constraints.cpp:9-47) after the drift: one
+// thread per group of constraints that share atoms (a molecule), its
+// constraints swept in their given order until the group's largest
+// |r^2 - d^2| (measured before each correction) is below the tolerance, at
+// most 100 sweeps.  Groups share no atoms, so this is the reference's
+// Gauss-Seidel sweep over all constraints, group by group.  The FP64
+// operations follow the reference's order; the moved atoms' mirror entries
+// are written again.  PHYS: the box is the drifted frame's (L times the
+// pending barostat scale), and SHAKE's displacement is also given to the
+// half-step velocities (v += dx / dt).
 __global__ void k_shake(Dev d) {
     const int g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= d.n_cgroups) return;
@@ -274,8 +276,18 @@ __global__ void k_shake(Dev d) {
     RepState* s = d.st + r;
     if (!(s->step < s->target_step)) return;  // the replicas k_kick_drift moved
     const Rep& R = d.rep[r];
-    const double L = s->L, inv = 1.0 / L, tol = R.cons_tol;
+    const bool phys = (R.flags & F_PHYS) != 0;
+    const double L = phys ? s->L * s->pscale : s->L, inv = 1.0 / L, tol = R.cons_tol;
     const int c0 = d.cgroup_begin[g], c1 = d.cgroup_begin[g + 1];
+    const int q0 = d.cgroup_atom_begin[g], q1 = d.cgroup_atom_begin[g + 1];
+    const int na = d.n_atoms;
+    if (phys)
+        for (int q = q0; q < q1; ++q) {
+            const int a = d.cgroup_atoms[q];
+            d.cons_x0[a] = d.x[a];
+            d.cons_x0[na + a] = d.y[a];
+            d.cons_x0[2 * na + a] = d.z[a];
+        }
     for (int it = 0; it < 100; ++it) {
         double worst = 0.0;
         for (int c = c0; c < c1; ++c) {
@@ -301,12 +313,16 @@ __global__ void k_shake(Dev d) {
         }
         if (worst < tol) break;
     }
-    for (int c = c0; c < c1; ++c) {
-        const int ab[2] = {d.cons_ij[c].x, d.cons_ij[c].y};
-        for (int a : ab) {
-            write_mirror(d, d.slot_of_atom[a], a, d.x[a], d.y[a], d.z[a], L);
-            skin_check(d, s, R, a, d.x[a], d.y[a], d.z[a]);
+    for (int q = q0; q < q1; ++q) {
+        const int a = d.cgroup_atoms[q];
+        const double x = d.x[a], y = d.y[a], z = d.z[a];
+        if (phys) {
+            d.vx[a] = __dadd_rn(d.vx[a], __dsub_rn(x, d.cons_x0[a]) / R.dt);
+            d.vy[a] = __dadd_rn(d.vy[a], __dsub_rn(y, d.cons_x0[na + a]) / R.dt);
+            d.vz[a] = __dadd_rn(d.vz[a], __dsub_rn(z, d.cons_x0[2 * na + a]) / R.dt);
         }
+        write_mirror(d, d.slot_of_atom[a], a, x, y, z, L);
+        skin_check(d, s, R, a, x, y, z);
     }
 }
 

@@ -167,6 +167,9 @@ struct Dev {
     const int* cgroup_rep;
     const int2* cons_ij;
     const double* cons_d;              // target distance
+    const int* cgroup_atom_begin;      // [n_cgroups + 1] into cgroup_atoms
+    const int* cgroup_atoms;           // each group's distinct atoms
+    double* cons_x0;                   // [3][n_atoms] positions before SHAKE (PHYS)
     // LJ tables per type pair
     const double2* lj64;               // (eps, sig^6)
     const float4* lj32;                // (c6, c12, 6 c6, 12 c12), c6 = 4 eps sig^6, c12 = 4 eps sig^12

@@ -44,8 +44,8 @@ enum { DMDGPU_THERMO_NONE = 0, DMDGPU_THERMO_BERENDSEN = 1, DMDGPU_THERMO_NOSE_H
 /* BarostatConfig::type (src/sim/simulation_config.h:18-23); "andersen"
  * (src/barostat/andersen_barostat.cpp:8-45) runs in the REF profile only.
  * Constraints (constraint_type 1, src/integrate/constraints.cpp:9-91): SHAKE
- * after the drift, RATTLE after the second half kick; REF profile, not with the
- * Andersen thermostat. */
+ * after the drift, RATTLE after the second half kick (PHYS also gives SHAKE's
+ * displacement to the half-step velocities); not with the Andersen thermostat. */
 enum { DMDGPU_BARO_NONE = 0, DMDGPU_BARO_BERENDSEN = 1, DMDGPU_BARO_ANDERSEN = 2 };
 /* Semantic profile: REF reproduces the reference's formulas (quirks included);
  * PHYS uses gradient-consistent forces (skin list, erfc real space with
@@ -102,7 +102,7 @@ typedef struct dmdgpu_system {
     double thermo_temperature, thermo_tau, thermo_frequency;
     int32_t barostat_type;
     double baro_pressure, baro_tau, baro_compressibility;
-    int32_t constraint_type; /* 0 "none", 1 "shake" (SHAKE + RATTLE, REF profile only) */
+    int32_t constraint_type; /* 0 "none", 1 "shake" (SHAKE + RATTLE) */
     int32_t checkpoint_interval;
     const char *checkpoint_path; /* may be NULL */
     /* distance constraints (ConstraintsParams, src/integrate/constraints.h:8-12),

@@ -252,38 +252,40 @@ def _rigid_water(n_mol=100, tol=1e-8):
     c.constraint_i = np.stack([mol, mol, mol + 1], 1).reshape(-1).astype(np.int32)
     c.constraint_j = np.stack([mol + 1, mol + 2, mol + 2], 1).reshape(-1).astype(np.int32)
     c.constraint_dist = np.tile([r0, r0, 2 * r0 * math.sin(th / 2)], n_mol)
-    c.coulomb_type = "cutoff"
     c.thermostat.type = "berendsen"
     c.dt = 0.001
     return c
 
 
+@pytest.mark.parametrize("profile", ["ref", "phys"])
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
-def test_water_shake_rattle_trajectory_ref(oracle, precision):
-    """REF rigid water: SHAKE after the drift and RATTLE after the second half
-    kick on the GPU (one thread per molecule) follow the FP64 oracle, whose
-    engine is pinned bit for bit to the reference's Constraints."""
+def test_water_shake_rattle_trajectory(oracle, precision, profile):
+    """Rigid water: SHAKE after the drift and RATTLE after the second half kick
+    on the GPU (one thread per molecule) follow the FP64 oracle, whose REF
+    engine is pinned bit for bit to the reference's Constraints (PHYS also
+    gives SHAKE's displacement to the half-step velocities)."""
     c = _rigid_water()
-    oe = oracle.engine(c, "ref")
-    eng = _engine(c, precision, "ref")
-    tol = {"fp64": 1e-8, "mixed": 1e-4}[precision]
+    oe = oracle.engine(c, profile)
+    eng = _engine(c, precision, profile)
+    # positions (over the box edge) and velocities (relative RMS) against the oracle
+    tol_x, tol_v = {"fp64": (1e-8, 1e-8), "mixed": (1e-4, 1e-3)}[precision]
     ci, cj, d0 = np.asarray(c.constraint_i), np.asarray(c.constraint_j), np.asarray(c.constraint_dist)
     L = c.box_size
     for k in range(3):
         oe.step(4)
         eng.run_n(4)
         x, v = eng.positions, eng.velocities
-        assert np.abs(x - oe.get(0)).max() / L < tol, k
-        assert rel_rms(v, oe.get(1)) < tol, k
+        assert np.abs(x - oe.get(0)).max() / L < tol_x, k
+        assert rel_rms(v, oe.get(1)) < tol_v, k
         d = x[cj] - x[ci]
         d -= np.round(d / L) * L
         assert np.abs((d ** 2).sum(1) - d0 ** 2).max() < 1e-7, k
+        # RATTLE: no relative velocity along the constraints
+        assert np.abs((d * (v[cj] - v[ci])).sum(1)).max() < 1e-6, k
 
 
-def test_constraints_rejected_where_not_supported():
+def test_constraints_rejected_with_andersen_thermostat():
     c = _rigid_water(n_mol=20)
-    with pytest.raises(Exception, match="ref profile only"):
-        _engine(c, "fp64", "phys")
     c.thermostat.type = "andersen"
     with pytest.raises(Exception, match="Andersen thermostat"):
         _engine(c, "fp64", "ref")
