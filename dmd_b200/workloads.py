@@ -53,6 +53,9 @@ class Workload:
     imp_k: np.ndarray = field(default_factory=lambda: np.zeros(0))
     imp_phi0: np.ndarray = field(default_factory=lambda: np.zeros(0))
     exclusions: np.ndarray = field(default_factory=lambda: np.zeros((0, 2), np.int32))
+    constraints: np.ndarray = field(default_factory=lambda: np.zeros((0, 2), np.int32))
+    constraint_dist: np.ndarray = field(default_factory=lambda: np.zeros(0))
+    constraint_tol: float = 1e-6
 
     @property
     def n_atoms(self) -> int:
@@ -68,7 +71,8 @@ class Workload:
             "electrostatics": dict(self.electrostatics),
             "thermostat": dict(self.thermostat),
             "barostat": dict(self.barostat),
-            "constraints": {"type": "none", "tolerance": 1e-6},
+            "constraints": {"type": "shake" if len(self.constraints) else "none",
+                            "tolerance": float(self.constraint_tol)},
         }
 
     def to_json(self) -> tuple[dict, dict]:
@@ -92,6 +96,9 @@ class Workload:
             ff["impropers"] = [{"i": int(i), "j": int(j), "k": int(k), "l": int(l), "k_phi": float(kp),
                                 "phi0": float(p0)}
                                for (i, j, k, l), kp, p0 in zip(self.impropers, self.imp_k, self.imp_phi0)]
+        if len(self.constraints):
+            ff["constraints"] = [{"i": int(i), "j": int(j), "distance": float(dd)}
+                                 for (i, j), dd in zip(self.constraints, self.constraint_dist)]
         system = {
             "cell": {"box_size": float(self.box), "positions": self.pos.tolist()},
             "atoms": {"mass": self.mass.tolist(), "charge": self.charge.tolist(),
@@ -140,6 +147,10 @@ class Workload:
             cfg.improper_k_phi, cfg.improper_phi0 = self.imp_k, self.imp_phi0
         cfg.excl_i = self.exclusions[:, 0].tolist() if len(self.exclusions) else []
         cfg.excl_j = self.exclusions[:, 1].tolist() if len(self.exclusions) else []
+        if len(self.constraints):
+            cfg.constraint_i = self.constraints[:, 0].tolist()
+            cfg.constraint_j = self.constraints[:, 1].tolist()
+            cfg.constraint_dist = self.constraint_dist.tolist()
         apply_config(cfg, self.config_json())
         return cfg
 
@@ -195,9 +206,12 @@ WATER = dict(q_o=-0.8476, q_h=0.4238, m_o=15.9994, m_h=1.008, r0=0.1, theta0_deg
 
 def water_box(n_mol: int = 10_000, box: float = 6.69, seed: int = 7, spacing: float = 0.1045,
               thermostat: str = "nose-hoover", barostat: str = "none", n_steps: int = 1000,
-              dt: float = 0.0005, T: float = 300.0, jitter: float = 0.1) -> Workload:
-    """Flexible 3-site water on a jittered cubic lattice with random orientations
-    (O, H1, H2 per molecule; 1-2 and 1-3 exclusions)."""
+              dt: float = 0.0005, T: float = 300.0, jitter: float = 0.1,
+              rigid: bool = False, constraint_tol: float = 1e-8) -> Workload:
+    """3-site water on a jittered cubic lattice with random orientations (O, H1,
+    H2 per molecule; 1-2 and 1-3 exclusions).  Flexible by default; rigid=True
+    adds SHAKE/RATTLE distance constraints O-H1, O-H2 and H1-H2 at the model's
+    bond length and angle (the bond and angle terms stay in the force field)."""
     W = WATER
     rng = np.random.default_rng(seed)
     ns = int(math.ceil(n_mol ** (1.0 / 3.0) - 1e-9))
@@ -229,7 +243,13 @@ def water_box(n_mol: int = 10_000, box: float = 6.69, seed: int = 7, spacing: fl
         thermostat=tstat, barostat=bstat, lj_cutoff=1.0,
         bonds=bonds, bond_k=np.full(len(bonds), W["k_b"]), bond_r0=np.full(len(bonds), W["r0"]),
         angles=angles, angle_k=np.full(n_mol, W["k_a"]), angle_t0=np.full(n_mol, th),
-        exclusions=excl)
+        exclusions=excl,
+        constraints=(np.stack([np.stack([mol, mol + 1], 1), np.stack([mol, mol + 2], 1),
+                               np.stack([mol + 1, mol + 2], 1)], 1).reshape(-1, 2).astype(np.int32)
+                     if rigid else np.zeros((0, 2), np.int32)),
+        constraint_dist=(np.tile([W["r0"], W["r0"], 2 * W["r0"] * math.sin(th / 2)], n_mol)
+                         if rigid else np.zeros(0)),
+        constraint_tol=constraint_tol)
 
 
 def lj_fluid(n: int, rho_star: float, t_star: float, seed: int, n_steps: int = 1000,
