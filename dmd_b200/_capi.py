@@ -115,6 +115,7 @@ def lib() -> C.CDLL:
         "dmdgpu_kernel_launches": (C.c_int64, [vp]),
         "dmdgpu_stream": (C.c_void_p, [vp]),
         "dmdgpu_step_timed": (C.c_int, [vp, C.c_int32, C.c_int64, C.POINTER(dmdgpu_timing)]),
+        "dmdgpu_test_inject": (C.c_int, [vp, C.c_int32]),
         "dmdgpu_last_error": (C.c_char_p, [vp]),
         "dmdgpu_destroy": (None, [vp]),
         "dmdgpu_batch_create": (C.c_int, [C.c_int64, C.POINTER(dmdgpu_options), C.POINTER(vp)]),

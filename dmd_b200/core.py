@@ -306,6 +306,13 @@ class Engine:
         another slot is admitted or released.  The trajectory is unchanged."""
         self._check(self._lib.dmdgpu_repack(self._h))
 
+    def test_inject(self, what: str):
+        """Test-only, host-side fault injection for the failure paths:
+        "barrier_timeout" (the next list build's bounded grid-barrier waits run
+        out) or "list_capacity" (the next list build overflows its capacity)."""
+        code = {"barrier_timeout": 1, "list_capacity": 2}[what]
+        self._check(self._lib.dmdgpu_test_inject(self._h, code))
+
     def step_timed(self, steps: int, l2_flush_bytes: int = 0) -> dict:
         """Advance `steps` steps as one CUDA graph with device timing of every step
         and of every non-bonded / PME launch (optional L2 flush between steps)."""

@@ -287,6 +287,12 @@ int dmdgpu_step_timed(dmdgpu_ctx* c, int32_t n, int64_t flush_bytes, dmdgpu_timi
     return rc ? ctx_fail(c, rc) : DMDGPU_OK;
 }
 
+int dmdgpu_test_inject(dmdgpu_ctx* c, int32_t what) {
+    if (!c || !c->b) return DMDGPU_ERR_INVALID;
+    int rc = c->b->inject(what);
+    return rc ? ctx_fail(c, rc) : DMDGPU_OK;
+}
+
 const char* dmdgpu_last_error(const dmdgpu_ctx* c) { return c ? c->err.c_str() : "null context"; }
 
 void dmdgpu_destroy(dmdgpu_ctx* c) { delete c; }

@@ -1282,10 +1282,13 @@ int Batch::sync_status() {
     for (size_t k = 0; k < order_.size(); ++k) {
         HostRep& h = *reps_[order_[k]];
         const int st = h_st_[k].status;
-        if (st & ST_TIMEOUT) rc = fail(DMDGPU_ERR_GPU, "list-build grid barrier timed out");
+        // the cause first: a truncated list makes every force after it meaningless
+        if (st & ST_TIMEOUT) {
+            failed_ = true;
+            rc = fail(DMDGPU_ERR_GPU, "list-build grid barrier timed out");
+        } else if (st & ST_CAPACITY) rc = fail(DMDGPU_ERR_CAPACITY, "pair list capacity exceeded");
         else if (st & ST_NAN) rc = fail(DMDGPU_ERR_NAN, "non-finite force or energy on device");
         else if (st & ST_RANGE) rc = fail(DMDGPU_ERR_BOND_EXPLOSION, "force outside the fixed-point range");
-        else if (st & ST_CAPACITY) rc = fail(DMDGPU_ERR_CAPACITY, "pair list capacity exceeded");
         if (!h.done && h.target > 0 && h_st_[k].step >= h.target) {
             h.done = true;
             finished_.push_back(order_[k]);
@@ -1296,6 +1299,7 @@ int Batch::sync_status() {
 
 int Batch::step(int n) {
     CK(cudaSetDevice(device_));
+    if (failed_) return fail(DMDGPU_ERR_GPU, "a list build timed out earlier; the table is unusable");
     if (!packed_) {
         int rc = pack();
         if (rc) return rc;
@@ -1356,6 +1360,7 @@ int Batch::step_timed(int n, long long flush_bytes, dmdgpu_timing* out) {
     st_fresh_ = false;  // device work follows: the host mirror is stale
     CK(cudaSetDevice(device_));
     std::memset(out, 0, sizeof(*out));
+    if (failed_) return fail(DMDGPU_ERR_GPU, "a list build timed out earlier; the table is unusable");
     if (!packed_) {
         int rc = pack();
         if (rc) return rc;
@@ -1436,6 +1441,44 @@ int Batch::active() const {
     for (int k : order_)
         if (reps_[k] && !reps_[k]->done) ++c;
     return c;
+}
+
+// Failure-path test hooks.  Both act on the host: they only change what the
+// next list build is given, and every wait they make run out is bounded.
+//  BARRIER_TIMEOUT: the grid barrier's arrival counter starts far above the
+//    block count, so no arrival completes it; each wait gives up after 20 ms,
+//    records ST_TIMEOUT and the blocks leave the kernel.  The forces of that
+//    step come from the previous (still intact) list.
+//  LIST_CAPACITY: every replica's chunk capacity becomes 1, so the next build
+//    overflows; the builders write no chunk beyond the capacity.
+int Batch::inject(int what) {
+    CK(cudaSetDevice(device_));
+    if (!packed_) {
+        int rc = pack();
+        if (rc) return rc;
+    }
+    if (order_.empty()) return fail(DMDGPU_ERR_INVALID, "empty batch");
+    CK(cudaStreamSynchronize(stream_));
+    st_fresh_ = false;
+    if (what == DMDGPU_INJECT_BARRIER_TIMEOUT) {
+        const unsigned poison = 0x40000000u;
+        CK(cudaMemcpy(dev_.grid_bar, &poison, 4, cudaMemcpyHostToDevice));
+        dev_.bar_limit_ns = 20000000ull;
+    } else if (what == DMDGPU_INJECT_LIST_CAPACITY) {
+        for (size_t k = 0; k < order_.size(); ++k) {
+            reps_[order_[k]]->rep.chunk_cap = 1;
+            const int one = 1;
+            CK(cudaMemcpy(&d_rep_[k].chunk_cap, &one, 4, cudaMemcpyHostToDevice));
+        }
+    } else {
+        return fail(DMDGPU_ERR_PARM, "unknown injection");
+    }
+    for (size_t k = 0; k < order_.size(); ++k) {
+        const int one = 1;
+        CK(cudaMemcpy(&d_st_[k].rebuild, &one, 4, cudaMemcpyHostToDevice));
+    }
+    graph_dirty_ = true;  // the kernels take the changed table by value
+    return DMDGPU_OK;
 }
 
 int Batch::poll(int32_t* slots, int cap, int* n_done) {
@@ -1585,6 +1628,7 @@ int Batch::compute_forces(int slot, double* fx, double* fy, double* fz, double* 
     st_fresh_ = false;  // device work follows: the host mirror is stale
     CK(cudaSetDevice(device_));
     if (!has(slot)) return fail(DMDGPU_ERR_INVALID, "no such slot");
+    if (failed_) return fail(DMDGPU_ERR_GPU, "a list build timed out earlier; the table is unusable");
     if (!packed_) {
         int rc = pack();
         if (rc) return rc;
@@ -1756,6 +1800,10 @@ int Batch::load_checkpoint(int slot, const char* path) {
     double tm = 0, pe = 0;
     is.read(reinterpret_cast<char*>(&magic), 4);
     is.read(reinterpret_cast<char*>(&version), 4);
+    // the reference writes both words and never reads them back
+    // (src/sim/checkpoint.cpp:40-47); a file with other values is refused here
+    if (!is || magic != CK_MAGIC) return fail(DMDGPU_ERR_MISMATCH, "not a DMD checkpoint (bad magic)");
+    if (version != CK_VERSION) return fail(DMDGPU_ERR_MISMATCH, "unsupported checkpoint version");
     is.read(reinterpret_cast<char*>(&nn), 8);
     if (!is || nn != static_cast<uint64_t>(n))
         return fail(DMDGPU_ERR_MISMATCH, "checkpoint atom count differs from the system");
@@ -1787,6 +1835,7 @@ int Batch::load_checkpoint(int slot, const char* path) {
         is.read(reinterpret_cast<char*>(&aseed), 4);
         is.read(reinterpret_cast<char*>(&prof), 4);
         trailer = static_cast<bool>(is);
+        if (trailer && (tv < 1 || tv > 5)) return fail(DMDGPU_ERR_MISMATCH, "unsupported checkpoint trailer version");
         if (trailer && tv >= 3 && !is.read(reinterpret_cast<char*>(&pscale), 8)) pscale = 1.0;
     }
     // v4: the frame of the last list build

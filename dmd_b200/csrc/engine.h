@@ -98,6 +98,8 @@ class Batch {
     int save_checkpoint(int slot, const char* path);
     int load_checkpoint(int slot, const char* path);
     int poll(int32_t* slots, int cap, int* n_done);
+    // Host-side fault injection for the failure-path tests (DMDGPU_INJECT_*).
+    int inject(int what);
 
     long long used_bytes() const { return used_bytes_; }
     long long launches() const { return launches_; }
@@ -149,6 +151,9 @@ class Batch {
     std::map<int, std::pair<cufftHandle, cufftHandle>> plans_;
     cudaGraphExec_t graph_ = nullptr;
     bool packed_ = false;
+    // a list build timed out: its sort and list buffers are in an unknown
+    // state, so no further device work is issued on this table
+    bool failed_ = false;
     bool graph_dirty_ = true;
     bool need_eval1_ = true;
     int nb_blocks_per_sm_ = 2;  // pair-kernel launch shape (autotuned)

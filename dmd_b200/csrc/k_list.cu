@@ -1236,10 +1236,12 @@ __device__ __forceinline__ unsigned long long global_ns() {
 
 // Grid-wide barrier over the co-resident blocks of the cooperative launch:
 // bar[0] counts arrivals, bar[1] is the generation.  A wait gives up after one
-// second, records ST_TIMEOUT and returns false (the caller leaves the kernel).
+// second (d.bar_limit_ns when set), records ST_TIMEOUT and returns false (the
+// caller leaves the kernel).
 __device__ bool grid_barrier(const Dev& d) {
     __shared__ int ok;
     unsigned* bar = d.grid_bar;
+    const unsigned long long limit = d.bar_limit_ns ? d.bar_limit_ns : 1000000000ull;
     __syncthreads();
     if (threadIdx.x == 0) {
         ok = 1;
@@ -1252,7 +1254,7 @@ __device__ bool grid_barrier(const Dev& d) {
         } else {
             const unsigned long long t0 = global_ns();
             while (ld_acquire(bar + 1) == gen) {
-                if (global_ns() - t0 > 1000000000ull) {
+                if (global_ns() - t0 > limit) {
                     atomicOr(&d.st[0].status, ST_TIMEOUT);
                     ok = 0;
                     break;

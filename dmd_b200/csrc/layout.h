@@ -149,6 +149,7 @@ struct Dev {
     int* build_prefix;                 // [3][n_rep + 1] prefixes of the rebuilding replicas'
                                        // atoms, sort cells and tiles
     unsigned* grid_bar;                // [2] rebuild grid barrier: arrivals, generation
+    unsigned long long bar_limit_ns;   // a barrier wait gives up after this long (0: one second)
     // bonded terms (global atom indices)
     int n_bonds, n_angles, n_dih, n_imp;
     const int2* bond_ij;

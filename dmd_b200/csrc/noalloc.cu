@@ -1,15 +1,21 @@
 // noalloc.cu -- non-bonded force evaluation that allocates no device memory.
 //
-// Who needs it: callers that cannot call cudaMalloc -- code running while a
-// CUDA stream is being captured (allocation is not capturable), hosts whose
-// device memory is owned by another allocator or pool (a framework's caching
-// allocator, a fixed arena on an embedded or real-time system), and callers that
-// must not pay allocation latency per call.  They pass their own device buffers
-// for the inputs and outputs; every intermediate buffer of the evaluation --
-// the spatial sort, the tiles, the pair list and the fixed-point force
-// accumulators -- lives in one file-scope static device array of
-// scratch_bytes() (about 6 MB for the limits in dmdgpu.h) that each GPU holds
-// from the moment the library is loaded on it until the process exits.
+// Who needs it: callers that cannot call cudaMalloc -- hosts whose device
+// memory is owned by another allocator or pool (a framework's caching
+// allocator, a fixed arena on an embedded or real-time system, where a stray
+// cudaMalloc would fragment or exceed the arena), and callers that must not
+// pay allocation latency or risk an allocation failure in the middle of a
+// run.  They pass their own device buffers for the inputs and outputs; every
+// intermediate buffer of the evaluation -- the spatial sort, the tiles, the
+// pair list and the fixed-point force accumulators -- lives in one file-scope
+// static device array of scratch_bytes() (about 6 MB for the limits in
+// dmdgpu.h) that each GPU holds from the moment the library is loaded on it
+// until the process exits.
+//
+// The call is synchronous: it copies small host tables into the array from
+// pageable memory and ends with cudaStreamSynchronize on the caller's stream
+// to read the status word, so it cannot be issued while that stream is being
+// captured into a CUDA graph.
 //
 // The work is the same as dmdgpu_component_compute for the Lennard-Jones and
 // real-space Coulomb components: the same kernels, run over a batch of one
@@ -80,6 +86,10 @@ std::mutex g_mu;
 void* g_addr[64] = {};  // device address of g_nb_scratch per device ordinal
 
 // Per-device set-up: with the device current, resolve the array's address once.
+// The address is cached per device ordinal, so calls must run in the device's
+// primary context (the runtime API's default); a caller that switches to
+// another context on the same device, or resets the device, would be handed
+// the old context's address.
 int scratch_address(int dev, unsigned char** out) {
     std::lock_guard<std::mutex> lk(g_mu);
     if (dev < 0 || dev >= 64) return DMDGPU_ERR_PARM;
@@ -139,6 +149,9 @@ extern "C" int dmdgpu_nonbonded_noalloc(const dmdgpu_nb_params* p, const double*
     const bool phys = p->profile == DMDGPU_PROFILE_PHYS;
     const bool fp64 = p->precision == DMDGPU_PRECISION_FP64;
     cudaStream_t st = static_cast<cudaStream_t>(stream_ptr);
+    // an error left pending by the caller's earlier work is reported before any
+    // work is issued and is not cleared, so it is not mistaken for this call's
+    if (cudaPeekAtLastError() != cudaSuccess) return DMDGPU_ERR_GPU;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return DMDGPU_ERR_GPU;
     unsigned char* base = nullptr;
@@ -313,11 +326,15 @@ extern "C" int dmdgpu_nonbonded_noalloc(const dmdgpu_nb_params* p, const double*
                 ok(cudaMemsetAsync(d.chunk_prefix, 0, 8 * sizeof(int), st));
     if (!good) return DMDGPU_ERR_GPU;
     long long nl = 0;
+    // every launch is checked as soon as it is issued
     k_noalloc_types<<<(n + 255) / 256, 256, 0, st>>>(d_type, types, n, nt, d_st);
+    if (cudaGetLastError() != cudaSuccess) return DMDGPU_ERR_GPU;
     int n_sm = 148;
-    cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return DMDGPU_ERR_GPU;
     launch_rebuild(d, bin_rep, n_sm, st, &nl);
+    if (cudaGetLastError() != cudaSuccess) return DMDGPU_ERR_GPU;
     launch_nonbonded(d, fp64, phys, n_sm, 2, st, &nl);
+    if (cudaGetLastError() != cudaSuccess) return DMDGPU_ERR_GPU;
     k_noalloc_out<<<(n + 255) / 256, 256, 0, st>>>(d, d_fx, d_fy, d_fz, d_energies);
     if (cudaGetLastError() != cudaSuccess) return DMDGPU_ERR_GPU;
     // the call is synchronous: the status word says whether the list fitted
@@ -325,6 +342,8 @@ extern "C" int dmdgpu_nonbonded_noalloc(const dmdgpu_nb_params* p, const double*
     if (!ok(cudaMemcpyAsync(&out, d_st, sizeof(out), cudaMemcpyDeviceToHost, st)) ||
         !ok(cudaStreamSynchronize(st)))
         return DMDGPU_ERR_GPU;
+    // a list build whose bounded grid barrier gave up left a partial list
+    if (out.status & ST_TIMEOUT) return DMDGPU_ERR_GPU;
     if (out.status & ST_LIST) return DMDGPU_ERR_PARM;  // an atom type outside [0, n_types)
     if (out.status & ST_CAPACITY) return DMDGPU_ERR_CAPACITY;
     if (out.status & ST_NAN) return DMDGPU_ERR_NAN;

@@ -230,6 +230,19 @@ typedef struct dmdgpu_timing {
  * the timed intervals) so each step starts with a cold L2. */
 int dmdgpu_step_timed(dmdgpu_ctx *ctx, int32_t n_steps, int64_t l2_flush_bytes, dmdgpu_timing *out);
 
+/* Test-only fault injection, done on the host; no counterpart in the reference.
+ * It changes only what the next list build is given, so the failure paths can
+ * be exercised without faulting, trapping or hanging the GPU:
+ *   DMDGPU_INJECT_BARRIER_TIMEOUT  the next build's grid barrier can never be
+ *     completed and each bounded wait gives up after 20 ms: that step returns
+ *     DMDGPU_ERR_GPU and every later step or force call on the context returns
+ *     DMDGPU_ERR_GPU without issuing work (state can still be read);
+ *   DMDGPU_INJECT_LIST_CAPACITY  the pair-list capacity becomes one chunk: the
+ *     next build returns DMDGPU_ERR_CAPACITY (no chunk is written past it). */
+#define DMDGPU_INJECT_BARRIER_TIMEOUT 1
+#define DMDGPU_INJECT_LIST_CAPACITY 2
+int dmdgpu_test_inject(dmdgpu_ctx *ctx, int32_t what);
+
 const char *dmdgpu_last_error(const dmdgpu_ctx *ctx);
 void dmdgpu_destroy(dmdgpu_ctx *ctx);
 
@@ -269,9 +282,10 @@ void dmdgpu_batch_destroy(dmdgpu_batch *b);
  * Non-bonded forces without any device allocation.
  *
  * No counterpart in the reference.  For callers that cannot call cudaMalloc:
- * code issuing work while a stream is being captured, hosts whose device memory
- * belongs to another allocator or a fixed arena, callers that must not pay for
- * an allocation per call.  It computes what dmdgpu_component_compute gives for
+ * hosts whose device memory belongs to another allocator or a fixed arena (a
+ * framework's caching allocator, an embedded or real-time system that sizes
+ * its memory up front), callers that must not pay for, or risk the failure
+ * of, an allocation per call.  It computes what dmdgpu_component_compute gives for
  * components 0 (Lennard-Jones) and 4 (real-space Coulomb) -- the same kernels --
  * on caller-owned device buffers: d_x/d_y/d_z (positions), d_q (charges) and
  * d_type (LJ type per atom) in; d_fx/d_fy/d_fz (forces, written, not
@@ -288,10 +302,16 @@ void dmdgpu_batch_destroy(dmdgpu_batch *b);
  * DMDGPU_NOALLOC_MAX_CHUNKS chunks returns DMDGPU_ERR_CAPACITY.
  *
  * The first call on a device resolves the array's device address (one-time
- * set-up): make that first call before any stream capture.  Calls run on
- * `stream` (a cudaStream_t, NULL = legacy default stream) and return after it
- * has synchronised.  All calls share the one array: calls that overlap on the
- * GPU (other threads, other streams) race and must be serialised by the caller.
+ * set-up) and caches it per device ordinal, so calls must run in the device's
+ * primary context (the runtime API's default).  Calls run on `stream` (a
+ * cudaStream_t, NULL = legacy default stream) and are synchronous: they copy
+ * small host tables from pageable memory and return after the stream has
+ * synchronised, so they cannot be issued while that stream is being captured.
+ * An error left pending by the caller's earlier work is returned as
+ * DMDGPU_ERR_GPU before any work is issued (and is not cleared); a list build
+ * whose bounded wait gave up returns DMDGPU_ERR_GPU.  All calls share the one
+ * array: calls that overlap on the GPU (other threads, other streams) race and
+ * must be serialised by the caller.
  */
 #define DMDGPU_NOALLOC_MAX_ATOMS 8192
 #define DMDGPU_NOALLOC_MAX_TYPES 16

@@ -1,12 +1,14 @@
 """dmdgpu_nonbonded_noalloc: the non-bonded evaluation for callers that cannot
-allocate device memory (stream capture in progress, memory owned by another
-allocator or a fixed arena, no per-call allocation latency allowed).
+allocate device memory (device memory owned by another allocator or a fixed
+arena, no per-call allocation latency or allocation failure allowed).
 
 It must give what the allocating entry point dmdgpu_component_compute gives
 for the Lennard-Jones and real-space Coulomb components, within the tolerance
 used by the other parity tests, on two calls in a row (the static scratch array
 keeps the previous call's contents, so the second call checks that everything
-that must start at zero is cleared).  Collected last on purpose."""
+that must start at zero is cleared), and what the FP64 oracle gives for the
+same two components.  Its documented error paths are exercised too.  Collected
+last on purpose."""
 import ctypes as C
 
 import numpy as np
@@ -29,7 +31,7 @@ class nb_params(C.Structure):
                 ("skin", C.c_double)]
 
 
-def _noalloc(cfg, pos, profile, precision):
+def _noalloc(cfg, pos, profile, precision, types=None, expect=0):
     import torch
     L = _capi.lib()
     f = L.dmdgpu_nonbonded_noalloc
@@ -45,13 +47,15 @@ def _noalloc(cfg, pos, profile, precision):
     dev = torch.device("cuda:0")
     x, y, z = (torch.tensor(np.ascontiguousarray(pos[:, k]), dtype=torch.float64, device=dev) for k in range(3))
     q = torch.tensor(cfg.charges, dtype=torch.float64, device=dev)
-    t = torch.tensor(cfg.atom_types, dtype=torch.int32, device=dev)
+    t = torch.tensor(cfg.atom_types if types is None else types, dtype=torch.int32, device=dev)
     fx, fy, fz = (torch.full((len(q),), 7.0, dtype=torch.float64, device=dev) for _ in range(3))
     en = torch.zeros(2, dtype=torch.float64, device=dev)
     torch.cuda.synchronize()
     rc = f(C.byref(p), x.data_ptr(), y.data_ptr(), z.data_ptr(), q.data_ptr(), t.data_ptr(),
            fx.data_ptr(), fy.data_ptr(), fz.data_ptr(), en.data_ptr(), None)
-    assert rc == 0, rc
+    assert rc == expect, rc
+    if rc:
+        return None, None
     F = torch.stack([fx, fy, fz], 1).cpu().numpy()
     return F, float(en.sum().item())
 
@@ -67,7 +71,7 @@ def _reference_entry(cfg, pos, profile, precision):
 
 @pytest.mark.parametrize("precision", ["mixed", "fp64"])
 @pytest.mark.parametrize("profile", ["phys", "ref"])
-def test_noalloc_matches_component_compute(profile, precision):
+def test_noalloc_matches_component_compute(oracle, profile, precision):
     n_mol = 1500
     box = (n_mol / 33.43) ** (1 / 3)
     cfg = W.water_box(n_mol=n_mol, box=box, seed=21, spacing=0.1).config()
@@ -80,6 +84,12 @@ def test_noalloc_matches_component_compute(profile, precision):
         err = np.linalg.norm(F - F_r) / np.linalg.norm(F_r)
         assert err < TOL[precision], (call, err)
         assert abs(e - e_r) <= TOL[precision] * max(abs(e_r), 1.0), (call, e, e_r)
+        # and the FP64 oracle's Lennard-Jones + real-space Coulomb components
+        f0, e0, _ = oracle.component(cfg, profile, 0, pos=pos)
+        f4, e4, _ = oracle.component(cfg, profile, 4, pos=pos)
+        err_o = np.linalg.norm(F - (f0 + f4)) / np.linalg.norm(f0 + f4)
+        assert err_o < TOL[precision], (call, err_o)
+        assert abs(e - (e0 + e4)) <= TOL[precision] * max(abs(e0 + e4), 1.0) * 10, (call, e, e0 + e4)
 
 
 def test_noalloc_rejects_oversize():
@@ -95,3 +105,30 @@ def test_noalloc_rejects_oversize():
     ptr = buf.data_ptr()
     rc = f(C.byref(p), ptr, ptr, ptr, ptr, ptr, ptr, ptr, ptr, None, None)
     assert rc == 4  # DMDGPU_ERR_PARM: more atoms than the static maximum
+
+
+def test_noalloc_rejects_bad_type():
+    """An atom type outside [0, n_types) is reported (and never indexes the LJ
+    table)."""
+    cfg = W.water_box(n_mol=300, box=(300 / 33.43) ** (1 / 3), seed=5, spacing=0.1).config()
+    pos = np.stack([cfg.pos_x, cfg.pos_y, cfg.pos_z], 1)
+    types = np.asarray(cfg.atom_types, np.int32).copy()
+    types[11] = cfg.lj_n_types
+    _noalloc(cfg, pos, "phys", "mixed", types=types, expect=4)  # DMDGPU_ERR_PARM
+
+
+def test_noalloc_reports_list_overflow():
+    """A pair list longer than the static chunk maximum is reported as
+    DMDGPU_ERR_CAPACITY (no chunk is written past the maximum): 8,190 atoms of
+    water with a 2.0 nm cutoff need more than 16,384 chunks."""
+    n_mol = 2730
+    cfg = W.water_box(n_mol=n_mol, box=(n_mol / 33.43) ** (1 / 3), seed=6, spacing=0.1).config()
+    cfg.lj_cutoff = 2.0
+    cfg.coulomb_cutoff = 2.0
+    pos = np.stack([cfg.pos_x, cfg.pos_y, cfg.pos_z], 1)
+    _noalloc(cfg, pos, "ref", "mixed", expect=9)
+    # the array is still usable afterwards: a normal call succeeds
+    small = W.water_box(n_mol=300, box=(300 / 33.43) ** (1 / 3), seed=5, spacing=0.1).config()
+    pos_s = np.stack([small.pos_x, small.pos_y, small.pos_z], 1)
+    F, _ = _noalloc(small, pos_s, "phys", "mixed")
+    assert np.all(np.isfinite(F))
