@@ -97,7 +97,16 @@ class ClockSampler:
         self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
         self.p = None
 
+    def _lines(self) -> int:
+        try:
+            with open(self.f.name) as fh:
+                return sum(1 for _ in fh)
+        except OSError:
+            return 0
+
     def start(self):
+        """Start sampling and return once the first sample is written (nvidia-smi
+        takes a moment to start, longer than a short timed region)."""
         try:
             self.p = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
@@ -105,17 +114,28 @@ class ClockSampler:
                 stdout=self.f, stderr=subprocess.DEVNULL)
         except OSError:
             self.p = None
+            return
+        t0 = time.time()
+        while self._lines() < 1 and time.time() - t0 < 5.0 and self.p.poll() is None:
+            time.sleep(0.02)
+        self.n0 = self._lines()
 
     def stop(self) -> dict:
         if self.p is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        # at least one sample taken after the timed region started
+        t0 = time.time()
+        while self._lines() < getattr(self, "n0", 0) + 2 and time.time() - t0 < 1.0:
+            time.sleep(0.02)
         self.p.terminate()
         self.p.wait()
         self.f.flush()
         self.f.seek(0)
         sm, mx, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.f:
+        lines = self.f.readlines()
+        skip = max(getattr(self, "n0", 0) - 1, 0)  # samples taken before the timed region
+        for line in lines[skip:] if len(lines) > skip else lines:
             parts = [p.strip() for p in line.split(",")]
             if len(parts) < 9:
                 continue
@@ -221,27 +241,37 @@ class Ranks:
 
 def roofline(kind_bytes: float, kind_flop: float, nb_ms: float, clocks: dict, traffic,
              kernel: str, fp32_binding: bool, launch_note: str) -> dict:
+    """The pair kernel against its binding roof (top-level fields) with the other
+    roof as a sub-field.  FP32 binds where the arithmetic intensity of the
+    algorithmic work is above the ridge (water: LJ + Ewald), HBM below it (LJ)."""
     hbm_peak, peak_kind = _peaks()
     t_nb = nb_ms / 1e3
-    achieved = kind_bytes / t_nb / 1e9
+    gbs = kind_bytes / t_nb / 1e9
     tflops = kind_flop / t_nb / 1e12
-    f_sm = (clocks.get("sm_mhz") or 1965.0) * 1e6
+    f_mhz = clocks.get("sm_mhz")
+    f_sm = (f_mhz or 1965.0) * 1e6
     p32 = SM_COUNT * FP32_LANES * 2 * f_sm / 1e12
-    return {
-        "kernel": kernel,
-        "bound": "hbm", "achieved": round(achieved, 2), "peak": hbm_peak, "unit": "GB/s",
-        "frac": round(achieved / hbm_peak, 4),
+    hbm = {"bound": "hbm", "achieved": round(gbs, 2), "peak": hbm_peak, "unit": "GB/s",
+           "frac": round(gbs / hbm_peak, 4),
+           "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"}
+    fp32 = {"bound": "fp32", "achieved": round(tflops, 3), "peak": round(p32, 2), "unit": "TFLOP/s",
+            "frac": round(tflops / p32, 4),
+            "peak_source": "148 SMs x 128 FP32 lanes x 2 FLOP x " +
+                           (f"the run's median SM clock ({f_mhz:.0f} MHz)" if f_mhz else
+                            "1,965 MHz (clocks.max.sm; no clock sample in the timed region)")}
+    top, other = (fp32, hbm) if fp32_binding else (hbm, fp32)
+    out = {"kernel": kernel}
+    out.update(top)
+    out.update({
         "traffic": traffic,
-        "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
         "launch_ms": round(nb_ms, 5),
         "launch_note": launch_note,
         "algorithmic_bytes_per_launch": kind_bytes, "algorithmic_flop_per_launch": kind_flop,
-        "fp32": {"achieved_tflops": round(tflops, 3), "peak_tflops": round(p32, 2),
-                 "frac": round(tflops / p32, 4),
-                 "peak_note": "148 SMs x 128 FP32 lanes x 2 x median SM clock of the run"},
         "binding_roof": ("fp32 (arithmetic intensity above the ridge)" if fp32_binding
                          else "hbm (arithmetic intensity below the ridge)"),
-    }
+        "other_roof": other,
+    })
+    return out
 
 
 def run_single(args, R: Ranks):
@@ -295,6 +325,7 @@ def run_single(args, R: Ranks):
 
     if R.rank != 0:
         return None
+    drift = nve_drift(cfg, R.local, args.drift_steps) if spec["kind"] == "argon" else None
     # accuracy at the starting configuration against the FP64 CPU oracle
     from oracle.oracle import Oracle
     F_o, e_o = Oracle().forces(cfg, "phys", pos=acc_pos)
@@ -310,10 +341,7 @@ def run_single(args, R: Ranks):
         e0.close()
     cpu = None
     if not args.skip_cpu and R.ws == 1 and n_atoms > CPU_MAX_ATOMS:
-        cpu = {"value": None, "unit": "atom-steps/s", "cores": 1, "kind": "reference",
-               "sample": f"not timed: the reference's first step alone builds its O(N^2) pair list "
-                         f"({n_atoms * (n_atoms - 1) // 2:.2e} pair tests on one core); see the "
-                         f"water30k line for the reference's rate on the same water model"}
+        cpu = cpu_reference_extrapolated(n_atoms, water30k(0).config(), args.cpu_steps)
     elif not args.skip_cpu and R.ws == 1:
         cpu = cpu_reference([cfg], args.cpu_steps, f"the same {n_atoms:,}-atom system")
     b_atom, f_atom = PAIR_WORK[spec["kind"]]
@@ -355,7 +383,58 @@ def run_single(args, R: Ranks):
         "gpu_launches": int(t_mixed["kernel_launches"]),
         "clocks": clocks,
         "list_builds": int(s.list_builds),
+        "energies_in_timed_steps": "the device-timed value evaluates the energies and the virial "
+                                   "only on the last timed step (the ensemble needs none inside a "
+                                   "step); e2e reads them after every step",
+        **({"nve_drift": drift} if drift else {}),
     }
+
+
+def nve_drift(cfg, device: int, steps: int) -> dict:
+    """NVE energy drift max_t |E(t) - E(0)| / |E(0)| over `steps` steps
+    (tests/integration/test_argon_nve.cpp:150-171 of the reference), E = the
+    potential energy plus sum(m v^2)/2 read after every step: the GPU paths
+    (one run_n(1) per step through the C ABI) and the reference's own engine
+    (src/ compiled unmodified, REF profile) on the same inputs."""
+    import numpy as np
+    from dmd_b200.core import Engine
+    from oracle.oracle import Ref, ref_available
+    m = np.asarray(cfg.masses)
+
+    def run(step, vel, pe):
+        e = []
+        for _ in range(steps):
+            step()
+            v = vel()
+            e.append(0.5 * float(np.sum(m[:, None] * v * v)) + pe())
+        e = np.asarray(e)
+        return float(np.max(np.abs(e - e[0])) / abs(e[0]))
+
+    out = {"steps": steps, "dt_ps": cfg.dt,
+           "metric": "max over steps of |E(t) - E(t1)| / |E(t1)|, E = potential + kinetic read "
+                     "after every step, t1 the first step (both engines evaluate their initial "
+                     "forces inside it); the criterion of the reference's "
+                     "tests/integration/test_argon_nve.cpp"}
+    for prec, prof in (("mixed", "phys"), ("fp64", "phys"), ("mixed", "ref")):
+        eng = Engine(cfg, precision=prec, profile=prof, device=device)
+        out[f"gpu_{prec}_{prof}"] = run(lambda: eng.run_n(1), lambda: eng.velocities,
+                                        lambda: eng.potential_energy)
+        eng.close()
+    if ref_available():
+        re_ = Ref().engine(cfg)
+        t0 = time.perf_counter()
+        out["reference_cpu_ref"] = run(lambda: re_.step(1), lambda: re_.get(1),
+                                       lambda: re_.scalars()["pe"])
+        out["reference_seconds"] = round(time.perf_counter() - t0, 1)
+    else:
+        out["reference_cpu_ref"] = None
+    return out
+
+
+# CPU sample of the batch: 8 replicas in the batch's 3:1 LJ : decane proportion,
+# one per host core at once
+BATCH_CPU_SAMPLE = (0, 1, 2, 3, 4, 5, 192, 193)
+BATCH_CPU_WHAT = "replicas 0-5 (LJ fluids) and 192-193 (decane melts) of the 256-replica batch"
 
 
 def run_batch(args, R: Ranks):
@@ -441,8 +520,8 @@ def run_batch(args, R: Ranks):
                      "replicas": sample}
     cpu = None
     if not args.skip_cpu and R.ws == 1:
-        cpu = cpu_reference([cfgs[k] for k in (0, 1, 192)], args.cpu_steps,
-                            "replicas 0, 1 (LJ) and 192 (decane) of the same batch, one after another")
+        cpu = cpu_reference_concurrent([cfgs[k] for k in BATCH_CPU_SAMPLE], args.cpu_steps,
+                                       BATCH_CPU_WHAT)
     # pair-kernel algorithmic work, summed over the replicas
     b_alg = f_alg = 0.0
     for w, c in zip(ws_, cfgs):
@@ -557,6 +636,71 @@ def run_serve(args, R: Ranks):
     }
 
 
+def _ref_worker(args):
+    """One replica on one host core (spawned process): the reference's engine
+    stepped `steps` times; returns (atom-steps, seconds, kind)."""
+    cfg, steps = args
+    sys.path.insert(0, ROOT)
+    from oracle.oracle import Oracle, Ref, ref_available
+    if ref_available():
+        eng, kind = Ref().engine(cfg), "reference"
+    else:
+        eng, kind = Oracle().engine(cfg, "ref", brute_list=True), "port"
+    t0 = time.perf_counter()
+    eng.step(steps)
+    return len(cfg.masses) * steps, time.perf_counter() - t0, kind
+
+
+def cpu_reference_concurrent(cfgs, steps, what_sample):
+    """Independent replicas on the host cores at once, one process per replica
+    and core (the reference's engine is single-threaded): aggregate atom-steps/s
+    = all replicas' atom-steps / the slowest replica's time.  Processes are
+    spawned, never forked, so no CUDA state is inherited."""
+    import multiprocessing as mp
+    cores = min(len(cfgs), os.cpu_count() or 1)
+    with mp.get_context("spawn").Pool(cores) as pool:
+        res = pool.map(_ref_worker, [(c, steps) for c in cfgs])
+    atom_steps = sum(r[0] for r in res)
+    secs = max(r[1] for r in res)
+    kind = res[0][2]
+    return {"value": round(atom_steps / secs, 1), "unit": "atom-steps/s", "cores": cores,
+            "kind": kind,
+            "sample": f"{steps} MD steps from the start of each of {what_sample}, {len(cfgs)} "
+                      f"processes on {cores} host cores at once (the reference's C++, src/ "
+                      f"unmodified, one replica per core); slowest replica {secs:.1f} s"}
+
+
+def cpu_reference_extrapolated(n_atoms, small_cfg, steps):
+    """The reference's rate for a system too large to time directly (its first
+    step alone builds an O(N^2) pair list), from the same water model at a
+    timed size: per step = (list rebuild, O(N^2) pair tests, every 5 steps) +
+    (everything else, linear in N), each part timed on the smaller box and
+    scaled by its own law."""
+    from oracle.oracle import Ref, ref_available
+    if not ref_available():
+        return None
+    n1 = len(small_cfg.masses)
+    ref = Ref()
+    t0 = time.perf_counter()
+    ref.lj(small_cfg)  # a fresh LennardJones: one O(N^2) rebuild + one pair pass
+    t_rb = time.perf_counter() - t0
+    eng = ref.engine(small_cfg)
+    t0 = time.perf_counter()
+    eng.step(steps)
+    t_steps = time.perf_counter() - t0
+    rebuilds = (2 * steps + 9) // 10  # every 10 force evaluations, 2 per step
+    t_other = max(t_steps - rebuilds * t_rb, 0.0) / steps
+    scale = n_atoms / n1
+    t_step = t_rb * scale * scale / 5.0 + t_other * scale
+    return {"value": round(n_atoms / t_step, 1), "unit": "atom-steps/s", "cores": 1,
+            "kind": "reference",
+            "sample": f"extrapolated: the reference's C++ (src/, unmodified) timed on the "
+                      f"{n1:,}-atom box of the same water model -- one O(N^2) list rebuild "
+                      f"({t_rb:.2f} s) and {steps} MD steps ({t_steps:.1f} s) -- then the "
+                      f"rebuild (every 5 steps) scaled by (N/{n1:,})^2 and the rest of the step "
+                      f"by N/{n1:,}; predicted {t_step:.0f} s per step at {n_atoms:,} atoms"}
+
+
 def cpu_reference(cfgs, steps, what_sample):
     """The reference's CPU path on one host core (the reference has no threading
     on this path), timed on a bounded sample from the start of each run.
@@ -590,35 +734,39 @@ def run_reference(args):
     ws, rank, _ = _dist()
     if rank != 0:
         return None
+    steps = min(args.steps, args.cpu_steps)
     if args.workload in SINGLE:
         w = SINGLE[args.workload]["make"](0)
         cfgs = [w.config()]
         what = f"the same {w.n_atoms:,}-atom system"
+        if w.n_atoms > CPU_MAX_ATOMS:
+            cpu = cpu_reference_extrapolated(w.n_atoms, water30k(0).config(), steps)
+        else:
+            cpu = cpu_reference(cfgs, steps, what)
     elif args.workload == "batch256":
         from dmd_b200 import workloads as W
         ws_ = W.batch_256(seed=1234)
-        cfgs = [ws_[k].config() for k in (0, 1, 192)]
-        what = "replicas 0, 1 (LJ) and 192 (decane) of the 256-replica batch"
+        cfgs = [ws_[k].config() for k in BATCH_CPU_SAMPLE]
+        cpu = cpu_reference_concurrent(cfgs, steps, BATCH_CPU_WHAT)
     else:
         from dmd_b200.serve import job_mix
         jobs = [j for j in job_mix(args.jobs, args.rate, seed=2025, scale=args.scale)
                 if j.n_atoms <= 20000][:2]
         cfgs = [j.cfg for j in jobs]
-        what = "two jobs of the served stream"
-    steps = min(args.steps, args.cpu_steps)
-    if sum(len(c.masses) for c in cfgs) > CPU_MAX_ATOMS:
+        cpu = cpu_reference(cfgs, steps, "two jobs of the served stream")
+    if cpu is None:
         return {"impl": "reference", "metric": "atom-steps/s", "value": None,
                 "unit": "atom-steps/s", "n_gpus": ws,
-                "unavailable": "the reference's O(N^2) pair-list build of this system alone "
-                               "takes hours on one core; not timed"}
-    cpu = cpu_reference(cfgs, steps, what)
+                "unavailable": "the reference build (oracle/_ref) is not present"}
     v = cpu["value"]
     return {"impl": "reference", "metric": "atom-steps/s", "value": v, "unit": "atom-steps/s",
             "n_gpus": ws, "steps": steps, "warmup": 0, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": args.workload, "n_atoms": sum(len(c.masses) for c in cfgs),
                        "profile": "ref",
-                       "implementation": cpu["sample"].split("(")[1].split(";")[0],
+                       "implementation": ("the reference's C++ (src/, unmodified; PME via the "
+                                          "FFTW-API shim)" if cpu["kind"] == "reference" else
+                                          "the oracle's restatement of the reference algorithm"),
                        "sample_steps": steps},
             "cpu_baseline": cpu,
             "e2e": {"value": v, "unit": "atom-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -648,6 +796,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=WORKLOADS, default="water30k")
     ap.add_argument("--cpu-steps", type=int, default=10)
+    ap.add_argument("--drift-steps", type=int, default=1000, help="argon4k: NVE drift run length")
     ap.add_argument("--skip-cpu", action="store_true")
     # served stream
     ap.add_argument("--jobs", type=int, default=24)

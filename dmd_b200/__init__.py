@@ -1,16 +1,16 @@
 """dmd_b200 -- B200 (sm_100a) implementation of DMD's per-step force-and-integrate path.
 
-Drop-in for the reference's Python API (python/dmd/__init__.py): SimulationConfig,
-Engine, SystemBuilder, run, validate_config, apply_config, generate_config_template.
-The engine runs on the GPU through the C ABI of include/dmdgpu.h (libdmdgpu.so);
-there is no CPU fallback.
+The engine runs on the GPU through the C ABI of include/dmdgpu.h
+(libdmdgpu.so); there is no CPU fallback.  ``SimulationConfig`` and ``Engine``
+carry the surface of the reference's pybind module (python/dmd/core.cpp), so
+the reference's own Python package can import them in place of its CPU core;
+``load_inputs`` reads the reference's system.json / config.json formats;
+``Batch`` and ``serve`` advance many systems in one device table.
 """
-from .config import apply_config, generate_config_template, validate_config
 from .core import BarostatConfig, DmdGpuError, Engine, SimulationConfig, ThermostatConfig
-from .system import SystemBuilder
-from .runner import run
+from .inputs import InputError, load_inputs
 
 __all__ = [
-    "SimulationConfig", "Engine", "SystemBuilder", "run", "validate_config", "apply_config",
-    "generate_config_template", "ThermostatConfig", "BarostatConfig", "DmdGpuError",
+    "SimulationConfig", "Engine", "ThermostatConfig", "BarostatConfig", "DmdGpuError",
+    "load_inputs", "InputError",
 ]

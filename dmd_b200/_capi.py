@@ -67,7 +67,10 @@ class dmdgpu_system(C.Structure):
 
 class dmdgpu_options(C.Structure):
     _fields_ = [("profile", C.c_int32), ("precision", C.c_int32), ("skin", C.c_double),
-                ("device", C.c_int32), ("rng_seed", C.c_uint64)]
+                ("device", C.c_int32), ("rng_seed", C.c_uint64), ("nb_form", C.c_int32)]
+
+
+NB_FORMS = {"auto": 0, "chunk32": 1, "cluster8": 2}
 
 
 class dmdgpu_timing(C.Structure):

@@ -122,7 +122,7 @@ class SimulationConfig:
         return int(math.isqrt(len(self._arrays["lj_sigma"]))) if len(self._arrays["lj_sigma"]) else 0
 
 
-def _options(precision=None, profile=None, skin=None, device=None, rng_seed=None):
+def _options(precision=None, profile=None, skin=None, device=None, rng_seed=None, nb_form=None):
     precision = precision or os.environ.get("DMD_PRECISION", "mixed")
     profile = profile or os.environ.get("DMD_PROFILE", "ref")
     if skin is None:
@@ -139,6 +139,10 @@ def _options(precision=None, profile=None, skin=None, device=None, rng_seed=None
     o.skin = float(skin)
     o.device = int(device)
     o.rng_seed = int(rng_seed if rng_seed is not None else 0x5EED)
+    nb_form = nb_form or os.environ.get("DMD_NB_FORM", "auto")
+    if nb_form not in _capi.NB_FORMS:
+        raise ValueError(f"nb_form must be one of {list(_capi.NB_FORMS)}")
+    o.nb_form = _capi.NB_FORMS[nb_form]
     return o
 
 
@@ -154,10 +158,10 @@ class Engine:
     """GPU-resident SimulationEngine with the EngineWrapper interface."""
 
     def __init__(self, cfg: SimulationConfig, precision=None, profile=None, skin=None,
-                 device=None, rng_seed=None):
+                 device=None, rng_seed=None, nb_form=None):
         self._lib = _capi.lib()
         self._desc = _capi.SystemDesc(cfg)
-        self._opt = _options(precision, profile, skin, device, rng_seed)
+        self._opt = _options(precision, profile, skin, device, rng_seed, nb_form)
         h = C.c_void_p()
         rc = self._lib.dmdgpu_create(C.byref(self._desc.s), C.byref(self._opt), C.byref(h))
         if rc != 0:

@@ -70,20 +70,30 @@ void sort_grid(int n, double L, int& nvx, int& nvz) {
 // size with every admission; nearby sizes share a shape).
 namespace {
 struct TuneKey {
-    int device, fp64, pme, bucket;
+    int device, fp64, pme, bucket, forced;
     bool operator<(const TuneKey& o) const {
-        return std::tie(device, fp64, pme, bucket) < std::tie(o.device, o.fp64, o.pme, o.bucket);
+        return std::tie(device, fp64, pme, bucket, forced) < std::tie(o.device, o.fp64, o.pme, o.bucket, o.forced);
     }
 };
+// A choice: the pair-kernel form (NbForm) and its blocks of 256 threads per SM.
+struct TuneChoice {
+    int form, bps;
+};
 std::mutex g_tune_mu;
-std::map<TuneKey, int> g_tune;
+std::map<TuneKey, TuneChoice> g_tune;
 constexpr int kTuneSteps = 6;               // timed steps per candidate
-constexpr int kTuneCand[] = {2, 3};         // pair-kernel blocks per SM
+constexpr TuneChoice kTuneCand[] = {{NB_CLUSTER8, 1}, {NB_CLUSTER8, 2}, {NB_CHUNK32, 2}, {NB_CHUNK32, 3}};
 
-TuneKey tune_key(int device, bool fp64, bool pme, long long n_atoms) {
+// forced: the caller's dmdgpu_options.nb_form (0: the tuner picks the form too)
+TuneKey tune_key(int device, bool fp64, bool pme, long long n_atoms, int forced) {
     int b = 0;
     while ((1LL << (2 * b + 2)) <= n_atoms) ++b;
-    return TuneKey{device, fp64 ? 1 : 0, pme ? 1 : 0, b};
+    return TuneKey{device, fp64 ? 1 : 0, pme ? 1 : 0, b, forced};
+}
+
+// DMDGPU_NB_* of the options -> NbForm, or -1 for the autotuner's choice
+int forced_form(int nb_form) {
+    return nb_form == DMDGPU_NB_CHUNK32 ? NB_CHUNK32 : (nb_form == DMDGPU_NB_CLUSTER8 ? NB_CLUSTER8 : -1);
 }
 }  // namespace
 
@@ -240,6 +250,10 @@ long long Batch::footprint(const HostSystem& s) const {
     long long chunks = tiles * 64;
     (void)rho;
     long long b = n * per_atom + tiles * 32 * per_slot + chunks * (4 + 32 * 8) + tiles * 64;
+    // mixed precision: the list regrouped by 8-atom i-cluster (rows of 32 entry
+    // words and 32 byte masks, up to 4 per chunk and 4 per tile) and its
+    // per-tile bookkeeping
+    if (!fp64_) b += (4 * chunks + 4 * tiles) * (32 * 4 + 32) + chunks * 8 + tiles * (12 + 4 * 8);
     b += static_cast<long long>(s.ci.size()) * (8 + 8 + 8);  // constraints and their groups
     if (s.coulomb_type == 1) {
         long long K = std::max(8, static_cast<int>(s.box / s.spacing + 0.5));
@@ -499,6 +513,7 @@ int Batch::pack() {
             RepState st = h_st_[k];
             st.have_forces = 0;      // forces are evaluated again at the same positions
             st.n_chunks = 0;
+            st.n_cl = 0;
             st.green_L = 0.0;        // the new arena holds no PME influence function yet
             o.init = st;
         }
@@ -514,7 +529,8 @@ int Batch::pack() {
     }
     // offsets
     long long n_atoms = 0, n_tiles = 0, n_bins = 0, n_chunks = 0, n_lj = 0, n_bond = 0, n_ang = 0,
-              n_dih = 0, n_imp = 0, n_excl = 0, mesh_fix = 0, mesh_real = 0, mesh_cplx = 0, n_bsp = 0;
+              n_dih = 0, n_imp = 0, n_excl = 0, mesh_fix = 0, mesh_real = 0, mesh_cplx = 0, n_bsp = 0,
+              n_cl = 0;
     int pme_blocks = 0, conv_blocks = 0;
     any_pme_ = any_baro_ = any_ref_lj_ = any_andersen_ref_ = any_andersen_phys_ = false;
     for (int k = 0; k < R; ++k) {
@@ -537,6 +553,12 @@ int Batch::pack() {
             if (P.rc_list <= 0) P.chunk_cap = 1;
         }
         P.chunk_begin = static_cast<int>(n_chunks);
+        // i-cluster rows: each of a tile's chunks adds at most 32 entries to each
+        // of its four clusters, so 4 rows per chunk plus one partial row per
+        // cluster always suffice
+        P.cl_cap = fp64_ ? 0 : static_cast<int>(std::min<long long>(4LL * P.chunk_cap + 4LL * P.n_tiles, INT32_MAX / 64));
+        P.cl_begin = static_cast<int>(n_cl);
+        n_cl += P.cl_cap;
         n_atoms += s.n;
         n_tiles += P.n_tiles;
         n_bins += static_cast<long long>(P.nvx) * P.nvx * P.nvz;
@@ -648,7 +670,17 @@ int Batch::pack() {
         d.nb_work = d.chunk_prefix + R + 1;
         d.build_work = d.chunk_prefix + R + 2;
         d.grid_bar = A.alloc<unsigned>(2);
-        d.build_prefix = A.alloc<int>(3 * (R + 1));
+        d.build_prefix = A.alloc<int>(4 * (R + 1));
+        if (!fp64_) {
+            d.tile_nch = A.alloc<int>(n_tiles);
+            d.tile_c0 = A.alloc<int>(n_tiles);
+            d.tile_fill = A.alloc<int>(n_tiles);
+            d.chunk_order = A.alloc<int>(n_chunks);
+            d.chunk_sorted = A.alloc<int>(n_chunks);
+            d.cl_j = A.alloc<uint32_t>(n_cl * 32);
+            d.cl_m = A.alloc<uint8_t>(n_cl * 32);
+            d.cl_job = A.alloc<int2>(4 * n_tiles);
+        }
         // host-side staging
         std::vector<double> hm(n_atoms), hq(n_atoms), hx(n_atoms), hy(n_atoms), hz(n_atoms), hvx(n_atoms),
             hvy(n_atoms), hvz(n_atoms), hxr(n_atoms), hyr(n_atoms), hzr(n_atoms);
@@ -980,9 +1012,11 @@ int Batch::pack() {
     }
     {
         std::lock_guard<std::mutex> lk(g_tune_mu);
-        auto it = g_tune.find(tune_key(device_, fp64_, any_pme_, dev_.n_atoms));
+        const int forced = forced_form(opt_.nb_form);
+        auto it = g_tune.find(tune_key(device_, fp64_, any_pme_, dev_.n_atoms, opt_.nb_form));
         tuned_ = fp64_ || it != g_tune.end();
-        nb_blocks_per_sm_ = (it != g_tune.end()) ? it->second : (any_pme_ ? 2 : 3);
+        nb_form_ = (it != g_tune.end()) ? it->second.form : (forced >= 0 ? forced : NB_CLUSTER8);
+        nb_blocks_per_sm_ = (it != g_tune.end()) ? it->second.bps : ((any_pme_ || nb_form_ == NB_CLUSTER8) ? 2 : 3);
     }
     packed_ = true;
     graph_dirty_ = true;
@@ -1010,7 +1044,7 @@ void Batch::enqueue_eval(int pass) {
         e0 = next_event();
         record(e0, stream_);
     }
-    launch_nonbonded(d, fp64_, phys_, n_sm_, nb_blocks_per_sm_, stream_, &launches_);
+    launch_nonbonded(d, fp64_, phys_, n_sm_, nb_blocks_per_sm_, nb_form_, stream_, &launches_);
     if (prof_nb_) {
         e1 = next_event();
         record(e1, stream_);
@@ -1187,14 +1221,19 @@ int Batch::run_steps(int n) {
 // only when the call has enough steps to spare.
 int Batch::autotune(int max_steps, int* used) {
     *used = 0;
-    const int n_cand = static_cast<int>(sizeof(kTuneCand) / sizeof(kTuneCand[0]));
+    const int forced = forced_form(opt_.nb_form);
+    std::vector<TuneChoice> cand;
+    for (const TuneChoice& c : kTuneCand)
+        if (forced < 0 || c.form == forced) cand.push_back(c);
+    const int n_cand = static_cast<int>(cand.size());
     if (max_steps < n_cand * kTuneSteps) return DMDGPU_OK;
     std::vector<cudaEvent_t> ev(kTuneSteps + 1);
     for (auto& e : ev) CK(cudaEventCreate(&e));
-    int best = nb_blocks_per_sm_;
+    TuneChoice best{nb_form_, nb_blocks_per_sm_};
     float best_ms = 1e30f;
     for (int c = 0; c < n_cand; ++c) {
-        nb_blocks_per_sm_ = kTuneCand[c];
+        nb_form_ = cand[c].form;
+        nb_blocks_per_sm_ = cand[c].bps;
         std::vector<float> t(kTuneSteps);
         CK(cudaEventRecord(ev[0], stream_));
         for (int i = 0; i < kTuneSteps; ++i) {
@@ -1208,15 +1247,16 @@ int Batch::autotune(int max_steps, int* used) {
         const float med = t[kTuneSteps / 2];
         if (med < best_ms) {
             best_ms = med;
-            best = kTuneCand[c];
+            best = cand[c];
         }
         *used += kTuneSteps;
     }
     for (auto& e : ev) cudaEventDestroy(e);
-    nb_blocks_per_sm_ = best;
+    nb_form_ = best.form;
+    nb_blocks_per_sm_ = best.bps;
     tuned_ = true;
     std::lock_guard<std::mutex> lk(g_tune_mu);
-    g_tune[tune_key(device_, fp64_, any_pme_, dev_.n_atoms)] = best;
+    g_tune[tune_key(device_, fp64_, any_pme_, dev_.n_atoms, opt_.nb_form)] = best;
     return DMDGPU_OK;
 }
 
@@ -1696,6 +1736,42 @@ int Batch::pair_list(int slot, int32_t* pi, int32_t* pj, long long cap, long lon
         }
     }
     std::sort(pairs.begin(), pairs.end());
+    if (dev_.cl_j && nc) {
+        // the i-cluster rows must encode exactly the same pair set
+        std::vector<int2> job(4LL * P.n_tiles);
+        CK(cudaMemcpy(job.data(), dev_.cl_job + 4LL * P.tile_begin, sizeof(int2) * job.size(),
+                      cudaMemcpyDeviceToHost));
+        const int rows = st.n_cl;
+        std::vector<uint32_t> cj(32LL * rows);
+        std::vector<uint8_t> cm(32LL * rows);
+        if (rows) {
+            CK(cudaMemcpy(cj.data(), dev_.cl_j + 32LL * P.cl_begin, 4LL * cj.size(), cudaMemcpyDeviceToHost));
+            CK(cudaMemcpy(cm.data(), dev_.cl_m + 32LL * P.cl_begin, cm.size(), cudaMemcpyDeviceToHost));
+        }
+        std::vector<std::pair<int, int>> cp;
+        cp.reserve(pairs.size());
+        for (int t = 0; t < P.n_tiles; ++t)
+            for (int k = 0; k < 4; ++k) {
+                const int2 jb = job[4 * t + k];
+                for (int g = jb.x; g < jb.x + jb.y; ++g) {
+                    const long long row = g - P.cl_begin;
+                    if (row < 0 || row >= rows) return fail(DMDGPU_ERR_MISMATCH, "i-cluster row out of range");
+                    for (int l = 0; l < 32; ++l) {
+                        const uint32_t m = cm[32 * row + l];
+                        if (!m) continue;
+                        const int js = static_cast<int>(cj[32 * row + l] & 0x03FFFFFFu);
+                        const int aj = aos[js - s0] - a0;
+                        for (int i = 0; i < 8; ++i)
+                            if ((m >> i) & 1u) {
+                                const int ai = aos[32 * (P.tile_begin + t) + 8 * k + i - s0] - a0;
+                                cp.emplace_back(std::min(ai, aj), std::max(ai, aj));
+                            }
+                    }
+                }
+            }
+        std::sort(cp.begin(), cp.end());
+        if (cp != pairs) return fail(DMDGPU_ERR_MISMATCH, "i-cluster rows differ from the chunk list");
+    }
     *count = static_cast<long long>(pairs.size());
     for (long long p = 0; p < std::min<long long>(cap, *count); ++p) {
         pi[p] = pairs[p].first;

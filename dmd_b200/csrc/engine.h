@@ -157,6 +157,7 @@ class Batch {
     bool graph_dirty_ = true;
     bool need_eval1_ = true;
     int nb_blocks_per_sm_ = 2;  // pair-kernel launch shape (autotuned)
+    int nb_form_ = 1;           // pair-kernel form (NbForm; autotuned)
     bool tuned_ = false;
     long long launches_ = 0;
     long long per_step_launches_ = 0;

@@ -157,6 +157,10 @@ __device__ __forceinline__ void tile_warp(const Dev& d, int t, int lane) {
                                           static_cast<float>(w[2] - c[2]), static_cast<float>(qa))
                             : make_float4(0.f, 0.f, 0.f, 0.f);
     if (d.xq64) d.xq64[slot] = make_double4(xa, ya, za, qa);
+    if (d.tile_nch && lane == 0) {  // chunk counters of the i-cluster regrouping
+        d.tile_nch[t] = 0;
+        d.tile_fill[t] = 0;
+    }
 }
 
 // Entry encoding: bits 0..25 j slot, 26..31 image shift (mx+1, my+1, mz+1), 2 bits each.
@@ -1179,19 +1183,40 @@ __device__ __forceinline__ void build_tile_cells(const Dev& d, int I, TileScratc
 }
 
 // R6 block scratch: one builder runs at a time.
+// R11 per-warp staging of one i-cluster row (fewer than 32 entries carried
+// plus one chunk's 32).
+constexpr int CL_STAGE = 64;
+struct ClusterScratch {
+    uint32_t e[BW][CL_STAGE];
+    uint8_t m[BW][CL_STAGE];
+};
+
 union BuildScratch {
     ScanScratch scan;
     TileScratch cells[BW];
+    ClusterScratch cl;  // R11, after the list build is complete
 };
 
 // R7: close the rebuild -- capacity check, counters, flat chunk numbering --
 // by one warp: each lane takes a contiguous run of replicas, a warp scan
-// places the runs.
+// places the runs.  With the i-cluster regrouping to follow (d.cl_j), it also
+// numbers the rebuilding replicas' chunks (build_prefix[3]) and leaves their
+// `rebuild` flags for the regrouping's closing phase to clear.
+__device__ __forceinline__ int warp_incl_scan(int v, int lane) {
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(FULL, v, o);
+        if (lane >= o) v += t;
+    }
+    return v;
+}
+
 __device__ __forceinline__ void rebuild_finish(const Dev& d, int lane) {
     const int n = d.n_rep;
     const int per = (n + 31) >> 5;
     const int r0 = min(lane * per, n), r1 = min(r0 + per, n);
-    int sum = 0;
+    const bool regroup = d.cl_j != nullptr;
+    int sum = 0, sum_rb = 0;
     for (int r = r0; r < r1; ++r) {
         RepState* s = d.st + r;
         if (s->rebuild) {
@@ -1199,25 +1224,157 @@ __device__ __forceinline__ void rebuild_finish(const Dev& d, int lane) {
                 s->status |= ST_CAPACITY;
                 s->n_chunks = d.rep[r].chunk_cap;
             }
-            s->rebuild = 0;
+            if (!regroup) s->rebuild = 0;
             s->lj_counter = 0;
             s->list_builds += 1;
             s->L_build = s->L;
+            sum_rb += s->n_chunks;
         }
         sum += s->n_chunks;
     }
-    int incl = sum;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const int v = __shfl_up_sync(FULL, incl, o);
-        if (lane >= o) incl += v;
-    }
+    const int incl = warp_incl_scan(sum, lane);
     int run = incl - sum;
     for (int r = r0; r < r1; ++r) {
         d.chunk_prefix[r] = run;
         run += d.st[r].n_chunks;
     }
     if (lane == 31) d.chunk_prefix[n] = incl;
+    if (regroup) {
+        int* pc = d.build_prefix + 3 * (n + 1);
+        const int incl_rb = warp_incl_scan(sum_rb, lane);
+        int run_rb = incl_rb - sum_rb;
+        for (int r = r0; r < r1; ++r) {
+            pc[r] = run_rb;
+            if (d.st[r].rebuild) run_rb += d.st[r].n_chunks;
+        }
+        if (lane == 31) pc[n] = incl_rb;
+    }
+}
+
+// ---- i-cluster regrouping (R8 .. R12, mixed precision only) -----------------
+// The pair list of every rebuilt replica regrouped by 8-atom i-cluster: for
+// i-tile I and k = 0..3, cluster 4 I + k holds the entries of I's chunks whose
+// mask has a bit among lanes 8k .. 8k+7, with those 8 bits as the entry's
+// mask, packed 32 to a row.  The pair set is the same bit for bit; the
+// cluster's j atoms are those within the list cutoff of its 8 atoms rather
+// than of all 32, so far fewer of the (i, j) lane pairs a row evaluates are
+// empty.  The order is canonical -- a tile's chunks sorted by their first
+// entry word (unique within a tile), entries in lane order -- so the rows do
+// not depend on the order in which the builders allocated the chunks.
+
+// R9: exclusive scan of one replica's per-tile chunk counts into tile_c0 (the
+// tile's first position in chunk_order), by one block.
+__device__ __forceinline__ void tile_scan_replica(const Dev& d, int r) {
+    __shared__ int s_warp[NT_B / 32];
+    const Rep& R = d.rep[r];
+    const int nt = R.n_tiles;
+    const int per = (nt + NT_B - 1) / NT_B;
+    const int t0 = R.tile_begin + min(static_cast<int>(threadIdx.x) * per, nt);
+    const int t1 = min(t0 + per, R.tile_begin + nt);
+    int local = 0;
+    for (int t = t0; t < t1; ++t) local += d.tile_nch[t];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int incl = warp_incl_scan(local, lane);
+    if (lane == 31) s_warp[w] = incl;
+    __syncthreads();
+    int off = 0;
+    for (int k = 0; k < w; ++k) off += s_warp[k];
+    int run = R.chunk_begin + off + incl - local;
+    for (int t = t0; t < t1; ++t) {
+        d.tile_c0[t] = run;
+        run += d.tile_nch[t];
+    }
+    __syncthreads();
+}
+
+// R11: one warp per rebuilt i-tile: canonical chunk order, then the tile's
+// four cluster lists.
+__device__ __forceinline__ void cluster_tile(const Dev& d, int t, int lane, uint32_t* se, uint8_t* sm) {
+    const int r = d.tile_rep[t];
+    RepState* s = d.st + r;
+    const Rep& R = d.rep[r];
+    const int n = d.tile_nch[t];
+    const int c0 = d.tile_c0[t];
+    const int* ids = d.chunk_order + c0;
+    int* sorted = d.chunk_sorted + c0;
+    // rank of each chunk by (first entry word, then position): distinct ranks
+    for (int base = 0; base < n; base += 32) {
+        const int mine = base + lane;
+        const int id = mine < n ? ids[mine] : -1;
+        const uint32_t key = id >= 0 ? d.chunk_j[32LL * id] : 0xffffffffu;
+        int rank = 0;
+        for (int b2 = 0; b2 < n; b2 += 32) {
+            const int other = b2 + lane;
+            const uint32_t ok = other < n ? d.chunk_j[32LL * ids[other]] : 0xffffffffu;
+            for (int k = 0; k < 32 && b2 + k < n; ++k) {
+                const uint32_t kk = __shfl_sync(FULL, ok, k);
+                rank += (kk < key || (kk == key && b2 + k < mine)) ? 1 : 0;
+            }
+        }
+        if (id >= 0) sorted[rank] = id;
+    }
+    __syncwarp();
+    // rows per cluster
+    int cnt[4] = {0, 0, 0, 0};
+    for (int k = 0; k < n; ++k) {
+        const uint32_t m = d.chunk_mask[32LL * sorted[k] + lane];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) cnt[q] += __popc(__ballot_sync(FULL, ((m >> (8 * q)) & 0xffu) != 0));
+    }
+    int rows[4], total = 0;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        rows[q] = (cnt[q] + 31) >> 5;
+        total += rows[q];
+    }
+    int base = 0;
+    if (lane == 0) base = atomicAdd(&s->n_cl, total);
+    base = __shfl_sync(FULL, base, 0);
+    if (base + total > R.cl_cap) {  // cannot happen with cl_cap = 4 chunk_cap + 4 n_tiles
+        if (lane == 0) set_status(s, ST_CAPACITY);
+        if (lane < 4) d.cl_job[4 * t + lane] = make_int2(0, 0);
+        return;
+    }
+    int g = R.cl_begin + base;
+    if (lane < 4) {
+        int first = g;
+        for (int q = 0; q < lane; ++q) first += rows[q];
+        d.cl_job[4 * t + lane] = make_int2(first, rows[lane]);
+    }
+    for (int q = 0; q < 4; ++q) {
+        int fill = 0;
+        for (int k = 0; k < n; ++k) {
+            const long long c = sorted[k];
+            const uint32_t e = d.chunk_j[32 * c + lane];
+            const uint32_t m8 = (d.chunk_mask[32 * c + lane] >> (8 * q)) & 0xffu;
+            const uint32_t has = __ballot_sync(FULL, m8 != 0);
+            const int pos = fill + __popc(has & ((1u << lane) - 1u));
+            if (m8) {
+                se[pos] = e;
+                sm[pos] = static_cast<uint8_t>(m8);
+            }
+            fill += __popc(has);
+            __syncwarp();
+            if (fill >= 32) {
+                d.cl_j[32LL * g + lane] = se[lane];
+                d.cl_m[32LL * g + lane] = sm[lane];
+                ++g;
+                const uint32_t te = se[lane + 32];
+                const uint8_t tm = sm[lane + 32];
+                __syncwarp();
+                se[lane] = te;
+                sm[lane] = tm;
+                fill -= 32;
+                __syncwarp();
+            }
+        }
+        if (fill > 0) {
+            d.cl_j[32LL * g + lane] = lane < fill ? se[lane] : 0u;
+            d.cl_m[32LL * g + lane] = lane < fill ? sm[lane] : static_cast<uint8_t>(0);
+            ++g;
+        }
+        __syncwarp();
+    }
 }
 
 __device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
@@ -1284,7 +1441,10 @@ __global__ void __launch_bounds__(NT_B, 4) k_rebuild(Dev d, const int* bin_rep) 
     // later phases visit only those)
     if (gtid == 0) *d.build_work = 0;
     for (int r = gtid; r < d.n_rep; r += gthreads)
-        if (d.st[r].rebuild) d.st[r].n_chunks = 0;
+        if (d.st[r].rebuild) {
+            d.st[r].n_chunks = 0;
+            d.st[r].n_cl = 0;
+        }
     if (blockIdx.x == 0 && tid < 96) {  // warps 0, 1, 2: atoms, sort cells, tiles
         const int kind = tid >> 5;
         int* pre = d.build_prefix + kind * (d.n_rep + 1);
@@ -1353,6 +1513,38 @@ __global__ void __launch_bounds__(NT_B, 4) k_rebuild(Dev d, const int* bin_rep) 
     }
     if (!grid_barrier(d)) return;
     if (gtid < 32) rebuild_finish(d, lane);
+    if (!d.cl_j) return;  // FP64 tables keep the chunk list only
+    if (!grid_barrier(d)) return;
+    // R8: chunks per rebuilt i-tile
+    const int* pc = pt + 2 * (d.n_rep + 1);  // build_prefix[3], written by R7
+    const int n_c = pc[d.n_rep];
+    for (int w = gtid; w < n_c; w += gthreads) {
+        const int r = chunk_replica(pc, d.n_rep, w);
+        atomicAdd(d.tile_nch + d.chunk_itile[d.rep[r].chunk_begin + (w - pc[r])], 1);
+    }
+    if (!grid_barrier(d)) return;
+    // R9: each tile's first position in chunk_order
+    for (int r = blockIdx.x; r < d.n_rep; r += gridDim.x)
+        if (d.st[r].rebuild) tile_scan_replica(d, r);
+    if (!grid_barrier(d)) return;
+    // R10: chunk ids grouped by tile (order within a tile fixed by R11)
+    for (int w = gtid; w < n_c; w += gthreads) {
+        const int r = chunk_replica(pc, d.n_rep, w);
+        const int c = d.rep[r].chunk_begin + (w - pc[r]);
+        const int I = d.chunk_itile[c];
+        d.chunk_order[d.tile_c0[I] + atomicAdd(d.tile_fill + I, 1)] = c;
+    }
+    if (!grid_barrier(d)) return;
+    // R11: canonical order and the four cluster lists of every rebuilt tile
+    const int wib = tid >> 5;
+    for (int w = gwarp; w < n_t; w += nwarps) {
+        const int r = chunk_replica(pt, d.n_rep, w);
+        cluster_tile(d, d.rep[r].tile_begin + (w - pt[r]), lane, s_scr.cl.e[wib], s_scr.cl.m[wib]);
+    }
+    if (!grid_barrier(d)) return;
+    // R12: the rebuild is complete
+    for (int r = gtid; r < d.n_rep; r += gthreads)
+        if (d.st[r].rebuild) d.st[r].rebuild = 0;
 }
 
 void launch_rebuild(const Dev& d, const int* bin_rep, int n_sm, cudaStream_t st, long long* nlaunch) {

@@ -350,6 +350,244 @@ __global__ void __launch_bounds__(256, 3) k_nb_f32(Dev d) {
     flush_acc(d, cur, acc);
 }
 
+// ---- 8-atom i-cluster form -------------------------------------------------
+// One warp per i-cluster (8 consecutive slots of a tile), over the cluster's
+// rows of 32 j entries.  Lane l owns j entry l of the row: it brings that j
+// atom into the i-tile frame once per row, visits the 8 cluster atoms in turn
+// (their coordinates are warp-uniform shared-memory broadcasts) and keeps the
+// j force in registers, flushed once per row.  Each lane also keeps its own
+// partial i forces for the 8 atoms (24 registers) over all the cluster's rows;
+// at the end a butterfly reduce-scatter sums them across the warp in a fixed
+// order.  No shuffle per pair, and because a cluster's entries are the j atoms
+// within the list cutoff of its 8 atoms (not of a whole 32-atom tile), far
+// fewer of the evaluated lane pairs are empty.  Masked and out-of-cutoff pairs
+// get zero force by a select, as in the 32-wide form; pairs within 1e-5
+// (relative) of a cutoff are redone with the FP64 reference membership test
+// and added by fixed-point atomics of their own.
+struct ClusterStage {
+    float4 xi[8];   // x, y, z (tile frame), KE q
+    int row[8];     // LJ table row of each cluster atom
+    int ai[8];      // atom index (-1: padding slot)
+};
+
+// Butterfly reduce-scatter of v[0..7] over the warp: afterwards every lane
+// holds the warp sum of v[i] for i = 4 b4 + 2 b3 + b2 (b = lane bits).
+__device__ __forceinline__ float reduce8(const float (&v)[8], int lane) {
+    float w4[4], w2[2];
+    const bool h16 = lane & 16, h8 = lane & 8, h4 = lane & 4;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const float send = h16 ? v[j] : v[j + 4];
+        const float keep = h16 ? v[j + 4] : v[j];
+        w4[j] = keep + __shfl_xor_sync(FULL, send, 16);
+    }
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+        const float send = h8 ? w4[j] : w4[j + 2];
+        const float keep = h8 ? w4[j + 2] : w4[j];
+        w2[j] = keep + __shfl_xor_sync(FULL, send, 8);
+    }
+    const float send = h4 ? w2[0] : w2[1];
+    float t = (h4 ? w2[1] : w2[0]) + __shfl_xor_sync(FULL, send, 4);
+    t += __shfl_xor_sync(FULL, t, 2);
+    t += __shfl_xor_sync(FULL, t, 1);
+    return t;
+}
+
+template <bool PHYS, bool SAME, bool ENERGY>
+__device__ __forceinline__ void nb_cluster(const Dev& d, const Rep& R, RepState* s, int cl, int2 job,
+                                           int lane, ClusterStage& S, const float4* lj_tab, Acc& acc) {
+    const double L = s->L;
+    const int I = cl >> 2;
+    const int s0 = 32 * I + 8 * (cl & 3);
+    if (lane < 8) {
+        const int si = s0 + lane;
+        const float4 x = d.xq32[si];
+        S.xi[lane] = make_float4(x.x, x.y, x.z, static_cast<float>(KE) * x.w);
+        S.row[lane] = R.lj_off + d.type_s[si] * R.n_types;
+        S.ai[lane] = d.atom_of_slot[si];
+    }
+    __syncwarp();
+    const double tIx = d.tcx[I], tIy = d.tcy[I], tIz = d.tcz[I];
+    const bool has_lj = (R.flags & F_LJ) != 0;
+    const bool has_c = PHYS && (R.flags & F_COUL_REAL) != 0;
+    const float rl2 = has_lj ? static_cast<float>(R.rc_lj2) : 0.f;
+    const float rcc2 = has_c ? static_cast<float>(R.rc_c2) : 0.f;
+    const float wl = rl2 * 1e-5f, wc = rcc2 * 1e-5f;
+    const float alpha = static_cast<float>(R.alpha);
+    const float a2l2e = -alpha * alpha * 1.4426950408889634f;
+    const float c2a = TWO_OVER_SQRTPI_F * alpha;
+    float fix[8], fiy[8], fiz[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) fix[i] = fiy[i] = fiz[i] = 0.f;
+    float el = 0.f, ec = 0.f, vir = 0.f;
+#pragma unroll 1
+    for (int k = 0; k < job.y; ++k) {
+        const long long g = job.x + k;
+        const uint32_t e = d.cl_j[32 * g + lane];
+        const uint32_t m8 = d.cl_m[32 * g + lane];
+        const int js = static_cast<int>(e & 0x03FFFFFFu);
+        float4 xj = make_float4(1e6f, 1e6f, 1e6f, 0.f);
+        int tj = 0;
+        if (m8) {
+            xj = d.xq32[js];
+            tj = d.type_s[js];
+            const int J = js >> 5;
+            const int mx = static_cast<int>((e >> 26) & 3u) - 1;
+            const int my = static_cast<int>((e >> 28) & 3u) - 1;
+            const int mz = static_cast<int>((e >> 30) & 3u) - 1;
+            xj.x += static_cast<float>(d.tcx[J] - tIx + mx * L);
+            xj.y += static_cast<float>(d.tcy[J] - tIy + my * L);
+            xj.z += static_cast<float>(d.tcz[J] - tIz + mz * L);
+        }
+        float fjx = 0.f, fjy = 0.f, fjz = 0.f;
+        uint32_t band = 0;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const float4 xi = S.xi[i];
+            const float4 p = lj_tab[S.row[i] + tj];
+            const bool bit = (m8 >> i) & 1u;
+            const float dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
+            const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+            float f;
+            if (!ENERGY && (!PHYS || SAME)) {
+                const bool near = bit & (fabsf(d2 - rl2) < wl);
+                const bool in = bit & !near & (d2 < rl2);
+                band |= static_cast<uint32_t>(near) << i;
+                float ir6, rinv, erfc_ar;
+                const float fa = pair_f<PHYS>(d2, p.z, p.w, xi.w * xj.w, alpha, a2l2e, c2a, ir6, rinv, erfc_ar);
+                f = in ? fa : 0.f;
+            } else {
+                const float r2 = fmaxf(d2, 1e-6f);
+                bool near, in_l, in_c;
+                if (!PHYS || SAME) {
+                    near = bit & (fabsf(r2 - rl2) < wl);
+                    in_l = bit & !near & (r2 < rl2);
+                    in_c = in_l;
+                } else {
+                    near = bit & ((fabsf(r2 - rl2) < wl) | (fabsf(r2 - rcc2) < wc));
+                    const bool use = bit & !near;
+                    in_l = use & (r2 < rl2);
+                    in_c = use & (r2 < rcc2);
+                }
+                band |= static_cast<uint32_t>(near) << i;
+                const float qq = (PHYS && in_c) ? xi.w * xj.w : 0.f;
+                float ir6, rinv, erfc_ar;
+                f = pair_f<PHYS>(r2, in_l ? p.z : 0.f, in_l ? p.w : 0.f, qq, alpha, a2l2e, c2a, ir6, rinv,
+                                 erfc_ar);
+                if (ENERGY) {
+                    el = fmaf(ir6, fmaf(in_l ? p.y : 0.f, ir6, in_l ? -p.x : 0.f), el);
+                    if (PHYS) ec = fmaf(qq * erfc_ar, rinv, ec);
+                    vir = fmaf(f, r2, vir);
+                }
+            }
+            fix[i] = fmaf(-f, dx, fix[i]);
+            fiy[i] = fmaf(-f, dy, fiy[i]);
+            fiz[i] = fmaf(-f, dz, fiz[i]);
+            fjx = fmaf(f, dx, fjx);
+            fjy = fmaf(f, dy, fjy);
+            fjz = fmaf(f, dz, fjz);
+        }
+        if (__any_sync(FULL, band != 0)) {  // pairs at a cutoff (rare): FP64 reference membership
+            const int aj = band ? d.atom_of_slot[js] : -1;
+            while (band) {
+                const int i = __ffs(band) - 1;
+                band &= band - 1;
+                const float4 xi = S.xi[i];
+                const float4 p = lj_tab[S.row[i] + tj];
+                const int ai = S.ai[i];
+                const bool in_l = has_lj && exact_inside(d, ai, aj, L, s->invL, R.rc_lj2);
+                const bool in_c = has_c && exact_inside(d, ai, aj, L, s->invL, R.rc_c2);
+                const float dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
+                const float r2 = fmaxf(fmaf(dz, dz, fmaf(dy, dy, dx * dx)), 1e-6f);
+                const float qq = (PHYS && in_c) ? xi.w * xj.w : 0.f;
+                float ir6, rinv, erfc_ar;
+                const float f = pair_f<PHYS>(r2, in_l ? p.z : 0.f, in_l ? p.w : 0.f, qq, alpha, a2l2e, c2a,
+                                             ir6, rinv, erfc_ar);
+                if (ENERGY) {
+                    el = fmaf(ir6, fmaf(in_l ? p.y : 0.f, ir6, in_l ? -p.x : 0.f), el);
+                    if (PHYS) ec = fmaf(qq * erfc_ar, rinv, ec);
+                    vir = fmaf(f, r2, vir);
+                }
+                const int si = s0 + i;
+                fix_add(d.fnx + si, to_fix(-f * dx, FSCALE, s));
+                fix_add(d.fny + si, to_fix(-f * dy, FSCALE, s));
+                fix_add(d.fnz + si, to_fix(-f * dz, FSCALE, s));
+                fjx = fmaf(f, dx, fjx);
+                fjy = fmaf(f, dy, fjy);
+                fjz = fmaf(f, dz, fjz);
+            }
+        }
+        if (m8) {
+            fix_add(d.fnx + js, to_fix(fjx, FSCALE, s));
+            fix_add(d.fny + js, to_fix(fjy, FSCALE, s));
+            fix_add(d.fnz + js, to_fix(fjz, FSCALE, s));
+        }
+    }
+    const float rx = reduce8(fix, lane), ry = reduce8(fiy, lane), rz = reduce8(fiz, lane);
+    if ((lane & 3) == 0) {
+        const int i = ((lane >> 2) & 1) | ((lane >> 2) & 2) | ((lane >> 2) & 4);
+        if (S.ai[i] >= 0) {
+            const int si = s0 + i;
+            fix_add(d.fnx + si, to_fix(rx, FSCALE, s));
+            fix_add(d.fny + si, to_fix(ry, FSCALE, s));
+            fix_add(d.fnz + si, to_fix(rz, FSCALE, s));
+        }
+    }
+    if (ENERGY) {
+        acc.lj += to_fix(el, ESCALE, s);
+        acc.c += to_fix(ec, ESCALE, s);
+        acc.v += to_fix(vir, ESCALE, s);
+    }
+    __syncwarp();
+}
+
+// Persistent over i-clusters (4 per tile, every replica), taken one per warp
+// from a counter.  The cluster's 8 atoms stay in registers across its rows
+// (up to 128 registers per thread: 2 blocks of 256 threads per SM).
+template <bool PHYS, bool LJS>
+__global__ void __launch_bounds__(256, 2) k_nb8_f32(Dev d) {
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    __shared__ ClusterStage s_stage[8];
+    __shared__ float4 s_lj[LJS ? LJ_SMEM : 1];
+    if (LJS)
+        for (int k = threadIdx.x; k < d.n_lj; k += blockDim.x) s_lj[k] = d.lj32[k];
+    __syncthreads();
+    const float4* lj_tab = LJS ? s_lj : d.lj32;
+    const int total = 4 * d.n_tiles;
+    Acc acc{0, 0, 0};
+    int cur = -1;
+    for (;;) {
+        int w = 0;
+        if (lane == 0) w = atomicAdd(d.nb_work, 1);
+        w = __shfl_sync(FULL, w, 0);
+        if (w >= total) break;
+        const int r = d.tile_rep[w >> 2];
+        RepState* s = d.st + r;
+        if (!s->eval) continue;
+        const int2 job = d.cl_job[w];
+        if (job.y == 0) continue;
+        if (r != cur) {
+            flush_acc(d, cur, acc);
+            cur = r;
+        }
+        const Rep& R = d.rep[r];
+        const bool coul = PHYS && (R.flags & F_COUL_REAL);
+        const bool same = coul && (R.flags & F_LJ) && R.rc_lj2 == R.rc_c2;
+        if (s->want_e) {
+            if (!coul) nb_cluster<false, false, true>(d, R, s, w, job, lane, s_stage[wib], lj_tab, acc);
+            else if (same) nb_cluster<true, true, true>(d, R, s, w, job, lane, s_stage[wib], lj_tab, acc);
+            else nb_cluster<true, false, true>(d, R, s, w, job, lane, s_stage[wib], lj_tab, acc);
+        } else {
+            if (!coul) nb_cluster<false, false, false>(d, R, s, w, job, lane, s_stage[wib], lj_tab, acc);
+            else if (same) nb_cluster<true, true, false>(d, R, s, w, job, lane, s_stage[wib], lj_tab, acc);
+            else nb_cluster<true, false, false>(d, R, s, w, job, lane, s_stage[wib], lj_tab, acc);
+        }
+    }
+    flush_acc(d, cur, acc);
+}
+
 template <bool PHYS>
 __global__ void __launch_bounds__(256) k_nb_f64(Dev d) {
     const int lane = threadIdx.x & 31;
@@ -454,11 +692,21 @@ __global__ void __launch_bounds__(256) k_nb_f64(Dev d) {
 
 }  // namespace
 
-void launch_nonbonded(const Dev& d, bool fp64, bool phys, int n_sm, int blocks_per_sm, cudaStream_t st,
-                      long long* nlaunch) {
+void launch_nonbonded(const Dev& d, bool fp64, bool phys, int n_sm, int blocks_per_sm, int form,
+                      cudaStream_t st, long long* nlaunch) {
     if (fp64) {
         if (phys) k_nb_f64<true><<<n_sm * 8, 256, 0, st>>>(d);
         else k_nb_f64<false><<<n_sm * 8, 256, 0, st>>>(d);
+    } else if (form == NB_CLUSTER8 && d.cl_j) {
+        const int g = n_sm * std::min(std::max(blocks_per_sm, 1), 2);
+        const bool ljs = d.n_lj <= LJ_SMEM;
+        if (phys) {
+            if (ljs) k_nb8_f32<true, true><<<g, 256, 0, st>>>(d);
+            else k_nb8_f32<true, false><<<g, 256, 0, st>>>(d);
+        } else {
+            if (ljs) k_nb8_f32<false, true><<<g, 256, 0, st>>>(d);
+            else k_nb8_f32<false, false><<<g, 256, 0, st>>>(d);
+        }
     } else {
         // persistent: up to the 3 blocks per SM its registers allow; fewer leave
         // room on every SM for the bonded / PME kernels running alongside

@@ -11,13 +11,16 @@ namespace dmd {
 // is set, as one cooperative launch (returns at once when no replica rebuilds).
 void launch_rebuild(const Dev& d, const int* bin_rep, int n_sm, cudaStream_t st, long long* nlaunch);
 
-// k_nonbonded.cu: LJ + real-space Ewald over the chunk list (replicas with `eval`).
+// k_nonbonded.cu: LJ + real-space Ewald over the pair list (replicas with `eval`).
 // Pair energies and virial are summed only for replicas whose `want_e` is set.
-// The mixed-precision kernel is persistent with blocks_per_sm blocks of 256
-// threads per SM (1..3, chosen by the engine's autotuner); results do not depend
-// on it (one warp per chunk, fixed-point sums).
-void launch_nonbonded(const Dev& d, bool fp64, bool phys, int n_sm, int blocks_per_sm, cudaStream_t st,
-                      long long* nlaunch);
+// The mixed-precision kernels are persistent with blocks_per_sm blocks of 256
+// threads per SM (1..3) and come in two forms -- one warp per 32 x 32 chunk,
+// or one warp per 8-atom i-cluster over its rows (needs d.cl_j) -- both chosen
+// by the engine's autotuner; results do not depend on the launch shape (one
+// warp per work item, fixed-point sums).
+enum NbForm { NB_CHUNK32 = 0, NB_CLUSTER8 = 1 };
+void launch_nonbonded(const Dev& d, bool fp64, bool phys, int n_sm, int blocks_per_sm, int form,
+                      cudaStream_t st, long long* nlaunch);
 
 // k_forces.cu
 // bonds, angles, dihedrals and the exclusion correction in one launch

@@ -48,6 +48,7 @@ struct Rep {
     int atom_begin, n_atoms, tile_begin, n_tiles;
     int bin_begin, nvx, nvz;            // sort grid: nvx x nvx columns, nvz slabs
     int chunk_begin, chunk_cap;
+    int cl_begin, cl_cap;               // 8-atom i-cluster lists (mixed precision)
     int n_types, lj_off;
     int flags, profile;
     int thermostat, barostat;
@@ -99,6 +100,7 @@ struct RepState {
     int have_forces;
     int status;
     int n_chunks;
+    int n_cl;             // i-cluster list rows in use
     int want_e;           // the current evaluation's pair energies / virial are read
     int green_ok;         // the cached PME influence function matches the box
     double green_L;       // box edge the cached influence function was made for
@@ -143,6 +145,20 @@ struct Dev {
     int* chunk_itile;
     uint32_t *chunk_j, *chunk_mask;
     int* chunk_prefix;                 // [n_rep + 1] flat chunk numbering
+    // The same pair list regrouped by 8-atom i-cluster (a quarter of an
+    // i-tile: slots 32 I + 8 k .. + 7, cluster index 4 I + k).  A row holds 32
+    // j entries (the chunk entry words) and one 8-bit mask per entry over the
+    // cluster's atoms; a cluster's rows are contiguous, the entries in the
+    // order of its tile's chunks sorted by their first entry word.  Built after
+    // every list build when the arrays exist (mixed precision), not otherwise.
+    int* tile_nch;                     // [n_tiles] chunks of each i-tile
+    int* tile_c0;                      // [n_tiles] first position of its chunk ids in chunk_order
+    int* tile_fill;                    // [n_tiles] scatter counter
+    int* chunk_order;                  // chunk ids grouped by i-tile (chunk capacity)
+    int* chunk_sorted;                 // the same, each tile's ids in canonical order
+    uint32_t* cl_j;                    // [rows][32] entry words
+    uint8_t* cl_m;                     // [rows][32] masks (bit k: cluster atom k)
+    int2* cl_job;                      // [4 n_tiles] per cluster: first row, row count
     void* pme_green;                   // cached PME influence function (mesh_cplx layout, T)
     int* nb_work;                      // pair-kernel chunk counter (reset per evaluation)
     int* build_work;                   // list-build i-tile counter (reset per rebuild)

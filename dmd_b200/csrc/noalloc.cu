@@ -333,7 +333,7 @@ extern "C" int dmdgpu_nonbonded_noalloc(const dmdgpu_nb_params* p, const double*
     if (cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return DMDGPU_ERR_GPU;
     launch_rebuild(d, bin_rep, n_sm, st, &nl);
     if (cudaGetLastError() != cudaSuccess) return DMDGPU_ERR_GPU;
-    launch_nonbonded(d, fp64, phys, n_sm, 2, st, &nl);
+    launch_nonbonded(d, fp64, phys, n_sm, 2, NB_CHUNK32, st, &nl);
     if (cudaGetLastError() != cudaSuccess) return DMDGPU_ERR_GPU;
     k_noalloc_out<<<(n + 255) / 256, 256, 0, st>>>(d, d_fx, d_fy, d_fz, d_energies);
     if (cudaGetLastError() != cudaSuccess) return DMDGPU_ERR_GPU;

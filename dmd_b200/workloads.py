@@ -18,8 +18,8 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from .config import apply_config
 from .core import SimulationConfig
+from .inputs import apply_config
 
 KB = 0.008314462618
 AR_SIGMA, AR_EPS, AR_MASS = 0.3405, 0.996, 39.948
@@ -109,7 +109,7 @@ class Workload:
         return system, self.config_json()
 
     def config(self) -> SimulationConfig:
-        """SimulationConfig equal to SystemBuilder(system).apply_config_json(config)."""
+        """SimulationConfig equal to load_inputs(*self.to_json())."""
         cfg = SimulationConfig()
         n = self.n_atoms
         cfg.box_size = float(self.box)

@@ -119,7 +119,13 @@ typedef struct dmdgpu_options {
     double skin;        /* Verlet skin (nm), PHYS only; REF uses the reference's no-skin list */
     int32_t device;     /* CUDA device ordinal */
     uint64_t rng_seed;  /* PHYS Andersen thermostat stream key */
+    int32_t nb_form;    /* mixed-precision pair-kernel form: DMDGPU_NB_* (results do not
+                           depend on it beyond FP32 summation order) */
 } dmdgpu_options;
+
+#define DMDGPU_NB_AUTO 0      /* chosen by the autotuner (default) */
+#define DMDGPU_NB_CHUNK32 1   /* one warp per 32 x 32 (i-tile, j entries) chunk */
+#define DMDGPU_NB_CLUSTER8 2  /* one warp per 8-atom i-cluster over its 32-entry rows */
 
 /* Scalars of the last force evaluation / current state. */
 typedef struct dmdgpu_scalars {

@@ -26,8 +26,9 @@ KB = 0.008314462618
 
 
 def build(ref: bool = True) -> None:
-    """Compile the oracle (and, when the reference tree exists, oracle/_ref)."""
-    targets = ["oracle"] + (["ref"] if ref else [])
+    """Compile the oracle (and, when the reference tree exists, oracle/_ref: the
+    reference's sources, and the adapter check once libdmdgpu.so is built)."""
+    targets = ["oracle"] + (["ref", "adapter"] if ref else [])
     subprocess.run(["make", "-s", "-C", HERE] + targets, check=True)
 
 

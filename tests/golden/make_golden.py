@@ -24,7 +24,7 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
 from dmd_b200 import workloads as W  # noqa: E402
-from dmd_b200.system import SystemBuilder  # noqa: E402
+from dmd_b200.inputs import load_inputs  # noqa: E402
 from oracle.oracle import Ref, build  # noqa: E402
 
 
@@ -56,7 +56,7 @@ def main():
     ref = Ref()
     for name, w, kind in cases():
         system, config = w.to_json()
-        cfg = SystemBuilder(system).apply_config_json(config).build()
+        cfg = load_inputs(system, config)
         out = {}
         if kind == "components":
             f, e, (pi, pj) = ref.lj(cfg)

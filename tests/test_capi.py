@@ -1,5 +1,6 @@
 """C-ABI library checks that need no GPU: it loads and exports every symbol
-that include/dmdgpu.h declares; host-side config handling mirrors the reference."""
+that include/dmdgpu.h declares; the input reader accepts the reference's
+system.json / config.json formats and refuses malformed documents."""
 import ctypes
 import json
 import os
@@ -7,9 +8,9 @@ import os
 import numpy as np
 import pytest
 
-from dmd_b200 import _capi, config, workloads
+from dmd_b200 import _capi, workloads
 from dmd_b200.core import SimulationConfig
-from dmd_b200.system import SystemBuilder
+from dmd_b200.inputs import InputError, check_config, load_inputs
 
 
 @pytest.fixture(scope="module")
@@ -48,33 +49,58 @@ def test_struct_layout_matches_header(tmp_path):
     assert got == want
 
 
-def test_validate_config_errors():
-    good = json.loads(config.generate_config_template())
-    config.validate_config(good)
+def test_config_check_errors():
+    _, good = workloads.argon_fcc(n_cells=2).to_json()
+    check_config(good)
     bad = json.loads(json.dumps(good))
     del bad["run"]["dt"]
-    with pytest.raises(ValueError, match="Missing required key 'run.dt'"):
-        config.validate_config(bad)
+    with pytest.raises(InputError, match="missing key 'run.dt'"):
+        check_config(bad)
+    bad = json.loads(json.dumps(good))
+    del bad["barostat"]
+    with pytest.raises(InputError, match="missing section 'barostat'"):
+        check_config(bad)
     bad = json.loads(json.dumps(good))
     bad["extra"] = {}
-    with pytest.raises(ValueError, match="Unknown section 'extra'"):
-        config.validate_config(bad)
+    with pytest.raises(InputError, match="unknown section 'extra'"):
+        check_config(bad)
+    bad = json.loads(json.dumps(good))
+    bad["lj"]["shift"] = True
+    with pytest.raises(InputError, match="unknown key 'lj.shift'"):
+        check_config(bad)
     bad = json.loads(json.dumps(good))
     bad["run"]["dt"] = "x"
-    with pytest.raises(ValueError, match="Type mismatch"):
-        config.validate_config(bad)
+    with pytest.raises(InputError, match="'run.dt' must be a float"):
+        check_config(bad)
+    bad = json.loads(json.dumps(good))
+    bad["constraints"]["type"] = "shake"  # no constraint pairs in the argon system
+    sysj, _ = workloads.argon_fcc(n_cells=2).to_json()
+    with pytest.raises(InputError, match="shake"):
+        load_inputs(sysj, bad)
 
 
-def test_system_builder_matches_workload_config():
-    w = workloads.water_box(n_mol=27, box=1.0, seed=1, spacing=0.1)
+@pytest.mark.parametrize("system", ["water", "decane", "rigid_water"])
+def test_reader_matches_workload_config(system, tmp_path):
+    """The reader rebuilds from the reference's input format exactly the
+    configuration the generators build directly (dicts, JSON text and files)."""
+    w = {"water": lambda: workloads.water_box(n_mol=27, box=1.0, seed=1, spacing=0.1),
+         "decane": lambda: workloads.decane_melt(6, 3, impropers=True),
+         "rigid_water": lambda: workloads.water_box(n_mol=27, box=1.0, seed=1, spacing=0.1,
+                                                    rigid=True)}[system]()
     sys_json, cfg_json = w.to_json()
-    b = SystemBuilder(sys_json).apply_config_json(cfg_json).build()
     c = w.config()
-    for k in ("masses", "charges", "pos_x", "atom_types", "lj_sigma", "lj_epsilon", "bond_i",
-              "bond_r0", "angle_k", "angle_theta0"):
-        assert np.array_equal(getattr(b, k), getattr(c, k)), k
-    assert b.excl_i == c.excl_i and b.lj_n_types == 2
-    assert b.coulomb_type == "pme" and b.thermostat.type == "nose-hoover" and b.use_lj
+    (tmp_path / "s.json").write_text(json.dumps(sys_json))
+    for b in (load_inputs(sys_json, cfg_json), load_inputs(json.dumps(sys_json), json.dumps(cfg_json)),
+              load_inputs(str(tmp_path / "s.json"), cfg_json)):
+        for k in SimulationConfig._F64 + SimulationConfig._I32:
+            assert np.array_equal(getattr(b, k), getattr(c, k)), k
+        for k in ("excl_i", "excl_j", "constraint_i", "constraint_j", "constraint_dist"):
+            assert list(getattr(b, k)) == list(getattr(c, k)), k
+        assert b.lj_n_types == c.lj_n_types and b.use_lj
+        for k in ("box_size", "lj_cutoff", "coulomb_type", "coulomb_cutoff", "dt", "seed", "gen_vel",
+                  "constraint_type", "constraint_tolerance"):
+            assert getattr(b, k) == getattr(c, k), k
+        assert b.thermostat.type == c.thermostat.type and b.barostat.tau == c.barostat.tau
 
 
 def test_system_desc_rejects_unknown_thermostat():

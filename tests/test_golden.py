@@ -26,13 +26,9 @@ TOL = {"fp64": 1e-9, "mixed": 1e-5}
 
 
 def _load(case):
-    from dmd_b200.system import SystemBuilder
+    from dmd_b200.inputs import load_inputs
     d = os.path.join(HERE, case)
-    with open(os.path.join(d, "system.json")) as fh:
-        system = json.load(fh)
-    with open(os.path.join(d, "config.json")) as fh:
-        config = json.load(fh)
-    cfg = SystemBuilder(system).apply_config_json(config).build()
+    cfg = load_inputs(os.path.join(d, "system.json"), os.path.join(d, "config.json"))
     exp = dict(np.load(os.path.join(d, "expected.npz")))
     return cfg, exp
 

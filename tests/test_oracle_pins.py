@@ -429,14 +429,14 @@ def test_trajectory_andersen_barostat_bitwise_vs_reference(oracle, ref, pressure
 
 def test_rigid_water_workload_round_trip_and_oracle(oracle):
     """water_box(rigid=True) in the reference's input format: system.json
-    constraints + config.json "shake" read back by SystemBuilder give the same
+    constraints + config.json "shake" read back by load_inputs give the same
     constraints as the direct config; the oracle keeps them through steps."""
-    from dmd_b200.system import SystemBuilder
+    from dmd_b200.inputs import load_inputs
     w = W.water_box(n_mol=64, box=(64 / 33.4) ** (1 / 3), seed=2, spacing=0.1, rigid=True,
                     dt=0.002, thermostat="berendsen")
     c = w.config()
     sysj, cfgj = w.to_json()
-    b = SystemBuilder(sysj).apply_config_json(cfgj).build()
+    b = load_inputs(sysj, cfgj)
     assert c.constraint_type == b.constraint_type == "shake"
     assert c.constraint_tolerance == b.constraint_tolerance == 1e-8
     for k in ("constraint_i", "constraint_j", "constraint_dist"):
