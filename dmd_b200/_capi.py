@@ -73,6 +73,15 @@ class dmdgpu_options(C.Structure):
 NB_FORMS = {"auto": 0, "chunk32": 1, "cluster8": 2}
 
 
+class dmdgpu_frame(C.Structure):
+    _fields_ = [("step", C.c_int64), ("time", C.c_double), ("box", C.c_double), ("n_atoms", C.c_int32),
+                ("x", C.POINTER(C.c_double)), ("y", C.POINTER(C.c_double)), ("z", C.POINTER(C.c_double)),
+                ("vx", C.POINTER(C.c_double)), ("vy", C.POINTER(C.c_double)), ("vz", C.POINTER(C.c_double))]
+
+
+FRAME_FN = C.CFUNCTYPE(None, C.POINTER(dmdgpu_frame), C.c_void_p)
+
+
 class dmdgpu_timing(C.Structure):
     _fields_ = [("step_ms", C.c_double), ("nonbonded_ms", C.c_double), ("pme_ms", C.c_double),
                 ("nonbonded_launches", C.c_int64), ("kernel_launches", C.c_int64)]
@@ -119,6 +128,8 @@ def lib() -> C.CDLL:
         "dmdgpu_stream": (C.c_void_p, [vp]),
         "dmdgpu_step_timed": (C.c_int, [vp, C.c_int32, C.c_int64, C.POINTER(dmdgpu_timing)]),
         "dmdgpu_test_inject": (C.c_int, [vp, C.c_int32]),
+        "dmdgpu_set_frame_writer": (C.c_int, [vp, C.c_int32, FRAME_FN, vp]),
+        "dmdgpu_flush_frames": (C.c_int, [vp]),
         "dmdgpu_last_error": (C.c_char_p, [vp]),
         "dmdgpu_destroy": (None, [vp]),
         "dmdgpu_batch_create": (C.c_int, [C.c_int64, C.POINTER(dmdgpu_options), C.POINTER(vp)]),

@@ -310,6 +310,35 @@ class Engine:
         another slot is admitted or released.  The trajectory is unchanged."""
         self._check(self._lib.dmdgpu_repack(self._h))
 
+    def set_frame_writer(self, interval: int, writer=None):
+        """Export a frame every `interval` steps while run_n / run continue on
+        the device (the reference's run_n writes H5MD frames at
+        trajectory_interval, python/dmd/core.cpp:29-44).  `writer(frame)` gets a
+        dict with step, time, box, positions and velocities (N x 3 copies); it
+        is called from a CUDA host-callback thread, in step order, and must not
+        call back into this engine.  `interval` <= 0 or writer None turns export
+        off.  Frames still in flight when a run returns are delivered by
+        flush_frames() (or close())."""
+        if interval <= 0 or writer is None:
+            self._frame_cb = None
+            self._check(self._lib.dmdgpu_set_frame_writer(self._h, 0, _capi.FRAME_FN(), None))
+            return
+
+        def deliver(fp, _user):
+            f = fp.contents
+            n = f.n_atoms
+            arr = lambda p: np.ctypeslib.as_array(p, shape=(n,)).copy()  # noqa: E731
+            writer({"step": int(f.step), "time": float(f.time), "box": float(f.box),
+                    "positions": np.stack([arr(f.x), arr(f.y), arr(f.z)], 1),
+                    "velocities": np.stack([arr(f.vx), arr(f.vy), arr(f.vz)], 1)})
+
+        self._frame_cb = _capi.FRAME_FN(deliver)  # kept alive while export is on
+        self._check(self._lib.dmdgpu_set_frame_writer(self._h, int(interval), self._frame_cb, None))
+
+    def flush_frames(self):
+        """Wait until every exported frame has been handed to the writer."""
+        self._check(self._lib.dmdgpu_flush_frames(self._h))
+
     def test_inject(self, what: str):
         """Test-only, host-side fault injection for the failure paths:
         "barrier_timeout" (the next list build's bounded grid-barrier waits run

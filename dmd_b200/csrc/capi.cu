@@ -287,6 +287,18 @@ int dmdgpu_step_timed(dmdgpu_ctx* c, int32_t n, int64_t flush_bytes, dmdgpu_timi
     return rc ? ctx_fail(c, rc) : DMDGPU_OK;
 }
 
+int dmdgpu_set_frame_writer(dmdgpu_ctx* c, int32_t interval, dmdgpu_frame_fn fn, void* user) {
+    if (!c || !c->b) return DMDGPU_ERR_INVALID;
+    int rc = c->b->set_frame_writer(interval, fn, user);
+    return rc ? ctx_fail(c, rc) : DMDGPU_OK;
+}
+
+int dmdgpu_flush_frames(dmdgpu_ctx* c) {
+    if (!c || !c->b) return DMDGPU_ERR_INVALID;
+    int rc = c->b->flush_frames();
+    return rc ? ctx_fail(c, rc) : DMDGPU_OK;
+}
+
 int dmdgpu_test_inject(dmdgpu_ctx* c, int32_t what) {
     if (!c || !c->b) return DMDGPU_ERR_INVALID;
     int rc = c->b->inject(what);

@@ -118,6 +118,7 @@ Batch::Batch(const dmdgpu_options& opt, long long budget) : opt_(opt), budget_(b
 
 Batch::~Batch() {
     cudaSetDevice(device_);
+    free_frames();
     free_device();
     if (flush_buf_) cudaFree(flush_buf_);
     for (cudaEvent_t e : ev_pool_) cudaEventDestroy(e);
@@ -1345,9 +1346,126 @@ int Batch::step(int n) {
         if (rc) return rc;
     }
     if (order_.empty()) return DMDGPU_OK;
+    if (frame_fn_ && frame_interval_ > 0 && order_.size() == 1) {
+        // steps in runs that end on frame steps, a frame issued after each
+        if (!st_fresh_) {
+            CK(cudaMemcpyAsync(h_st_, d_st_, sizeof(RepState), cudaMemcpyDeviceToHost, stream_));
+            CK(cudaStreamSynchronize(stream_));
+            st_fresh_ = true;
+        }
+        long long s = h_st_[0].step;
+        const long long I = frame_interval_;
+        int left = n;
+        while (left > 0) {
+            const long long next = (s / I + 1) * I;
+            const int k = static_cast<int>(std::min<long long>(left, next - s));
+            int rc = run_steps(k);
+            if (rc) return rc;
+            s += k;
+            left -= k;
+            if (s == next) {
+                rc = enqueue_frame();
+                if (rc) return rc;
+            }
+        }
+        return sync_status();
+    }
     int rc = run_steps(n);
     if (rc) return rc;
     return sync_status();
+}
+
+// ---------------------------------------------------------------------------
+// Trajectory frames.  The snapshot kernel reads the state the last step left
+// (positions, velocities with the pending thermostat scale, step, time, box)
+// and changes nothing, so exporting leaves the trajectory bit for bit as it is.
+// Slot k is reused only after the copy stream has delivered its previous
+// frame (frame_done_), so the main stream waits only when the writer is
+// DMDGPU_FRAME_SLOTS frames behind.
+// ---------------------------------------------------------------------------
+int Batch::set_frame_writer(int interval, dmdgpu_frame_fn fn, void* user) {
+    CK(cudaSetDevice(device_));
+    if (!packed_) {
+        int rc = pack();
+        if (rc) return rc;
+    }
+    free_frames();
+    if (interval <= 0 || !fn) return DMDGPU_OK;
+    if (order_.size() != 1) return fail(DMDGPU_ERR_INVALID, "frames are exported for a single-system context");
+    frame_n_ = reps_[order_[0]]->sys.n;
+    const size_t bytes = sizeof(double) * (3 + 6 * static_cast<size_t>(frame_n_));
+    CK(cudaStreamCreateWithFlags(&copy_stream_, cudaStreamNonBlocking));
+    for (int k = 0; k < DMDGPU_FRAME_SLOTS; ++k) {
+        CK(cudaMalloc(&frame_dev_[k], bytes));
+        CK(cudaMallocHost(&frame_host_[k], bytes));
+        CK(cudaEventCreateWithFlags(&frame_snap_[k], cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&frame_done_[k], cudaEventDisableTiming));
+        CK(cudaEventRecord(frame_done_[k], copy_stream_));
+        frame_slot_[k] = FrameSlot{this, k};
+    }
+    frame_interval_ = interval;
+    frame_fn_ = fn;
+    frame_user_ = user;
+    frame_count_ = 0;
+    return DMDGPU_OK;
+}
+
+int Batch::flush_frames() {
+    if (copy_stream_) CK(cudaStreamSynchronize(copy_stream_));
+    return DMDGPU_OK;
+}
+
+void Batch::free_frames() {
+    if (copy_stream_) cudaStreamSynchronize(copy_stream_);
+    for (int k = 0; k < DMDGPU_FRAME_SLOTS; ++k) {
+        if (frame_dev_[k]) cudaFree(frame_dev_[k]);
+        if (frame_host_[k]) cudaFreeHost(frame_host_[k]);
+        if (frame_snap_[k]) cudaEventDestroy(frame_snap_[k]);
+        if (frame_done_[k]) cudaEventDestroy(frame_done_[k]);
+        frame_dev_[k] = nullptr;
+        frame_host_[k] = nullptr;
+        frame_snap_[k] = nullptr;
+        frame_done_[k] = nullptr;
+    }
+    if (copy_stream_) cudaStreamDestroy(copy_stream_);
+    copy_stream_ = nullptr;
+    frame_fn_ = nullptr;
+    frame_interval_ = 0;
+}
+
+int Batch::enqueue_frame() {
+    const int k = static_cast<int>(frame_count_ % DMDGPU_FRAME_SLOTS);
+    const size_t bytes = sizeof(double) * (3 + 6 * static_cast<size_t>(frame_n_));
+    CK(cudaStreamWaitEvent(stream_, frame_done_[k], 0));
+    launch_frame_snapshot(dev_, 0, frame_n_, frame_dev_[k], stream_, &launches_);
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(frame_snap_[k], stream_));
+    CK(cudaStreamWaitEvent(copy_stream_, frame_snap_[k], 0));
+    CK(cudaMemcpyAsync(frame_host_[k], frame_dev_[k], bytes, cudaMemcpyDeviceToHost, copy_stream_));
+    CK(cudaLaunchHostFunc(copy_stream_, &Batch::deliver_frame, &frame_slot_[k]));
+    CK(cudaEventRecord(frame_done_[k], copy_stream_));
+    ++frame_count_;
+    st_fresh_ = false;
+    return DMDGPU_OK;
+}
+
+void CUDART_CB Batch::deliver_frame(void* p) {
+    const FrameSlot* fs = static_cast<const FrameSlot*>(p);
+    const Batch* b = fs->self;
+    const double* h = b->frame_host_[fs->index];
+    const int n = b->frame_n_;
+    dmdgpu_frame f;
+    f.step = static_cast<int64_t>(h[0]);
+    f.time = h[1];
+    f.box = h[2];
+    f.n_atoms = n;
+    f.x = h + 3;
+    f.y = h + 3 + n;
+    f.z = h + 3 + 2 * n;
+    f.vx = h + 3 + 3 * n;
+    f.vy = h + 3 + 4 * n;
+    f.vz = h + 3 + 5 * n;
+    b->frame_fn_(&f, b->frame_user_);
 }
 
 cudaEvent_t Batch::next_event() {
@@ -1485,8 +1603,8 @@ int Batch::active() const {
 
 // Failure-path test hooks.  Both act on the host: they only change what the
 // next list build is given, and every wait they make run out is bounded.
-//  BARRIER_TIMEOUT: the grid barrier's arrival counter starts far above the
-//    block count, so no arrival completes it; each wait gives up after 20 ms,
+//  BARRIER_TIMEOUT: the grid barrier waits for one arrival more than the grid
+//    has blocks, so no arrival completes it; each wait gives up after 20 ms,
 //    records ST_TIMEOUT and the blocks leave the kernel.  The forces of that
 //    step come from the previous (still intact) list.
 //  LIST_CAPACITY: every replica's chunk capacity becomes 1, so the next build
@@ -1501,8 +1619,7 @@ int Batch::inject(int what) {
     CK(cudaStreamSynchronize(stream_));
     st_fresh_ = false;
     if (what == DMDGPU_INJECT_BARRIER_TIMEOUT) {
-        const unsigned poison = 0x40000000u;
-        CK(cudaMemcpy(dev_.grid_bar, &poison, 4, cudaMemcpyHostToDevice));
+        dev_.bar_extra = 1;
         dev_.bar_limit_ns = 20000000ull;
     } else if (what == DMDGPU_INJECT_LIST_CAPACITY) {
         for (size_t k = 0; k < order_.size(); ++k) {

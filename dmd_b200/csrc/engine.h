@@ -100,6 +100,9 @@ class Batch {
     int poll(int32_t* slots, int cap, int* n_done);
     // Host-side fault injection for the failure-path tests (DMDGPU_INJECT_*).
     int inject(int what);
+    // Trajectory frames of a single-system table (dmdgpu_set_frame_writer).
+    int set_frame_writer(int interval, dmdgpu_frame_fn fn, void* user);
+    int flush_frames();
 
     long long used_bytes() const { return used_bytes_; }
     long long launches() const { return launches_; }
@@ -170,6 +173,27 @@ class Batch {
     void* flush_buf_ = nullptr;
     long long flush_bytes_ = 0;
     void record(cudaEvent_t e, cudaStream_t st);
+    // frame export: a device snapshot on the main stream into one of
+    // DMDGPU_FRAME_SLOTS staging buffers, then a copy to pinned host memory and
+    // the writer call on copy_stream_
+    struct FrameSlot {
+        Batch* self;
+        int index;
+    };
+    int enqueue_frame();
+    void free_frames();
+    static void CUDART_CB deliver_frame(void* p);
+    int frame_interval_ = 0;
+    dmdgpu_frame_fn frame_fn_ = nullptr;
+    void* frame_user_ = nullptr;
+    int frame_n_ = 0;
+    cudaStream_t copy_stream_ = nullptr;
+    double* frame_dev_[DMDGPU_FRAME_SLOTS] = {};
+    double* frame_host_[DMDGPU_FRAME_SLOTS] = {};
+    cudaEvent_t frame_snap_[DMDGPU_FRAME_SLOTS] = {};
+    cudaEvent_t frame_done_[DMDGPU_FRAME_SLOTS] = {};
+    FrameSlot frame_slot_[DMDGPU_FRAME_SLOTS] = {};
+    long long frame_count_ = 0;
     cudaEvent_t next_event();
     std::string err_;
     std::vector<int> finished_;

@@ -558,6 +558,31 @@ __global__ void k_finalize_v(Dev d) {
     d.vz[a] = __dmul_rn(d.vz[a], lam);
 }
 
+// One replica's frame into a device staging buffer, without changing any
+// state: [step, time, box, x[n], y[n], z[n], vx[n], vy[n], vz[n]], the
+// velocities with the pending thermostat scale applied as k_finalize_v would.
+__global__ void k_frame_snapshot(Dev d, int r, double* out) {
+    const Rep& R = d.rep[r];
+    const RepState& s = d.st[r];
+    const int n = R.n_atoms;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) {
+        out[0] = static_cast<double>(s.step);
+        out[1] = s.time;
+        out[2] = s.L;
+    }
+    if (i >= n) return;
+    const int a = R.atom_begin + i;
+    const double lam = s.vscale;
+    double* o = out + 3;
+    o[i] = d.x[a];
+    o[n + i] = d.y[a];
+    o[2 * n + i] = d.z[a];
+    o[3 * n + i] = lam == 1.0 ? d.vx[a] : __dmul_rn(d.vx[a], lam);
+    o[4 * n + i] = lam == 1.0 ? d.vy[a] : __dmul_rn(d.vy[a], lam);
+    o[5 * n + i] = lam == 1.0 ? d.vz[a] : __dmul_rn(d.vz[a], lam);
+}
+
 __global__ void k_finalize_reset(Dev d) {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r < d.n_rep) d.st[r].vscale = 1.0;
@@ -616,6 +641,10 @@ void launch_finalize_velocities(const Dev& d, cudaStream_t st, long long* n) {
     k_finalize_v<<<(d.n_atoms + 255) / 256, 256, 0, st>>>(d);
     k_finalize_reset<<<(d.n_rep + 127) / 128, 128, 0, st>>>(d);
     *n += 2;
+}
+void launch_frame_snapshot(const Dev& d, int r, int n_atoms, double* out, cudaStream_t st, long long* n) {
+    k_frame_snapshot<<<(n_atoms + 255) / 256, 256, 0, st>>>(d, r, out);
+    ++*n;
 }
 void launch_energy_reduce(const Dev& d, cudaStream_t st, long long* n) {
     k_energy_reduce<<<d.n_rep, 256, 0, st>>>(d);

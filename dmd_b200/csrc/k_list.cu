@@ -1404,7 +1404,7 @@ __device__ bool grid_barrier(const Dev& d) {
         ok = 1;
         const unsigned gen = ld_acquire(bar + 1);
         __threadfence();
-        if (atomicAdd(bar, 1u) == gridDim.x - 1) {
+        if (atomicAdd(bar, 1u) == gridDim.x - 1 + d.bar_extra) {
             bar[0] = 0;
             __threadfence();
             st_release(bar + 1, gen + 1);

@@ -45,6 +45,9 @@ void launch_replica_update(const Dev& d, cudaStream_t st, long long* nlaunch);
 void launch_apply_scale(const Dev& d, bool fp64, cudaStream_t st, long long* nlaunch);
 void launch_finalize_velocities(const Dev& d, cudaStream_t st, long long* nlaunch);
 void launch_energy_reduce(const Dev& d, cudaStream_t st, long long* nlaunch);
+// replica r's frame (step, time, box, positions, velocities) into `out`
+// (3 + 6 n_atoms doubles), state unchanged
+void launch_frame_snapshot(const Dev& d, int r, int n_atoms, double* out, cudaStream_t st, long long* nlaunch);
 void launch_write_mirror(const Dev& d, bool fp64, cudaStream_t st, long long* nlaunch);
 
 }  // namespace dmd

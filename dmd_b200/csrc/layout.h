@@ -166,6 +166,8 @@ struct Dev {
                                        // atoms, sort cells and tiles
     unsigned* grid_bar;                // [2] rebuild grid barrier: arrivals, generation
     unsigned long long bar_limit_ns;   // a barrier wait gives up after this long (0: one second)
+    unsigned bar_extra;                // arrivals a barrier needs beyond the grid's blocks (0;
+                                       // only the failure-path test hook sets it)
     // bonded terms (global atom indices)
     int n_bonds, n_angles, n_dih, n_imp;
     const int2* bond_ij;

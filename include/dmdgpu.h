@@ -236,6 +236,38 @@ typedef struct dmdgpu_timing {
  * the timed intervals) so each step starts with a cold L2. */
 int dmdgpu_step_timed(dmdgpu_ctx *ctx, int32_t n_steps, int64_t l2_flush_bytes, dmdgpu_timing *out);
 
+/* Trajectory frames, exported while the run continues.  Replaces the frame
+ * writing inside the reference's run loop (EngineWrapper::run_n,
+ * python/dmd/core.cpp:29-44, and SimulationEngine::run,
+ * src/sim/simulation_engine.cpp:88-104): after every step whose step counter
+ * is a multiple of `interval`, the step, time, box and the positions and
+ * velocities of that step (what H5MDWriter::write_frame,
+ * src/trajectory/h5md_writer.cpp:191, records) are copied on the device into
+ * one of a few staging buffers, then to pinned host memory on a copy stream
+ * while the next steps compute, and `fn` is called with them in step order.
+ * The run waits for the writer only when it falls DMDGPU_FRAME_SLOTS frames
+ * behind.
+ *
+ * `fn` runs on a CUDA host-callback thread: it must not call CUDA or any
+ * dmdgpu_ function, and the arrays it receives are valid only during the
+ * call (copy what you keep).  dmdgpu_step / dmdgpu_run return without
+ * waiting for frames still in flight; dmdgpu_flush_frames waits for them (so
+ * does dmdgpu_destroy).  interval <= 0 or fn == NULL turns export off.
+ * Exporting changes no bit of the trajectory.  No counterpart in the
+ * reference for the callback itself: the reference writes HDF5 inline. */
+#define DMDGPU_FRAME_SLOTS 4
+typedef struct dmdgpu_frame {
+    int64_t step;
+    double time;                 /* ps */
+    double box;                  /* cubic box edge (nm) */
+    int32_t n_atoms;
+    const double *x, *y, *z;     /* positions (nm), unwrapped as the engine keeps them */
+    const double *vx, *vy, *vz;  /* velocities (nm/ps) */
+} dmdgpu_frame;
+typedef void (*dmdgpu_frame_fn)(const dmdgpu_frame *frame, void *user);
+int dmdgpu_set_frame_writer(dmdgpu_ctx *ctx, int32_t interval, dmdgpu_frame_fn fn, void *user);
+int dmdgpu_flush_frames(dmdgpu_ctx *ctx);
+
 /* Test-only fault injection, done on the host; no counterpart in the reference.
  * It changes only what the next list build is given, so the failure paths can
  * be exercised without faulting, trapping or hanging the GPU:

@@ -32,7 +32,8 @@ def test_struct_layout_matches_header(tmp_path):
     import subprocess
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "dmdgpu.h"', "int main(void){"]
-    for cls in (_capi.dmdgpu_system, _capi.dmdgpu_options, _capi.dmdgpu_scalars, _capi.dmdgpu_timing):
+    for cls in (_capi.dmdgpu_system, _capi.dmdgpu_options, _capi.dmdgpu_scalars, _capi.dmdgpu_timing,
+                _capi.dmdgpu_frame):
         lines.append(f'printf("%zu\\n", sizeof({cls.__name__}));')
         for f in cls._fields_:
             lines.append(f'printf("%zu\\n", offsetof({cls.__name__}, {f[0]}));')
@@ -43,7 +44,8 @@ def test_struct_layout_matches_header(tmp_path):
     subprocess.run(["gcc", "-I", os.path.join(root, "include"), str(src), "-o", str(exe)], check=True)
     got = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
     want = []
-    for cls in (_capi.dmdgpu_system, _capi.dmdgpu_options, _capi.dmdgpu_scalars, _capi.dmdgpu_timing):
+    for cls in (_capi.dmdgpu_system, _capi.dmdgpu_options, _capi.dmdgpu_scalars, _capi.dmdgpu_timing,
+                _capi.dmdgpu_frame):
         want.append(ctypes.sizeof(cls))
         want.extend(getattr(cls, f[0]).offset for f in cls._fields_)
     assert got == want
