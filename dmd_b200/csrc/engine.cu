@@ -84,7 +84,7 @@ std::map<TuneKey, TuneChoice> g_tune;
 constexpr int kTuneSteps = 6;               // timed steps per candidate
 constexpr TuneChoice kTuneCand[] = {{NB_CLUSTER8, 1}, {NB_CLUSTER8, 2}, {NB_CHUNK32, 2}, {NB_CHUNK32, 3}};
 
-// forced: the caller's dmdgpu_options.nb_form (0: the tuner picks the form too)
+// forced: the caller's dmdgpu_options.nb_form (0: the default form)
 TuneKey tune_key(int device, bool fp64, bool pme, long long n_atoms, int forced) {
     int b = 0;
     while ((1LL << (2 * b + 2)) <= n_atoms) ++b;
@@ -1016,7 +1016,7 @@ int Batch::pack() {
         const int forced = forced_form(opt_.nb_form);
         auto it = g_tune.find(tune_key(device_, fp64_, any_pme_, dev_.n_atoms, opt_.nb_form));
         tuned_ = fp64_ || it != g_tune.end();
-        nb_form_ = (it != g_tune.end()) ? it->second.form : (forced >= 0 ? forced : NB_CLUSTER8);
+        nb_form_ = fp64_ ? NB_CHUNK32 : (forced >= 0 ? forced : NB_CLUSTER8);
         nb_blocks_per_sm_ = (it != g_tune.end()) ? it->second.bps : ((any_pme_ || nb_form_ == NB_CLUSTER8) ? 2 : 3);
     }
     packed_ = true;
@@ -1222,10 +1222,15 @@ int Batch::run_steps(int n) {
 // only when the call has enough steps to spare.
 int Batch::autotune(int max_steps, int* used) {
     *used = 0;
+    // The form itself is not tuned: its FP32 summation order differs, so a
+    // choice made by timing would make results differ from run to run and
+    // between a system alone and the same system in a batch.  Only the launch
+    // shape, which changes no result bit, is chosen by measurement.
     const int forced = forced_form(opt_.nb_form);
+    const int form = fp64_ ? NB_CHUNK32 : (forced >= 0 ? forced : NB_CLUSTER8);
     std::vector<TuneChoice> cand;
     for (const TuneChoice& c : kTuneCand)
-        if (forced < 0 || c.form == forced) cand.push_back(c);
+        if (c.form == form) cand.push_back(c);
     const int n_cand = static_cast<int>(cand.size());
     if (max_steps < n_cand * kTuneSteps) return DMDGPU_OK;
     std::vector<cudaEvent_t> ev(kTuneSteps + 1);

@@ -1516,7 +1516,7 @@ __global__ void __launch_bounds__(NT_B, 4) k_rebuild(Dev d, const int* bin_rep) 
     if (!d.cl_j) return;  // FP64 tables keep the chunk list only
     if (!grid_barrier(d)) return;
     // R8: chunks per rebuilt i-tile
-    const int* pc = pt + 2 * (d.n_rep + 1);  // build_prefix[3], written by R7
+    const int* pc = pt + (d.n_rep + 1);  // build_prefix[3] (pa, pb, pt, pc), written by R7
     const int n_c = pc[d.n_rep];
     for (int w = gtid; w < n_c; w += gthreads) {
         const int r = chunk_replica(pc, d.n_rep, w);
