@@ -264,11 +264,19 @@ __device__ __forceinline__ int wrap_mesh(int g, int K) {
     return g - ((g >= K) ? K : 0);
 }
 
-__device__ __forceinline__ void mesh_coord(double x, double invL, int K, int& m0, double& u) {
+// The first stencil index m0 always lies in [-1, K - 1] (u = K when f - floor(f)
+// rounds up to 1): a coordinate that is not finite (a NaN or infinite
+// position) gives m0 = -1 and a non-finite u (its weights are then NaN and the
+// caller flags the status word), so no float-to-integer conversion of a
+// non-finite value ever becomes an index.  Returns whether u is finite.
+__device__ __forceinline__ bool mesh_coord(double x, double invL, int K, int& m0, double& u) {
     double f = x * invL;
     f -= floor(f);
     u = f * K;
-    m0 = static_cast<int>(floor(u)) - 1;
+    const double fl = floor(u);
+    const bool ok = fl >= 0.0 && fl <= static_cast<double>(K);
+    m0 = ok ? static_cast<int>(fl) - 1 : -1;
+    return ok;
 }
 
 // 16 threads per atom: thread (iy, ix) = (sub >> 2, sub & 3) adds the atom's
@@ -291,9 +299,9 @@ __global__ void k_pme_spread(Dev d) {
     const int ix = threadIdx.x & 3, iy = (threadIdx.x >> 2) & 3;
     int m0[3];
     double u[3];
-    mesh_coord(d.x[a], s->invL, K, m0[0], u[0]);
-    mesh_coord(d.y[a], s->invL, K, m0[1], u[1]);
-    mesh_coord(d.z[a], s->invL, K, m0[2], u[2]);
+    const bool fin = mesh_coord(d.x[a], s->invL, K, m0[0], u[0]) & mesh_coord(d.y[a], s->invL, K, m0[1], u[1]) &
+                     mesh_coord(d.z[a], s->invL, K, m0[2], u[2]);
+    if (!fin && (threadIdx.x & 15) == 0) set_status(s, ST_NAN);
     const T wx = theta4<T>((T)(u[0] - (m0[0] + ix)));
     const T wy = theta4<T>((T)(u[1] - (m0[1] + iy)));
     long long* mesh = d.mesh_fix + R.mesh_fix_off;

@@ -25,13 +25,16 @@ __device__ __forceinline__ void bin_atom(const Dev& d, int a) {
     const double L = s->L;
     double p[3] = {d.x[a], d.y[a], d.z[a]};
     int im[3], v[3];
+    // a position that is not finite is reported and binned as image 0, cell 0:
+    // every float-to-integer conversion below takes a clamped, finite value
+    if (!(isfinite(p[0]) && isfinite(p[1]) && isfinite(p[2]))) set_status(s, ST_NAN);
     for (int k = 0; k < 3; ++k) {
         const int nk = (k < 2) ? R.nvx : R.nvz;
         double f = floor(p[k] / L);
-        im[k] = static_cast<int>(f);
+        im[k] = fabs(f) < 1e9 ? static_cast<int>(f) : 0;
         double w = p[k] - f * L;
-        int c = static_cast<int>(w / L * nk);
-        v[k] = min(max(c, 0), nk - 1);
+        const double cw = w / L * nk;
+        v[k] = cw >= 0.0 ? (cw < nk ? static_cast<int>(cw) : nk - 1) : 0;
     }
     d.imgx[a] = im[0];
     d.imgy[a] = im[1];
