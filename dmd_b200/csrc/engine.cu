@@ -120,6 +120,11 @@ Batch::~Batch() {
     cudaSetDevice(device_);
     free_frames();
     free_device();
+    for (auto& kv : plans_) {
+        cufftDestroy(kv.second.first);
+        cufftDestroy(kv.second.second);
+    }
+    plans_.clear();
     if (flush_buf_) cudaFree(flush_buf_);
     for (cudaEvent_t e : ev_pool_) cudaEventDestroy(e);
     if (ev_fork_) cudaEventDestroy(ev_fork_);
@@ -134,11 +139,9 @@ void Batch::free_device() {
     if (stream_) cudaStreamSynchronize(stream_);
     if (graph_) cudaGraphExecDestroy(graph_);
     graph_ = nullptr;
-    for (auto& kv : plans_) {
-        cufftDestroy(kv.second.first);
-        cufftDestroy(kv.second.second);
-    }
-    plans_.clear();
+    // cuFFT plans depend only on the mesh size: they are kept across table
+    // rebuilds (an admission or release rebuilds the table) and destroyed with
+    // the batch
     arena_.reset();
     if (h_st_) cudaFreeHost(h_st_);
     h_st_ = nullptr;
@@ -1014,7 +1017,24 @@ int Batch::pack() {
     {
         std::lock_guard<std::mutex> lk(g_tune_mu);
         const int forced = forced_form(opt_.nb_form);
-        auto it = g_tune.find(tune_key(device_, fp64_, any_pme_, dev_.n_atoms, opt_.nb_form));
+        const TuneKey key = tune_key(device_, fp64_, any_pme_, dev_.n_atoms, opt_.nb_form);
+        auto it = g_tune.find(key);
+        if (it == g_tune.end()) {
+            // a table of a size not tuned yet takes the shape tuned for the
+            // nearest size of the same kind, so a serving loop whose table size
+            // changes with every admission tunes once, not at every rebuild
+            int best = 1 << 30;
+            for (auto jt = g_tune.begin(); jt != g_tune.end(); ++jt) {
+                const TuneKey& k = jt->first;
+                if (k.device != key.device || k.fp64 != key.fp64 || k.pme != key.pme || k.forced != key.forced)
+                    continue;
+                const int dist = std::abs(k.bucket - key.bucket);
+                if (dist < best) {
+                    best = dist;
+                    it = jt;
+                }
+            }
+        }
         tuned_ = fp64_ || it != g_tune.end();
         nb_form_ = fp64_ ? NB_CHUNK32 : (forced >= 0 ? forced : NB_CLUSTER8);
         nb_blocks_per_sm_ = (it != g_tune.end()) ? it->second.bps : ((any_pme_ || nb_form_ == NB_CLUSTER8) ? 2 : 3);
