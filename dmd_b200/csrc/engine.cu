@@ -91,11 +91,19 @@ TuneKey tune_key(int device, bool fp64, bool pme, long long n_atoms, int forced)
     return TuneKey{device, fp64 ? 1 : 0, pme ? 1 : 0, b, forced};
 }
 
-// DMDGPU_NB_* of the options -> NbForm, or -1 for the autotuner's choice
+// DMDGPU_NB_* of the options -> NbForm, or -1 for the default form
 int forced_form(int nb_form) {
     return nb_form == DMDGPU_NB_CHUNK32 ? NB_CHUNK32 : (nb_form == DMDGPU_NB_CLUSTER8 ? NB_CLUSTER8 : -1);
 }
 }  // namespace
+
+// The 8-atom i-cluster form runs only when the options ask for it: measured on
+// one B200, its pair kernel is faster alone (water 30k: 62.7 vs 66.8 us per
+// launch in the step) but it holds every register of its SMs, so the SPME
+// chain no longer runs beside it, and regrouping the list adds ~70 us to each
+// rebuild; the 32-wide chunk form is the default.  The cluster rows and their
+// bookkeeping are allocated (and built) only for that form.
+bool Batch::uses_clusters() const { return !fp64_ && forced_form(opt_.nb_form) == NB_CLUSTER8; }
 
 Batch::Batch(const dmdgpu_options& opt, long long budget) : opt_(opt), budget_(budget) {
     fp64_ = opt.precision == DMDGPU_PRECISION_FP64;
@@ -257,7 +265,7 @@ long long Batch::footprint(const HostSystem& s) const {
     // mixed precision: the list regrouped by 8-atom i-cluster (rows of 32 entry
     // words and 32 byte masks, up to 4 per chunk and 4 per tile) and its
     // per-tile bookkeeping
-    if (!fp64_) b += (4 * chunks + 4 * tiles) * (32 * 4 + 32) + chunks * 8 + tiles * (12 + 4 * 8);
+    if (uses_clusters()) b += (4 * chunks + 4 * tiles) * (32 * 4 + 32) + chunks * 8 + tiles * (12 + 4 * 8);
     b += static_cast<long long>(s.ci.size()) * (8 + 8 + 8);  // constraints and their groups
     if (s.coulomb_type == 1) {
         long long K = std::max(8, static_cast<int>(s.box / s.spacing + 0.5));
@@ -560,7 +568,7 @@ int Batch::pack() {
         // i-cluster rows: each of a tile's chunks adds at most 32 entries to each
         // of its four clusters, so 4 rows per chunk plus one partial row per
         // cluster always suffice
-        P.cl_cap = fp64_ ? 0 : static_cast<int>(std::min<long long>(4LL * P.chunk_cap + 4LL * P.n_tiles, INT32_MAX / 64));
+        P.cl_cap = uses_clusters() ? static_cast<int>(std::min<long long>(4LL * P.chunk_cap + 4LL * P.n_tiles, INT32_MAX / 64)) : 0;
         P.cl_begin = static_cast<int>(n_cl);
         n_cl += P.cl_cap;
         n_atoms += s.n;
@@ -675,7 +683,7 @@ int Batch::pack() {
         d.build_work = d.chunk_prefix + R + 2;
         d.grid_bar = A.alloc<unsigned>(2);
         d.build_prefix = A.alloc<int>(4 * (R + 1));
-        if (!fp64_) {
+        if (uses_clusters()) {
             d.tile_nch = A.alloc<int>(n_tiles);
             d.tile_c0 = A.alloc<int>(n_tiles);
             d.tile_fill = A.alloc<int>(n_tiles);
@@ -1016,7 +1024,6 @@ int Batch::pack() {
     }
     {
         std::lock_guard<std::mutex> lk(g_tune_mu);
-        const int forced = forced_form(opt_.nb_form);
         const TuneKey key = tune_key(device_, fp64_, any_pme_, dev_.n_atoms, opt_.nb_form);
         auto it = g_tune.find(key);
         if (it == g_tune.end()) {
@@ -1036,7 +1043,7 @@ int Batch::pack() {
             }
         }
         tuned_ = fp64_ || it != g_tune.end();
-        nb_form_ = fp64_ ? NB_CHUNK32 : (forced >= 0 ? forced : NB_CLUSTER8);
+        nb_form_ = uses_clusters() ? NB_CLUSTER8 : NB_CHUNK32;
         nb_blocks_per_sm_ = (it != g_tune.end()) ? it->second.bps : ((any_pme_ || nb_form_ == NB_CLUSTER8) ? 2 : 3);
     }
     packed_ = true;
@@ -1246,8 +1253,7 @@ int Batch::autotune(int max_steps, int* used) {
     // choice made by timing would make results differ from run to run and
     // between a system alone and the same system in a batch.  Only the launch
     // shape, which changes no result bit, is chosen by measurement.
-    const int forced = forced_form(opt_.nb_form);
-    const int form = fp64_ ? NB_CHUNK32 : (forced >= 0 ? forced : NB_CLUSTER8);
+    const int form = uses_clusters() ? NB_CLUSTER8 : NB_CHUNK32;
     std::vector<TuneChoice> cand;
     for (const TuneChoice& c : kTuneCand)
         if (c.form == form) cand.push_back(c);

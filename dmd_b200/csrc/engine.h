@@ -100,6 +100,7 @@ class Batch {
     int poll(int32_t* slots, int cap, int* n_done);
     // Host-side fault injection for the failure-path tests (DMDGPU_INJECT_*).
     int inject(int what);
+    bool uses_clusters() const;  // the options select the 8-atom i-cluster pair form
     // Trajectory frames of a single-system table (dmdgpu_set_frame_writer).
     int set_frame_writer(int interval, dmdgpu_frame_fn fn, void* user);
     int flush_frames();

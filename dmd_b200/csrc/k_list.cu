@@ -1290,17 +1290,15 @@ __device__ __forceinline__ void tile_scan_replica(const Dev& d, int r) {
     __syncthreads();
 }
 
-// R11: one warp per rebuilt i-tile: canonical chunk order, then the tile's
-// four cluster lists.
-__device__ __forceinline__ void cluster_tile(const Dev& d, int t, int lane, uint32_t* se, uint8_t* sm) {
-    const int r = d.tile_rep[t];
-    RepState* s = d.st + r;
-    const Rep& R = d.rep[r];
+// R11a: one warp per rebuilt i-tile puts its chunks in canonical order: rank
+// by (first entry word, then position) -- the first entry words of a tile's
+// chunks are distinct, so the order does not depend on how the builders
+// allocated them.
+__device__ __forceinline__ void sort_tile_chunks(const Dev& d, int t, int lane) {
     const int n = d.tile_nch[t];
     const int c0 = d.tile_c0[t];
     const int* ids = d.chunk_order + c0;
     int* sorted = d.chunk_sorted + c0;
-    // rank of each chunk by (first entry word, then position): distinct ranks
     for (int base = 0; base < n; base += 32) {
         const int mine = base + lane;
         const int id = mine < n ? ids[mine] : -1;
@@ -1316,68 +1314,79 @@ __device__ __forceinline__ void cluster_tile(const Dev& d, int t, int lane, uint
         }
         if (id >= 0) sorted[rank] = id;
     }
-    __syncwarp();
-    // rows per cluster
-    int cnt[4] = {0, 0, 0, 0};
-    for (int k = 0; k < n; ++k) {
-        const uint32_t m = d.chunk_mask[32LL * sorted[k] + lane];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) cnt[q] += __popc(__ballot_sync(FULL, ((m >> (8 * q)) & 0xffu) != 0));
-    }
-    int rows[4], total = 0;
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        rows[q] = (cnt[q] + 31) >> 5;
-        total += rows[q];
-    }
+}
+
+// R11b: one warp per i-cluster (cluster 4 t + q of a rebuilt tile t) streams
+// the tile's chunks in canonical order and packs the entries with a bit among
+// lanes 8q .. 8q+7 into 32-entry rows.  It reserves the most rows the cluster
+// can need (one per chunk plus a partial one; 4 (chunks + tiles) in all, the
+// capacity) and records the rows it wrote.  The next chunk's ids, entries and
+// masks are loaded while the current one is packed.
+__device__ __forceinline__ void cluster_rows(const Dev& d, int cl, int lane, uint32_t* se, uint8_t* sm) {
+    const int t = cl >> 2, q = cl & 3;
+    const int r = d.tile_rep[t];
+    RepState* s = d.st + r;
+    const Rep& R = d.rep[r];
+    const int n = d.tile_nch[t];
+    const int* sorted = d.chunk_sorted + d.tile_c0[t];
     int base = 0;
-    if (lane == 0) base = atomicAdd(&s->n_cl, total);
+    if (lane == 0) base = atomicAdd(&s->n_cl, n + 1);
     base = __shfl_sync(FULL, base, 0);
-    if (base + total > R.cl_cap) {  // cannot happen with cl_cap = 4 chunk_cap + 4 n_tiles
-        if (lane == 0) set_status(s, ST_CAPACITY);
-        if (lane < 4) d.cl_job[4 * t + lane] = make_int2(0, 0);
+    if (base + n + 1 > R.cl_cap) {  // cannot happen with cl_cap = 4 chunk_cap + 4 n_tiles
+        if (lane == 0) {
+            set_status(s, ST_CAPACITY);
+            d.cl_job[cl] = make_int2(0, 0);
+        }
         return;
     }
-    int g = R.cl_begin + base;
-    if (lane < 4) {
-        int first = g;
-        for (int q = 0; q < lane; ++q) first += rows[q];
-        d.cl_job[4 * t + lane] = make_int2(first, rows[lane]);
-    }
-    for (int q = 0; q < 4; ++q) {
-        int fill = 0;
-        for (int k = 0; k < n; ++k) {
-            const long long c = sorted[k];
-            const uint32_t e = d.chunk_j[32 * c + lane];
-            const uint32_t m8 = (d.chunk_mask[32 * c + lane] >> (8 * q)) & 0xffu;
-            const uint32_t has = __ballot_sync(FULL, m8 != 0);
-            const int pos = fill + __popc(has & ((1u << lane) - 1u));
-            if (m8) {
-                se[pos] = e;
-                sm[pos] = static_cast<uint8_t>(m8);
-            }
-            fill += __popc(has);
-            __syncwarp();
-            if (fill >= 32) {
-                d.cl_j[32LL * g + lane] = se[lane];
-                d.cl_m[32LL * g + lane] = sm[lane];
-                ++g;
-                const uint32_t te = se[lane + 32];
-                const uint8_t tm = sm[lane + 32];
-                __syncwarp();
-                se[lane] = te;
-                sm[lane] = tm;
-                fill -= 32;
-                __syncwarp();
-            }
+    const int first = R.cl_begin + base;
+    int g = first;
+    int fill = 0;
+    int ids = n > 0 ? sorted[min(lane, n - 1)] : 0;  // ids of chunks 32 b .. 32 b + 31
+    long long c = __shfl_sync(FULL, ids, 0);
+    uint32_t e = n > 0 ? d.chunk_j[32 * c + lane] : 0u;
+    uint32_t m = n > 0 ? d.chunk_mask[32 * c + lane] : 0u;
+    for (int k = 0; k < n; ++k) {
+        // next chunk's data, in flight while this one is packed
+        const int k1 = k + 1;
+        if ((k1 & 31) == 0 && k1 < n) ids = sorted[min(k1 + lane, n - 1)];
+        uint32_t e1 = 0u, m1 = 0u;
+        if (k1 < n) {
+            const long long c1 = __shfl_sync(FULL, ids, k1 & 31);
+            e1 = d.chunk_j[32 * c1 + lane];
+            m1 = d.chunk_mask[32 * c1 + lane];
         }
-        if (fill > 0) {
-            d.cl_j[32LL * g + lane] = lane < fill ? se[lane] : 0u;
-            d.cl_m[32LL * g + lane] = lane < fill ? sm[lane] : static_cast<uint8_t>(0);
-            ++g;
+        const uint32_t m8 = (m >> (8 * q)) & 0xffu;
+        const uint32_t has = __ballot_sync(FULL, m8 != 0);
+        const int pos = fill + __popc(has & ((1u << lane) - 1u));
+        if (m8) {
+            se[pos] = e;
+            sm[pos] = static_cast<uint8_t>(m8);
         }
+        fill += __popc(has);
         __syncwarp();
+        if (fill >= 32) {
+            d.cl_j[32LL * g + lane] = se[lane];
+            d.cl_m[32LL * g + lane] = sm[lane];
+            ++g;
+            const uint32_t te = se[lane + 32];
+            const uint8_t tm = sm[lane + 32];
+            __syncwarp();
+            se[lane] = te;
+            sm[lane] = tm;
+            fill -= 32;
+            __syncwarp();
+        }
+        e = e1;
+        m = m1;
     }
+    if (fill > 0) {
+        d.cl_j[32LL * g + lane] = lane < fill ? se[lane] : 0u;
+        d.cl_m[32LL * g + lane] = lane < fill ? sm[lane] : static_cast<uint8_t>(0);
+        ++g;
+    }
+    __syncwarp();
+    if (lane == 0) d.cl_job[cl] = make_int2(first, g - first);
 }
 
 __device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
@@ -1538,11 +1547,18 @@ __global__ void __launch_bounds__(NT_B, 4) k_rebuild(Dev d, const int* bin_rep) 
         d.chunk_order[d.tile_c0[I] + atomicAdd(d.tile_fill + I, 1)] = c;
     }
     if (!grid_barrier(d)) return;
-    // R11: canonical order and the four cluster lists of every rebuilt tile
-    const int wib = tid >> 5;
+    // R11a: canonical chunk order of every rebuilt tile
     for (int w = gwarp; w < n_t; w += nwarps) {
         const int r = chunk_replica(pt, d.n_rep, w);
-        cluster_tile(d, d.rep[r].tile_begin + (w - pt[r]), lane, s_scr.cl.e[wib], s_scr.cl.m[wib]);
+        sort_tile_chunks(d, d.rep[r].tile_begin + (w - pt[r]), lane);
+    }
+    if (!grid_barrier(d)) return;
+    // R11b: the rows of every cluster of the rebuilt tiles
+    const int wib = tid >> 5;
+    for (int w = gwarp; w < 4 * n_t; w += nwarps) {
+        const int r = chunk_replica(pt, d.n_rep, w >> 2);
+        const int t = d.rep[r].tile_begin + ((w >> 2) - pt[r]);
+        cluster_rows(d, 4 * t + (w & 3), lane, s_scr.cl.e[wib], s_scr.cl.m[wib]);
     }
     if (!grid_barrier(d)) return;
     // R12: the rebuild is complete

@@ -123,7 +123,7 @@ typedef struct dmdgpu_options {
                            depend on it beyond FP32 summation order) */
 } dmdgpu_options;
 
-#define DMDGPU_NB_AUTO 0      /* the default form (8-atom i-clusters); the autotuner picks only
+#define DMDGPU_NB_AUTO 0      /* the default form (32 x 32 chunks); the autotuner picks only
                                  its launch shape, which changes no result bit */
 #define DMDGPU_NB_CHUNK32 1   /* one warp per 32 x 32 (i-tile, j entries) chunk */
 #define DMDGPU_NB_CLUSTER8 2  /* one warp per 8-atom i-cluster over its 32-entry rows */

@@ -111,3 +111,25 @@ def test_gpu_trajectory_matches_golden():
     s = eng.scalars()
     assert s.lj_step_since_rebuild == int(exp["lj_counter"])
     assert abs(s.potential_energy - float(exp["pe"])) < 1e-8 * abs(float(exp["pe"]))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_gpu_water_pme_trajectory_matches_golden(precision):
+    """REF profile flexible water with SPME (64-atom mesh rule, Nose-Hoover)
+    from Maxwell-Boltzmann velocities the engine generates: the GPU lands on the
+    end state the reference's compiled SimulationEngine::step reached.
+    Tolerances: fp64 1e-9 of the box edge in positions and 1e-8 relative RMS in
+    velocities; mixed 1e-6 / 1e-4 (a 1e-6 relative force error over 6 steps of
+    0.5 fs)."""
+    from dmd_b200.core import Engine
+    cfg, exp = _load("water_pme_trajectory")
+    eng = Engine(cfg, precision=precision, profile="ref")
+    eng.run_n(int(exp["steps"]))
+    L = cfg.box_size
+    tol_x, tol_v = {"fp64": (1e-9, 1e-8), "mixed": (1e-6, 1e-4)}[precision]
+    assert np.abs(eng.positions - exp["pos"]).max() / L < tol_x
+    assert rel_rms(eng.velocities, exp["vel"]) < tol_v
+    s = eng.scalars()
+    assert s.lj_step_since_rebuild == int(exp["lj_counter"])
+    assert abs(s.zeta - float(exp["zeta"])) <= 1e-6 * abs(float(exp["zeta"])) + 1e-12

@@ -171,3 +171,17 @@ def test_nve_drift_no_worse_than_reference(ref):
     d_fp64 = _nve_drift(_gpu_energies(cfg, "fp64", "phys", steps))
     assert d_mixed <= d_ref, (d_mixed, d_ref)
     assert d_fp64 <= d_ref, (d_fp64, d_ref)
+
+
+def test_single_point_water750k(oracle):
+    """The 750k-atom water box at full size (192^3 SPME mesh, Berendsen NPT
+    configuration), mixed precision, PHYS: total forces and energy against the
+    FP64 oracle on identical inputs (1e-5)."""
+    cfg = W.water_box(n_mol=250_000, box=19.56, seed=7, spacing=0.1019, thermostat="berendsen",
+                      barostat="berendsen").config()
+    F_o, e_o = oracle.forces(cfg, "phys")
+    eng = _engine(cfg, "mixed", "phys")
+    F, e = eng.compute_forces()
+    assert rel_rms(F, F_o) < 1e-5, rel_rms(F, F_o)
+    tot = sum(e.values())
+    assert abs(tot - e_o["total"]) <= 1e-5 * abs(e_o["total"]), (tot, e_o["total"])

@@ -385,3 +385,24 @@ def test_repack_is_invisible():
     assert np.array_equal(a.positions, b.positions)
     assert np.array_equal(a.velocities, b.velocities)
     assert a.potential_energy == b.potential_energy
+
+
+@pytest.mark.parametrize("system", ["argon", "water", "decane"])
+def test_cluster_form(oracle, system):
+    """The 8-atom i-cluster pair form (nb_form="cluster8"): its rows hold the
+    same pair set as the chunk list (pair_list checks them pair for pair),
+    forces follow the FP64 oracle within the mixed tolerance, and runs repeat
+    bit for bit."""
+    cfg = SYSTEMS[system]()
+    eng = _engine(cfg, "mixed", "phys", nb_form="cluster8")
+    F, e = eng.compute_forces()
+    pi, _ = eng.pair_list()  # raises if the cluster rows and the chunks disagree
+    assert len(pi) > 0
+    F_o, e_o = oracle.forces(cfg, "phys")
+    assert rel_rms(F, F_o) < TOL["mixed"], rel_rms(F, F_o)
+    a = _engine(cfg, "mixed", "phys", nb_form="cluster8")
+    b = _engine(cfg, "mixed", "phys", nb_form="cluster8")
+    a.run_n(20)
+    b.run_n(20)
+    assert np.array_equal(a.positions, b.positions)
+    assert a.potential_energy == b.potential_energy
