@@ -25,20 +25,75 @@
 
 namespace dmd {
 
+namespace {
+size_t size_class(size_t bytes) {
+    size_t c = 256;
+    while (c < bytes) c += std::max<size_t>(256, c / 4);  // classes about 2^(1/4) apart
+    return c;
+}
+}  // namespace
+
+void* BlockPool::take(size_t bytes, size_t* cls) {
+    *cls = size_class(bytes);
+    auto it = free_blocks.lower_bound(*cls);
+    // a block of the same class, or one class up at most (less than 2x waste)
+    if (it != free_blocks.end() && it->first <= *cls + *cls / 2) {
+        void* p = it->second;
+        *cls = it->first;
+        held -= it->first;
+        free_blocks.erase(it);
+        return p;
+    }
+    void* p = nullptr;
+    if (cudaMalloc(&p, *cls) != cudaSuccess) {
+        cudaGetLastError();
+        trim(0);  // out of memory: release every cached block and retry once
+        if (cudaMalloc(&p, *cls) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+    }
+    return p;
+}
+
+void BlockPool::give(void* p, size_t cls) {
+    free_blocks.emplace(cls, p);
+    held += cls;
+}
+
+void BlockPool::trim(size_t keep_bytes) {
+    while (held > keep_bytes && !free_blocks.empty()) {
+        auto it = std::prev(free_blocks.end());
+        cudaFree(it->second);
+        held -= it->first;
+        free_blocks.erase(it);
+    }
+}
+
+BlockPool::~BlockPool() { trim(0); }
+
 DeviceArena::~DeviceArena() {
-    for (void* p : ptrs) cudaFree(p);
+    for (auto& b : ptrs) {
+        if (pool) pool->give(b.first, b.second);
+        else cudaFree(b.first);
+    }
 }
 
 template <typename T>
 T* DeviceArena::alloc(size_t n) {
     if (n == 0) n = 1;
+    const size_t want = n * sizeof(T);
+    size_t cls = want;
     void* p = nullptr;
-    if (cudaMalloc(&p, n * sizeof(T)) != cudaSuccess) {
-        throw std::runtime_error("cudaMalloc failed");
+    if (pool) {
+        p = pool->take(want, &cls);
+    } else if (cudaMalloc(&p, want) != cudaSuccess) {
+        p = nullptr;
     }
-    cudaMemset(p, 0, n * sizeof(T));
-    ptrs.push_back(p);
-    bytes += n * sizeof(T);
+    if (!p) throw std::runtime_error("cudaMalloc failed");
+    cudaMemset(p, 0, want);
+    ptrs.emplace_back(p, cls);
+    bytes += want;
     return static_cast<T*>(p);
 }
 
@@ -460,9 +515,31 @@ int Batch::add(const dmdgpu_system& in, long long n_steps, unsigned comp_mask, i
         slot = static_cast<int>(reps_.size());
         reps_.emplace_back();
     }
+    // the cuFFT plans of a new mesh size are made here, at admission, not in
+    // the table rebuild of the next step (a plan takes tens of ms to make)
+    if (hr->rep.flags & F_PME) {
+        CK(cudaSetDevice(device_));
+        int rc = ensure_plans(hr->rep.pme_K);
+        if (rc) return rc;
+    }
     reps_[slot] = std::move(hr);
     packed_ = false;
     *out_slot = slot;
+    return DMDGPU_OK;
+}
+
+int Batch::ensure_plans(int K) {
+    if (plans_.count(K)) return DMDGPU_OK;
+    cufftHandle f, b;
+    if (cufftPlan3d(&f, K, K, K, fp64_ ? CUFFT_D2Z : CUFFT_R2C) != CUFFT_SUCCESS)
+        return fail(DMDGPU_ERR_GPU, "cufftPlan3d failed");
+    if (cufftPlan3d(&b, K, K, K, fp64_ ? CUFFT_Z2D : CUFFT_C2R) != CUFFT_SUCCESS) {
+        cufftDestroy(f);
+        return fail(DMDGPU_ERR_GPU, "cufftPlan3d failed");
+    }
+    cufftSetStream(f, aux_stream_);
+    cufftSetStream(b, aux_stream_);
+    plans_[K] = {f, b};
     return DMDGPU_OK;
 }
 
@@ -544,7 +621,7 @@ int Batch::pack() {
               n_dih = 0, n_imp = 0, n_excl = 0, mesh_fix = 0, mesh_real = 0, mesh_cplx = 0, n_bsp = 0,
               n_cl = 0;
     int pme_blocks = 0, conv_blocks = 0;
-    any_pme_ = any_baro_ = any_ref_lj_ = any_andersen_ref_ = any_andersen_phys_ = false;
+    any_pme_ = any_baro_ = any_narrow_ = any_ref_lj_ = any_andersen_ref_ = any_andersen_phys_ = false;
     for (int k = 0; k < R; ++k) {
         HostRep& h = *reps_[order_[k]];
         HostSystem& s = h.sys;
@@ -605,6 +682,9 @@ int Batch::pack() {
             any_pme_ = true;
         }
         if (s.barostat) any_baro_ = true;
+        // a box narrower than twice the list cutoff (or one a barostat may
+        // shrink): the pair kernels take the minimum image per evaluation
+        if (s.barostat || s.box * s.box < 4.0 * P.rc_list2) any_narrow_ = true;
         if (!phys_ && (P.flags & F_LJ)) any_ref_lj_ = true;
         if (s.thermostat == 3 && !phys_) any_andersen_ref_ = true;
         if (s.thermostat == 3 && phys_) any_andersen_phys_ = true;
@@ -613,6 +693,7 @@ int Batch::pack() {
     n_conv_blocks_ = conv_blocks;
     try {
         arena_ = std::make_unique<DeviceArena>();
+        arena_->pool = &pool_;
         DeviceArena& A = *arena_;
         Dev& d = dev_;
         d = Dev{};
@@ -678,9 +759,11 @@ int Batch::pack() {
         d.chunk_itile = A.alloc<int>(n_chunks);
         d.chunk_j = A.alloc<uint32_t>(n_chunks * 32);
         d.chunk_mask = A.alloc<uint32_t>(n_chunks * 32);
-        d.chunk_prefix = A.alloc<int>(R + 3);
+        d.chunk_prefix = A.alloc<int>(R + 4);
         d.nb_work = d.chunk_prefix + R + 1;
         d.build_work = d.chunk_prefix + R + 2;
+        d.nb_work_mi = d.chunk_prefix + R + 3;
+        d.mi_split = any_narrow_ ? 1 : 0;
         d.grid_bar = A.alloc<unsigned>(2);
         d.build_prefix = A.alloc<int>(4 * (R + 1));
         if (uses_clusters()) {
@@ -994,6 +1077,9 @@ int Batch::pack() {
         }
         up(d_st_, hst.data(), sizeof(RepState) * R);
         used_bytes_ = static_cast<long long>(A.bytes);
+        // blocks left over from a larger table are kept up to the table's own
+        // size; beyond that they are released
+        pool_.trim(std::max<size_t>(A.bytes, size_t(1) << 28));
     } catch (const std::exception& e) {
         arena_.reset();
         return fail(DMDGPU_ERR_OOM, std::string("device allocation/upload failed: ") + e.what());
@@ -1001,18 +1087,13 @@ int Batch::pack() {
     CK(cudaMallocHost(&h_st_, sizeof(RepState) * R));
     CK(cudaMallocHost(&h_tgt_, sizeof(long long) * R));
     st_fresh_ = false;
-    // cuFFT plans per mesh size
+    // cuFFT plans per mesh size (normally made at admission already)
     for (int k = 0; k < R; ++k) {
         const Rep& P = reps_[order_[k]]->rep;
-        if (!(P.flags & F_PME) || plans_.count(P.pme_K)) continue;
-        cufftHandle f, b;
-        const int K = P.pme_K;
-        if (cufftPlan3d(&f, K, K, K, fp64_ ? CUFFT_D2Z : CUFFT_R2C) != CUFFT_SUCCESS ||
-            cufftPlan3d(&b, K, K, K, fp64_ ? CUFFT_Z2D : CUFFT_C2R) != CUFFT_SUCCESS)
-            return fail(DMDGPU_ERR_GPU, "cufftPlan3d failed");
-        cufftSetStream(f, aux_stream_);
-        cufftSetStream(b, aux_stream_);
-        plans_[K] = {f, b};
+        if (P.flags & F_PME) {
+            int rc = ensure_plans(P.pme_K);
+            if (rc) return rc;
+        }
     }
     for (int k : order_) reps_[k]->on_device = true;
     {

@@ -4,6 +4,7 @@
 #include <cufft.h>
 
 #include <map>
+#include <utility>
 #include <memory>
 #include <string>
 #include <vector>
@@ -66,9 +67,24 @@ struct HostRep {
     bool on_device = false;    // packed into the current device table (its state lives there)
 };
 
+// Device blocks kept for reuse across table rebuilds, by size: a serving loop
+// rebuilds its table at every admission and release, and freeing and
+// allocating every array each time stalls the device (cudaFree waits for it
+// and unmaps; measured up to ~0.7 s in one rebuild).  Sizes are rounded up to
+// classes 2^(k/4) apart, so a rebuilt table of a similar size finds blocks.
+struct BlockPool {
+    std::multimap<size_t, void*> free_blocks;  // size class -> block
+    size_t held = 0;                           // bytes of the blocks in free_blocks
+    void* take(size_t bytes, size_t* cls);
+    void give(void* p, size_t cls);
+    void trim(size_t keep_bytes);              // frees the largest blocks down to keep_bytes
+    ~BlockPool();
+};
+
 struct DeviceArena {
-    std::vector<void*> ptrs;
-    size_t bytes = 0;
+    std::vector<std::pair<void*, size_t>> ptrs;  // block and its size class
+    size_t bytes = 0;                            // bytes requested (budget accounting)
+    BlockPool* pool = nullptr;                   // blocks return here instead of cudaFree
     ~DeviceArena();
     template <typename T>
     T* alloc(size_t n);
@@ -126,6 +142,7 @@ class Batch {
     int replica_index(int slot) const;
     void free_device();
     void andersen_ref_prepare();
+    int ensure_plans(int K);  // cuFFT R2C/C2R plans of mesh size K, made once per batch
 
     dmdgpu_options opt_;
     long long budget_;
@@ -140,6 +157,7 @@ class Batch {
     bool capture_error_ = false;
     std::vector<std::unique_ptr<HostRep>> reps_;   // indexed by slot (nullptr = free)
     std::vector<int> order_;                        // packed replica index -> slot
+    BlockPool pool_;                                 // declared before arena_: outlives it
     std::unique_ptr<DeviceArena> arena_;
     Dev dev_{};
     Rep* d_rep_ = nullptr;
@@ -150,7 +168,7 @@ class Batch {
     int* d_bin_rep_ = nullptr;
     int n_pme_blocks_ = 0, n_conv_blocks_ = 0;
     bool any_cons_ = false;  // some replica has distance constraints
-    bool any_pme_ = false, any_baro_ = false, any_ref_lj_ = false, any_andersen_ref_ = false,
+    bool any_pme_ = false, any_baro_ = false, any_narrow_ = false, any_ref_lj_ = false, any_andersen_ref_ = false,
          any_andersen_phys_ = false;
     std::map<int, std::pair<cufftHandle, cufftHandle>> plans_;
     cudaGraphExec_t graph_ = nullptr;

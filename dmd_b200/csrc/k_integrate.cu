@@ -34,6 +34,7 @@ __global__ void k_eval_begin(Dev d, int pass) {
     int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r == 0) {
         *d.nb_work = 0;
+        if (d.nb_work_mi) *d.nb_work_mi = 0;
         d.grid_bar[0] = 0;  // arrivals (the generation word keeps counting)
     }
     if (r >= d.n_rep) return;

@@ -132,11 +132,16 @@ __device__ __forceinline__ float pair_f(float r2, float c6f, float c12f, float q
 //
 // PHYS = false evaluates LJ only (the REF profile, and PHYS replicas without
 // charges); SAME = true is the PHYS form whose LJ and Coulomb cutoffs are equal
-// (one band test, one cutoff test per pair).
-template <bool PHYS, bool SAME, bool ENERGY>
+// (one band test, one cutoff test per pair).  MI = true (boxes narrower than
+// twice the list cutoff) takes the minimum image of every pair at every
+// evaluation, as the reference does (Cell::minimum_image, cell.cpp:26-38): in
+// such a box the nearest image of a listed pair can change between list
+// builds, so the image frozen at the build is not enough.
+template <bool PHYS, bool SAME, bool ENERGY, bool MI>
 __device__ __forceinline__ void nb_chunk(const Dev& d, const Rep& R, RepState* s, int c, int lane,
                                          ChunkStage& S, const float4* lj_tab, Acc& acc) {
     const double L = s->L;
+    const float Lf = static_cast<float>(L), iLf = static_cast<float>(s->invL);
     const int I = d.chunk_itile[c];
     const int si = 32 * I + lane;
     const float4 xi = d.xq32[si];
@@ -192,7 +197,12 @@ __device__ __forceinline__ void nb_chunk(const Dev& d, const Rep& R, RepState* s
             const bool bit = (rm >> u) & 1u;
             const float4 pj = px[u];
             const float4 p = lj[pt[u]];
-            const float dx = pj.x - xi.x, dy = pj.y - xi.y, dz = pj.z - xi.z;
+            float dx = pj.x - xi.x, dy = pj.y - xi.y, dz = pj.z - xi.z;
+            if (MI) {
+                dx = fmaf(-Lf, rintf(dx * iLf), dx);
+                dy = fmaf(-Lf, rintf(dy * iLf), dy);
+                dz = fmaf(-Lf, rintf(dz * iLf), dz);
+            }
             const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
             if (!ENERGY && (!PHYS || SAME)) {
                 // one cutoff: evaluate with the table coefficients and keep the
@@ -262,7 +272,12 @@ __device__ __forceinline__ void nb_chunk(const Dev& d, const Rep& R, RepState* s
         const int aj2 = S.aj[src];
         const bool in_l = has_lj && exact_inside(d, ai, aj2, L, s->invL, R.rc_lj2);
         const bool in_c = has_c && exact_inside(d, ai, aj2, L, s->invL, R.rc_c2);
-        const float dx = pj.x - xi.x, dy = pj.y - xi.y, dz = pj.z - xi.z;
+        float dx = pj.x - xi.x, dy = pj.y - xi.y, dz = pj.z - xi.z;
+        if (MI) {
+            dx = fmaf(-Lf, rintf(dx * iLf), dx);
+            dy = fmaf(-Lf, rintf(dy * iLf), dy);
+            dz = fmaf(-Lf, rintf(dz * iLf), dz);
+        }
         const float r2 = fmaxf(fmaf(dz, dz, fmaf(dy, dy, dx * dx)), 1e-6f);
         const float qq = (PHYS && in_c) ? keqi * pj.w : 0.f;
         float ir6, rinv, erfc_ar;
@@ -304,8 +319,12 @@ __device__ __forceinline__ void nb_chunk(const Dev& d, const Rep& R, RepState* s
 constexpr int LJ_SMEM = 512;
 
 // LJS: the LJ table fits LJ_SMEM and is staged in shared memory (a compile-time
-// choice, so the table loads are shared-memory loads).
-template <bool PHYS, bool LJS>
+// choice, so the table loads are shared-memory loads).  MIK: the kernel for the
+// replicas whose box is narrower than twice their list cutoff (minimum image
+// per evaluation); launched, with its own work counter, only when the table
+// has such replicas (d.mi_split), in which case the main kernel leaves them to
+// it -- so their forms do not weigh on the main kernel's registers.
+template <bool PHYS, bool LJS, bool MIK>
 __global__ void __launch_bounds__(256, 3) k_nb_f32(Dev d) {
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
@@ -320,9 +339,10 @@ __global__ void __launch_bounds__(256, 3) k_nb_f32(Dev d) {
     int cur = -1;
     // chunks are taken one per warp from a counter, so warps on SMs shared with
     // the concurrent PME kernels simply take fewer
+    int* counter = MIK ? d.nb_work_mi : d.nb_work;
     for (;;) {
         int w = 0;
-        if (lane == 0) w = atomicAdd(d.nb_work, 1);
+        if (lane == 0) w = atomicAdd(counter, 1);
         w = __shfl_sync(FULL, w, 0);
         if (w >= total) break;
         const int r = chunk_replica(d.chunk_prefix, d.n_rep, w);
@@ -331,20 +351,36 @@ __global__ void __launch_bounds__(256, 3) k_nb_f32(Dev d) {
             cur = r;
         }
         RepState* s = d.st + r;
-        if (!s->eval) continue;
         const Rep& R = d.rep[r];
+        // box narrower than twice the list cutoff: minimum image per evaluation
+        // (d.mi_split is set whenever a replica's box is, or under a barostat
+        // may become, that narrow)
+        const bool mi = 4.0 * R.rc_list2 > s->L * s->L;
+        if (!s->eval || MIK != (mi && d.mi_split)) {
+            // a replica this kernel skips: move the counter past its chunks
+            if (lane == 0) atomicMax(counter, d.chunk_prefix[r + 1]);
+            continue;
+        }
         const int c = R.chunk_begin + (w - d.chunk_prefix[r]);
         // warp-uniform choice of the pair form for this replica
         const bool coul = PHYS && (R.flags & F_COUL_REAL);
         const bool same = coul && (R.flags & F_LJ) && R.rc_lj2 == R.rc_c2;
-        if (s->want_e) {
-            if (!coul) nb_chunk<false, false, true>(d, R, s, c, lane, s_stage[wib], lj_tab, acc);
-            else if (same) nb_chunk<true, true, true>(d, R, s, c, lane, s_stage[wib], lj_tab, acc);
-            else nb_chunk<true, false, true>(d, R, s, c, lane, s_stage[wib], lj_tab, acc);
+        if (MIK) {
+            if (!coul) {
+                if (s->want_e) nb_chunk<false, false, true, true>(d, R, s, c, lane, s_stage[wib], lj_tab, acc);
+                else nb_chunk<false, false, false, true>(d, R, s, c, lane, s_stage[wib], lj_tab, acc);
+            } else {
+                if (s->want_e) nb_chunk<PHYS, false, true, true>(d, R, s, c, lane, s_stage[wib], lj_tab, acc);
+                else nb_chunk<PHYS, false, false, true>(d, R, s, c, lane, s_stage[wib], lj_tab, acc);
+            }
+        } else if (s->want_e) {
+            if (!coul) nb_chunk<false, false, true, false>(d, R, s, c, lane, s_stage[wib], lj_tab, acc);
+            else if (same) nb_chunk<true, true, true, false>(d, R, s, c, lane, s_stage[wib], lj_tab, acc);
+            else nb_chunk<true, false, true, false>(d, R, s, c, lane, s_stage[wib], lj_tab, acc);
         } else {
-            if (!coul) nb_chunk<false, false, false>(d, R, s, c, lane, s_stage[wib], lj_tab, acc);
-            else if (same) nb_chunk<true, true, false>(d, R, s, c, lane, s_stage[wib], lj_tab, acc);
-            else nb_chunk<true, false, false>(d, R, s, c, lane, s_stage[wib], lj_tab, acc);
+            if (!coul) nb_chunk<false, false, false, false>(d, R, s, c, lane, s_stage[wib], lj_tab, acc);
+            else if (same) nb_chunk<true, true, false, false>(d, R, s, c, lane, s_stage[wib], lj_tab, acc);
+            else nb_chunk<true, false, false, false>(d, R, s, c, lane, s_stage[wib], lj_tab, acc);
         }
     }
     flush_acc(d, cur, acc);
@@ -566,6 +602,8 @@ __global__ void __launch_bounds__(256, 2) k_nb8_f32(Dev d) {
         const int r = d.tile_rep[w >> 2];
         RepState* s = d.st + r;
         if (!s->eval) continue;
+        // narrow-box replicas are left to the minimum-image chunk kernel
+        if (d.mi_split && 4.0 * d.rep[r].rc_list2 > s->L * s->L) continue;
         const int2 job = d.cl_job[w];
         if (job.y == 0) continue;
         if (r != cur) {
@@ -697,27 +735,41 @@ void launch_nonbonded(const Dev& d, bool fp64, bool phys, int n_sm, int blocks_p
     if (fp64) {
         if (phys) k_nb_f64<true><<<n_sm * 8, 256, 0, st>>>(d);
         else k_nb_f64<false><<<n_sm * 8, 256, 0, st>>>(d);
-    } else if (form == NB_CLUSTER8 && d.cl_j) {
-        const int g = n_sm * std::min(std::max(blocks_per_sm, 1), 2);
-        const bool ljs = d.n_lj <= LJ_SMEM;
-        if (phys) {
-            if (ljs) k_nb8_f32<true, true><<<g, 256, 0, st>>>(d);
-            else k_nb8_f32<true, false><<<g, 256, 0, st>>>(d);
-        } else {
-            if (ljs) k_nb8_f32<false, true><<<g, 256, 0, st>>>(d);
-            else k_nb8_f32<false, false><<<g, 256, 0, st>>>(d);
-        }
     } else {
-        // persistent: up to the 3 blocks per SM its registers allow; fewer leave
-        // room on every SM for the bonded / PME kernels running alongside
-        const int g = n_sm * std::min(std::max(blocks_per_sm, 1), 3);
         const bool ljs = d.n_lj <= LJ_SMEM;
-        if (phys) {
-            if (ljs) k_nb_f32<true, true><<<g, 256, 0, st>>>(d);
-            else k_nb_f32<true, false><<<g, 256, 0, st>>>(d);
+        // persistent: up to the blocks per SM its registers allow (2 for the
+        // cluster form, 3 for the chunk form); fewer leave room on every SM for
+        // the bonded / PME kernels running alongside
+        const int bps = std::max(blocks_per_sm, 1);
+        if (form == NB_CLUSTER8 && d.cl_j) {
+            const int g = n_sm * std::min(bps, 2);
+            if (phys) {
+                if (ljs) k_nb8_f32<true, true><<<g, 256, 0, st>>>(d);
+                else k_nb8_f32<true, false><<<g, 256, 0, st>>>(d);
+            } else {
+                if (ljs) k_nb8_f32<false, true><<<g, 256, 0, st>>>(d);
+                else k_nb8_f32<false, false><<<g, 256, 0, st>>>(d);
+            }
         } else {
-            if (ljs) k_nb_f32<false, true><<<g, 256, 0, st>>>(d);
-            else k_nb_f32<false, false><<<g, 256, 0, st>>>(d);
+            const int g = n_sm * std::min(bps, 3);
+            if (phys) {
+                if (ljs) k_nb_f32<true, true, false><<<g, 256, 0, st>>>(d);
+                else k_nb_f32<true, false, false><<<g, 256, 0, st>>>(d);
+            } else {
+                if (ljs) k_nb_f32<false, true, false><<<g, 256, 0, st>>>(d);
+                else k_nb_f32<false, false, false><<<g, 256, 0, st>>>(d);
+            }
+        }
+        if (d.mi_split) {  // narrow-box replicas: their own kernel on the same stream
+            const int g = n_sm * std::min(bps, 3);
+            if (phys) {
+                if (ljs) k_nb_f32<true, true, true><<<g, 256, 0, st>>>(d);
+                else k_nb_f32<true, false, true><<<g, 256, 0, st>>>(d);
+            } else {
+                if (ljs) k_nb_f32<false, true, true><<<g, 256, 0, st>>>(d);
+                else k_nb_f32<false, false, true><<<g, 256, 0, st>>>(d);
+            }
+            *nlaunch += 1;
         }
     }
     *nlaunch += 1;

@@ -161,6 +161,8 @@ struct Dev {
     int2* cl_job;                      // [4 n_tiles] per cluster: first row, row count
     void* pme_green;                   // cached PME influence function (mesh_cplx layout, T)
     int* nb_work;                      // pair-kernel chunk counter (reset per evaluation)
+    int* nb_work_mi;                   // the same for the narrow-box pair kernel
+    int mi_split;                      // narrow-box replicas go to their own pair kernel
     int* build_work;                   // list-build i-tile counter (reset per rebuild)
     int* build_prefix;                 // [3][n_rep + 1] prefixes of the rebuilding replicas'
                                        // atoms, sort cells and tiles

@@ -183,6 +183,7 @@ extern "C" int dmdgpu_nonbonded_noalloc(const dmdgpu_nb_params* p, const double*
     d.chunk_prefix = reinterpret_cast<int*>(at(8 * sizeof(int)));
     d.build_prefix = d.chunk_prefix + 8;  // [3][2]: words 8..13 of the 256-byte block
     d.nb_work = d.chunk_prefix + 4;  // zeroed with the prefix below
+    d.nb_work_mi = d.chunk_prefix + 3;  // words 0, 1: the chunk prefix of the one replica
     d.build_work = d.chunk_prefix + 5;
     d.grid_bar = reinterpret_cast<unsigned*>(d.chunk_prefix + 6);  // [2]: words 6, 7
     d.rep = d_rep;
@@ -295,6 +296,8 @@ extern "C" int dmdgpu_nonbonded_noalloc(const dmdgpu_nb_params* p, const double*
                      : p->lj_cutoff;
     R.rc_list2 = R.rc_list * R.rc_list;
     R.alpha = p->ewald_coeff;
+    // a box narrower than twice the list cutoff: minimum image per evaluation
+    d.mi_split = L * L < 4.0 * R.rc_list2 ? 1 : 0;
     RepState S{};
     S.L = L;
     S.invL = 1.0 / L;

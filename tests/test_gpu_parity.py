@@ -267,8 +267,11 @@ def test_water_shake_rattle_trajectory(oracle, precision, profile):
     c = _rigid_water()
     oe = oracle.engine(c, profile)
     eng = _engine(c, precision, profile)
-    # positions (over the box edge) and velocities (relative RMS) against the oracle
-    tol_x, tol_v = {"fp64": (1e-8, 1e-8), "mixed": (1e-4, 1e-3)}[precision]
+    # positions (over the box edge) and velocities (relative RMS) against the
+    # oracle.  The box (1.44 nm) is narrower than twice the list cutoff, so
+    # the pair kernels take the minimum image of every pair at every
+    # evaluation, as the oracle does.
+    tol_x, tol_v = {"fp64": (1e-8, 1e-8), "mixed": (1e-4, 1e-4)}[precision]
     ci, cj, d0 = np.asarray(c.constraint_i), np.asarray(c.constraint_j), np.asarray(c.constraint_dist)
     L = c.box_size
     for k in range(3):
