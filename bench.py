@@ -299,6 +299,7 @@ def run_single(args, R: Ranks):
 
     eng, t_mixed, step_ms, nb_ms, clocks = timed("mixed")
     value = R.ws * n_atoms * args.steps / (step_ms / 1e3)
+    launch = eng.launch_info()
     s = eng.scalars()
     evals_per_step = t_mixed["nonbonded_launches"] / args.steps
     # accuracy is checked at the starting configuration, except on a perfect
@@ -381,6 +382,7 @@ def run_single(args, R: Ranks):
         "roofline": roof,
         "cpu_baseline": cpu,
         "gpu_launches": int(t_mixed["kernel_launches"]),
+        "launch": launch,
         "clocks": clocks,
         "list_builds": int(s.list_builds),
         "energies_in_timed_steps": "the device-timed value evaluates the energies and the virial "
@@ -460,6 +462,7 @@ def run_batch(args, R: Ranks):
         return b, slots, t, clocks
 
     b, slots, t_mixed, clocks = timed("mixed")
+    launch = b.launch_info()
     step_ms = R.max(t_mixed["step_ms"])
     nb_ms = R.max(t_mixed["nonbonded_ms"] / max(t_mixed["nonbonded_launches"], 1))
     value = R.ws * n_atoms * args.steps / (step_ms / 1e3)
@@ -562,6 +565,7 @@ def run_batch(args, R: Ranks):
         "roofline": roof,
         "cpu_baseline": cpu,
         "gpu_launches": int(t_mixed["kernel_launches"]),
+        "launch": launch,
         "clocks": clocks,
         "list_builds": list_builds,
         "potential_energy_finite": bool(all(math.isfinite(x) for x in pe)),
@@ -618,7 +622,9 @@ def run_serve(args, R: Ranks):
                    "atoms_max": max(j.n_atoms for j in jobs), "profile": "phys",
                    "l2": "not flushed (jobs' state stays resident, far above L2 in total)",
                    "parallelism": f"replicas x{R.ws} (one job stream per GPU)"},
-        "latency": {"step_ms": res["step_latency_ms"], "job_s": res["job_latency"]},
+        "latency": {"step_ms": res["step_latency_ms"], "job_s": res["job_latency"],
+                    "step_ms_steady": res["step_latency_ms_steady"],
+                    "step_ms_rebuild": res["step_latency_ms_rebuild"]},
         "wall_s": round(res["wall_s"], 3),
         "fp64_path": {"value": round(res64["atom_steps_per_s"], 1),
                       "latency": {"step_ms": res64["step_latency_ms"], "job_s": res64["job_latency"]},
@@ -632,6 +638,7 @@ def run_serve(args, R: Ranks):
         "roofline": None,
         "cpu_baseline": cpu,
         "gpu_launches": None,
+        "launch": res["launch_configs"],
         "clocks": clocks,
     }
 

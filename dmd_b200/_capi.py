@@ -73,6 +73,15 @@ class dmdgpu_options(C.Structure):
 NB_FORMS = {"auto": 0, "chunk32": 1, "cluster8": 2}
 
 
+def launch_info_dict(info) -> dict:
+    """dmdgpu_launch_info as a plain dict (form by name)."""
+    names = {v: k for k, v in NB_FORMS.items()}
+    return {"packed": bool(info.packed), "nb_form": names.get(info.nb_form, "none"),
+            "nb_blocks_per_sm": int(info.nb_blocks_per_sm), "tuned": bool(info.tuned),
+            "min_image_kernel": bool(info.min_image_kernel), "n_replicas": int(info.n_replicas),
+            "n_atoms": int(info.n_atoms), "launches_per_step": int(info.launches_per_step)}
+
+
 class dmdgpu_frame(C.Structure):
     _fields_ = [("step", C.c_int64), ("time", C.c_double), ("box", C.c_double), ("n_atoms", C.c_int32),
                 ("x", C.POINTER(C.c_double)), ("y", C.POINTER(C.c_double)), ("z", C.POINTER(C.c_double)),
@@ -85,6 +94,12 @@ FRAME_FN = C.CFUNCTYPE(None, C.POINTER(dmdgpu_frame), C.c_void_p)
 class dmdgpu_timing(C.Structure):
     _fields_ = [("step_ms", C.c_double), ("nonbonded_ms", C.c_double), ("pme_ms", C.c_double),
                 ("nonbonded_launches", C.c_int64), ("kernel_launches", C.c_int64)]
+
+
+class dmdgpu_launch_info(C.Structure):
+    _fields_ = [("packed", C.c_int32), ("nb_form", C.c_int32), ("nb_blocks_per_sm", C.c_int32),
+                ("tuned", C.c_int32), ("min_image_kernel", C.c_int32), ("n_replicas", C.c_int32),
+                ("n_atoms", C.c_int64), ("launches_per_step", C.c_int64)]
 
 
 class dmdgpu_scalars(C.Structure):
@@ -126,6 +141,7 @@ def lib() -> C.CDLL:
         "dmdgpu_footprint_bytes": (C.c_int64, [C.POINTER(dmdgpu_system), C.POINTER(dmdgpu_options)]),
         "dmdgpu_kernel_launches": (C.c_int64, [vp]),
         "dmdgpu_stream": (C.c_void_p, [vp]),
+        "dmdgpu_get_launch_info": (C.c_int, [vp, C.POINTER(dmdgpu_launch_info)]),
         "dmdgpu_step_timed": (C.c_int, [vp, C.c_int32, C.c_int64, C.POINTER(dmdgpu_timing)]),
         "dmdgpu_test_inject": (C.c_int, [vp, C.c_int32]),
         "dmdgpu_set_frame_writer": (C.c_int, [vp, C.c_int32, FRAME_FN, vp]),
@@ -141,6 +157,7 @@ def lib() -> C.CDLL:
         "dmdgpu_batch_get_scalars": (C.c_int, [vp, C.c_int32, C.POINTER(dmdgpu_scalars)]),
         "dmdgpu_batch_release": (C.c_int, [vp, C.c_int32]),
         "dmdgpu_batch_used_bytes": (C.c_int64, [vp]),
+        "dmdgpu_batch_get_launch_info": (C.c_int, [vp, C.POINTER(dmdgpu_launch_info)]),
         "dmdgpu_batch_active": (C.c_int32, [vp]),
         "dmdgpu_batch_last_error": (C.c_char_p, [vp]),
         "dmdgpu_batch_destroy": (None, [vp]),

@@ -124,6 +124,12 @@ class Batch:
     def active(self) -> int:
         return int(self._lib.dmdgpu_batch_active(self._h))
 
+    def launch_info(self) -> dict:
+        """Launch configuration of the current device table (see Engine.launch_info)."""
+        info = _capi.dmdgpu_launch_info()
+        self._check(self._lib.dmdgpu_batch_get_launch_info(self._h, C.byref(info)))
+        return _capi.launch_info_dict(info)
+
     @property
     def slots(self) -> list[int]:
         return sorted(self._n)

@@ -303,6 +303,14 @@ class Engine:
         """cudaStream_t (as an integer) every launch of this engine is issued on."""
         return int(self._lib.dmdgpu_stream(self._h) or 0)
 
+    def launch_info(self) -> dict:
+        """The launch configuration of the device table (valid after a step):
+        pair-kernel form, blocks per SM the autotuner chose, whether the
+        minimum-image pair kernel runs, kernels per captured step."""
+        info = _capi.dmdgpu_launch_info()
+        self._check(self._lib.dmdgpu_get_launch_info(self._h, C.byref(info)))
+        return _capi.launch_info_dict(info)
+
     def repack(self):
         """Rebuild the device table with the state carried over bit for bit (pair
         list rebuilt in the frame of its last build, forces evaluated again at

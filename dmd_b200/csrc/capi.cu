@@ -280,6 +280,12 @@ int64_t dmdgpu_kernel_launches(dmdgpu_ctx* c) { return (c && c->b) ? c->b->launc
 
 void* dmdgpu_stream(dmdgpu_ctx* c) { return (c && c->b) ? static_cast<void*>(c->b->stream()) : nullptr; }
 
+int dmdgpu_get_launch_info(dmdgpu_ctx* c, dmdgpu_launch_info* out) {
+    if (!c || !c->b || !out) return DMDGPU_ERR_INVALID;
+    c->b->launch_info(out);
+    return DMDGPU_OK;
+}
+
 int dmdgpu_step_timed(dmdgpu_ctx* c, int32_t n, int64_t flush_bytes, dmdgpu_timing* out) {
     if (!c || !c->b || n <= 0 || !out) return DMDGPU_ERR_INVALID;
     int rc = c->b->extend_targets(n);
@@ -381,6 +387,12 @@ int dmdgpu_batch_release(dmdgpu_batch* b, int32_t slot) {
 }
 
 int64_t dmdgpu_batch_used_bytes(dmdgpu_batch* b) { return (b && b->b) ? b->b->used_bytes() : 0; }
+
+int dmdgpu_batch_get_launch_info(dmdgpu_batch* b, dmdgpu_launch_info* out) {
+    if (!b || !b->b || !out) return DMDGPU_ERR_INVALID;
+    b->b->launch_info(out);
+    return DMDGPU_OK;
+}
 
 int32_t dmdgpu_batch_active(dmdgpu_batch* b) { return (b && b->b) ? b->b->active() : 0; }
 

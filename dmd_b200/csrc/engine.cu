@@ -25,76 +25,84 @@
 
 namespace dmd {
 
-namespace {
-size_t size_class(size_t bytes) {
-    size_t c = 256;
-    while (c < bytes) c += std::max<size_t>(256, c / 4);  // classes about 2^(1/4) apart
-    return c;
-}
-}  // namespace
-
-void* BlockPool::take(size_t bytes, size_t* cls) {
-    *cls = size_class(bytes);
-    auto it = free_blocks.lower_bound(*cls);
-    // a block of the same class, or one class up at most (less than 2x waste)
-    if (it != free_blocks.end() && it->first <= *cls + *cls / 2) {
-        void* p = it->second;
-        *cls = it->first;
-        held -= it->first;
-        free_blocks.erase(it);
-        return p;
-    }
+void SlabStore::prepare(size_t expect) {
+    const size_t n1 = slabs.size();
+    // keep a single slab that holds the table and is not more than 4x too big
+    if (n1 == 1 && slabs[0].cap >= expect && slabs[0].cap <= 4 * expect + (size_t(64) << 20)) return;
+    release();
+    const size_t cap = ((expect + expect / 4 + (size_t(8) << 20)) + 0xFFFFF) & ~size_t(0xFFFFF);
     void* p = nullptr;
-    if (cudaMalloc(&p, *cls) != cudaSuccess) {
+    if (cudaMalloc(&p, cap) != cudaSuccess) {
         cudaGetLastError();
-        trim(0);  // out of memory: release every cached block and retry once
-        if (cudaMalloc(&p, *cls) != cudaSuccess) {
-            cudaGetLastError();
-            return nullptr;
-        }
+        return;  // DeviceArena::alloc makes smaller slabs as it goes
     }
-    return p;
+    slabs.push_back({static_cast<char*>(p), cap});
 }
 
-void BlockPool::give(void* p, size_t cls) {
-    free_blocks.emplace(cls, p);
-    held += cls;
-}
-
-void BlockPool::trim(size_t keep_bytes) {
-    while (held > keep_bytes && !free_blocks.empty()) {
-        auto it = std::prev(free_blocks.end());
-        cudaFree(it->second);
-        held -= it->first;
-        free_blocks.erase(it);
-    }
-}
-
-BlockPool::~BlockPool() { trim(0); }
-
-DeviceArena::~DeviceArena() {
-    for (auto& b : ptrs) {
-        if (pool) pool->give(b.first, b.second);
-        else cudaFree(b.first);
-    }
+void SlabStore::release() {
+    for (auto& sl : slabs) cudaFree(sl.p);
+    slabs.clear();
 }
 
 template <typename T>
 T* DeviceArena::alloc(size_t n) {
     if (n == 0) n = 1;
-    const size_t want = n * sizeof(T);
-    size_t cls = want;
-    void* p = nullptr;
-    if (pool) {
-        p = pool->take(want, &cls);
-    } else if (cudaMalloc(&p, want) != cudaSuccess) {
-        p = nullptr;
+    const size_t want = (n * sizeof(T) + 255) & ~size_t(255);
+    for (;;) {
+        if (slab < store->slabs.size()) {
+            SlabStore::Slab& sl = store->slabs[slab];
+            if (off + want <= sl.cap) {
+                char* p = sl.p + off;
+                off += want;
+                bytes += want;
+                if (cudaMemsetAsync(p, 0, want, stream) != cudaSuccess) throw std::runtime_error("memset failed");
+                return reinterpret_cast<T*>(p);
+            }
+            ++slab;
+            off = 0;
+            continue;
+        }
+        // the table outgrew the slabs: another one (the next rebuild makes one
+        // slab of the whole size)
+        void* p = nullptr;
+        const size_t cap = std::max(want, size_t(64) << 20);
+        if (cudaMalloc(&p, cap) != cudaSuccess) {
+            cudaGetLastError();
+            throw std::runtime_error("cudaMalloc failed");
+        }
+        store->slabs.push_back({static_cast<char*>(p), cap});
     }
-    if (!p) throw std::runtime_error("cudaMalloc failed");
-    cudaMemset(p, 0, want);
-    ptrs.emplace_back(p, cls);
-    bytes += want;
-    return static_cast<T*>(p);
+}
+
+void* PinnedStaging::put(const void* src, size_t bytes) {
+    const size_t want = (bytes + 255) & ~size_t(255);
+    while (blk < blocks.size() && off + want > blocks[blk].second) {
+        ++blk;
+        off = 0;
+    }
+    if (blk == blocks.size()) {
+        void* p = nullptr;
+        const size_t cap = std::max(want, size_t(64) << 20);
+        if (cudaMallocHost(&p, cap) != cudaSuccess) {
+            cudaGetLastError();
+            throw std::runtime_error("pinned staging alloc failed");
+        }
+        blocks.emplace_back(static_cast<char*>(p), cap);
+        off = 0;
+    }
+    char* dst = blocks[blk].first + off;
+    std::memcpy(dst, src, bytes);
+    off += want;
+    return dst;
+}
+
+void PinnedStaging::trim(size_t keep) {
+    size_t held = 0;
+    size_t k = 0;
+    for (; k < blocks.size() && held + blocks[k].second <= keep; ++k) held += blocks[k].second;
+    for (size_t m = k; m < blocks.size(); ++m) cudaFreeHost(blocks[m].first);
+    blocks.resize(k);
+    reset();
 }
 
 namespace {
@@ -189,6 +197,10 @@ Batch::~Batch() {
     }
     plans_.clear();
     if (flush_buf_) cudaFree(flush_buf_);
+    if (h_st_) cudaFreeHost(h_st_);
+    if (h_tgt_) cudaFreeHost(h_tgt_);
+    if (h_and_flag_) cudaFreeHost(h_and_flag_);
+    if (h_and_v_) cudaFreeHost(h_and_v_);
     for (cudaEvent_t e : ev_pool_) cudaEventDestroy(e);
     if (ev_fork_) cudaEventDestroy(ev_fork_);
     if (ev_join_) cudaEventDestroy(ev_join_);
@@ -205,16 +217,10 @@ void Batch::free_device() {
     // cuFFT plans depend only on the mesh size: they are kept across table
     // rebuilds (an admission or release rebuilds the table) and destroyed with
     // the batch
+    // the pinned mirrors are kept (cudaFreeHost synchronises the device and
+    // costs milliseconds); the next table grows them when it needs more
     arena_.reset();
-    if (h_st_) cudaFreeHost(h_st_);
-    h_st_ = nullptr;
-    if (h_tgt_) cudaFreeHost(h_tgt_);
-    h_tgt_ = nullptr;
     st_fresh_ = false;
-    if (h_and_flag_) cudaFreeHost(h_and_flag_);
-    if (h_and_v_) cudaFreeHost(h_and_v_);
-    h_and_flag_ = nullptr;
-    h_and_v_ = nullptr;
     packed_ = false;
     used_bytes_ = 0;
 }
@@ -572,7 +578,7 @@ int Batch::replica_index(int slot) const {
 int Batch::pack() {
     CK(cudaSetDevice(device_));
     // carry the device state of replicas that were already packed
-    if (arena_ && h_st_) {
+    if (arena_) {
         CK(cudaStreamSynchronize(stream_));
         launch_finalize_velocities(dev_, stream_, &launches_);
         CK(cudaMemcpyAsync(h_st_, d_st_, sizeof(RepState) * order_.size(), cudaMemcpyDeviceToHost, stream_));
@@ -691,9 +697,16 @@ int Batch::pack() {
     }
     n_pme_blocks_ = pme_blocks;
     n_conv_blocks_ = conv_blocks;
+    // one slab for the table, sized from the footprint estimates scaled by
+    // what the last table actually took of its estimate
+    size_t fp_sum = 0;
+    for (int k = 0; k < R; ++k) fp_sum += static_cast<size_t>(footprint(reps_[order_[k]]->sys));
+    slabs_.prepare(static_cast<size_t>(static_cast<double>(fp_sum) * std::max(1.0, fp_ratio_)));
+    staging_.reset();
     try {
         arena_ = std::make_unique<DeviceArena>();
-        arena_->pool = &pool_;
+        arena_->store = &slabs_;
+        arena_->stream = stream_;
         DeviceArena& A = *arena_;
         Dev& d = dev_;
         d = Dev{};
@@ -792,7 +805,6 @@ int Batch::pack() {
         std::vector<int4> iijkl;
         std::vector<double2> ikp;
         std::vector<int2> ex;
-        std::vector<std::vector<int>> exl(n_atoms);
         std::vector<int2> cij;              // constraints grouped by connected atom set
         std::vector<double> cdist;
         std::vector<int> cgb(1, 0), cgr;    // group begin offsets, group replica
@@ -908,14 +920,7 @@ int Batch::pack() {
                     cgr.push_back(k);
                 }
             }
-            for (size_t t = 0; t < s.ei.size(); ++t) {
-                const int gi = a0 + s.ei[t], gj = a0 + s.ej[t];
-                ex.push_back(make_int2(gi, gj));
-                if (gi != gj) {
-                    exl[gi].push_back(gj);
-                    exl[gj].push_back(gi);
-                }
-            }
+            for (size_t t = 0; t < s.ei.size(); ++t) ex.push_back(make_int2(a0 + s.ei[t], a0 + s.ej[t]));
             if (P.flags & F_PME) {
                 const int K = P.pme_K;
                 for (int kk = 0; kk < K; ++kk) {
@@ -938,16 +943,39 @@ int Batch::pack() {
             }
             hrep[k] = P;
         }
-        // exclusion CSR
+        // exclusion CSR: each atom's excluded partners, ascending, without
+        // repeats (counted, filled, then each short row sorted in place)
         std::vector<int> ex_start(n_atoms + 1, 0), ex_list;
-        for (long long a = 0; a < n_atoms; ++a) {
-            std::sort(exl[a].begin(), exl[a].end());
-            exl[a].erase(std::unique(exl[a].begin(), exl[a].end()), exl[a].end());
-            ex_start[a + 1] = ex_start[a] + static_cast<int>(exl[a].size());
-            ex_list.insert(ex_list.end(), exl[a].begin(), exl[a].end());
+        {
+            std::vector<int> cnt(n_atoms + 1, 0);
+            for (const int2& e : ex)
+                if (e.x != e.y) {
+                    ++cnt[e.x + 1];
+                    ++cnt[e.y + 1];
+                }
+            for (long long a = 0; a < n_atoms; ++a) cnt[a + 1] += cnt[a];
+            std::vector<int> raw(cnt[n_atoms]);
+            std::vector<int> fill(cnt.begin(), cnt.end() - 1);
+            for (const int2& e : ex)
+                if (e.x != e.y) {
+                    raw[fill[e.x]++] = e.y;
+                    raw[fill[e.y]++] = e.x;
+                }
+            ex_list.reserve(raw.size());
+            for (long long a = 0; a < n_atoms; ++a) {
+                auto b = raw.begin() + cnt[a], e = raw.begin() + cnt[a + 1];
+                std::sort(b, e);
+                e = std::unique(b, e);
+                ex_list.insert(ex_list.end(), b, e);
+                ex_start[a + 1] = static_cast<int>(ex_list.size());
+            }
         }
+        // staged in pinned memory, copied in order on the main stream after the
+        // zero fills of the arena
         auto up = [&](void* dst, const void* src, size_t bytes) {
-            if (bytes && cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice) != cudaSuccess)
+            if (!bytes) return;
+            const void* h = staging_.put(src, bytes);
+            if (cudaMemcpyAsync(dst, h, bytes, cudaMemcpyHostToDevice, stream_) != cudaSuccess)
                 throw std::runtime_error("upload failed");
         };
         up(d.x, hx.data(), 8 * n_atoms);
@@ -1064,9 +1092,18 @@ int Batch::pack() {
             d_and_v_ = A.alloc<double>(3 * n_atoms);
             d.and_flag = d_and_flag_;
             d.and_v = d_and_v_;
-            if (cudaMallocHost(&h_and_flag_, 4 * n_atoms) != cudaSuccess ||
-                cudaMallocHost(&h_and_v_, 24 * n_atoms) != cudaSuccess)
-                throw std::runtime_error("pinned alloc failed");
+            if (n_atoms > h_and_cap_) {
+                if (h_and_flag_) cudaFreeHost(h_and_flag_);
+                if (h_and_v_) cudaFreeHost(h_and_v_);
+                h_and_flag_ = nullptr;
+                h_and_v_ = nullptr;
+                h_and_cap_ = 0;
+                const long long cap = n_atoms + n_atoms / 4;
+                if (cudaMallocHost(&h_and_flag_, 4 * cap) != cudaSuccess ||
+                    cudaMallocHost(&h_and_v_, 24 * cap) != cudaSuccess)
+                    throw std::runtime_error("pinned alloc failed");
+                h_and_cap_ = cap;
+            }
         }
         up(d_rep_, hrep.data(), sizeof(Rep) * R);
         std::vector<RepState> hst(R);
@@ -1077,15 +1114,26 @@ int Batch::pack() {
         }
         up(d_st_, hst.data(), sizeof(RepState) * R);
         used_bytes_ = static_cast<long long>(A.bytes);
-        // blocks left over from a larger table are kept up to the table's own
-        // size; beyond that they are released
-        pool_.trim(std::max<size_t>(A.bytes, size_t(1) << 28));
+        fp_ratio_ = fp_sum ? static_cast<double>(A.bytes) / static_cast<double>(fp_sum) : 1.0;
     } catch (const std::exception& e) {
+        cudaStreamSynchronize(stream_);
         arena_.reset();
         return fail(DMDGPU_ERR_OOM, std::string("device allocation/upload failed: ") + e.what());
     }
-    CK(cudaMallocHost(&h_st_, sizeof(RepState) * R));
-    CK(cudaMallocHost(&h_tgt_, sizeof(long long) * R));
+    // every zero fill and upload done; the staging blocks beyond 256 MB go back
+    CK(cudaStreamSynchronize(stream_));
+    staging_.trim(size_t(256) << 20);
+    if (R > h_st_cap_) {
+        if (h_st_) cudaFreeHost(h_st_);
+        if (h_tgt_) cudaFreeHost(h_tgt_);
+        h_st_ = nullptr;
+        h_tgt_ = nullptr;
+        h_st_cap_ = 0;
+        const int cap = (R + 63) & ~63;
+        CK(cudaMallocHost(&h_st_, sizeof(RepState) * cap));
+        CK(cudaMallocHost(&h_tgt_, sizeof(long long) * cap));
+        h_st_cap_ = cap;
+    }
     st_fresh_ = false;
     // cuFFT plans per mesh size (normally made at admission already)
     for (int k = 0; k < R; ++k) {
@@ -1704,6 +1752,19 @@ int Batch::step_timed(int n, long long flush_bytes, dmdgpu_timing* out) {
     int rc = sync_status();
     out->kernel_launches = captured;
     return rc;
+}
+
+void Batch::launch_info(dmdgpu_launch_info* out) const {
+    *out = dmdgpu_launch_info{};
+    out->packed = packed_ && !order_.empty() ? 1 : 0;
+    if (!out->packed) return;
+    out->nb_form = nb_form_ == NB_CLUSTER8 ? DMDGPU_NB_CLUSTER8 : DMDGPU_NB_CHUNK32;
+    out->nb_blocks_per_sm = fp64_ ? 8 : nb_blocks_per_sm_;
+    out->tuned = tuned_ ? 1 : 0;
+    out->min_image_kernel = fp64_ ? 0 : dev_.mi_split;  // the FP64 kernel always takes it
+    out->n_replicas = static_cast<int32_t>(order_.size());
+    out->n_atoms = dev_.n_atoms;
+    out->launches_per_step = per_step_launches_;
 }
 
 int Batch::active() const {

@@ -67,27 +67,42 @@ struct HostRep {
     bool on_device = false;    // packed into the current device table (its state lives there)
 };
 
-// Device blocks kept for reuse across table rebuilds, by size: a serving loop
-// rebuilds its table at every admission and release, and freeing and
-// allocating every array each time stalls the device (cudaFree waits for it
-// and unmaps; measured up to ~0.7 s in one rebuild).  Sizes are rounded up to
-// classes 2^(k/4) apart, so a rebuilt table of a similar size finds blocks.
-struct BlockPool {
-    std::multimap<size_t, void*> free_blocks;  // size class -> block
-    size_t held = 0;                           // bytes of the blocks in free_blocks
-    void* take(size_t bytes, size_t* cls);
-    void give(void* p, size_t cls);
-    void trim(size_t keep_bytes);              // frees the largest blocks down to keep_bytes
-    ~BlockPool();
+// Device memory of the packed table: slabs kept by the batch across table
+// rebuilds, handed out by a bump pointer.  A serving loop rebuilds its table at
+// every admission and release; cudaMalloc and cudaFree of every array each
+// time stall the device (cudaFree waits for it and unmaps: measured up to
+// ~0.7 s in one rebuild), so the table reuses one slab while it fits and a
+// new slab is made only when it grows (or shrinks far below it).
+struct SlabStore {
+    struct Slab {
+        char* p;
+        size_t cap;
+    };
+    std::vector<Slab> slabs;
+    void prepare(size_t expect);  // one slab of at least `expect` bytes
+    void release();
+    ~SlabStore() { release(); }
 };
 
 struct DeviceArena {
-    std::vector<std::pair<void*, size_t>> ptrs;  // block and its size class
-    size_t bytes = 0;                            // bytes requested (budget accounting)
-    BlockPool* pool = nullptr;                   // blocks return here instead of cudaFree
-    ~DeviceArena();
+    SlabStore* store = nullptr;
+    cudaStream_t stream = nullptr;  // zero fills are issued here, before the uploads
+    size_t slab = 0, off = 0;       // bump position
+    size_t bytes = 0;               // bytes handed out (budget accounting)
     template <typename T>
     T* alloc(size_t n);
+};
+
+// Pinned host blocks the table uploads are staged in (kept across rebuilds):
+// every upload is one asynchronous copy on the main stream, with one
+// synchronisation for all of them.
+struct PinnedStaging {
+    std::vector<std::pair<char*, size_t>> blocks;
+    size_t blk = 0, off = 0;
+    void* put(const void* src, size_t bytes);
+    void reset() { blk = off = 0; }
+    void trim(size_t keep);       // frees the later blocks beyond `keep` bytes
+    ~PinnedStaging() { trim(0); }
 };
 
 class Batch {
@@ -123,6 +138,7 @@ class Batch {
 
     long long used_bytes() const { return used_bytes_; }
     long long launches() const { return launches_; }
+    void launch_info(dmdgpu_launch_info* out) const;
     int active() const;
     const std::string& error() const { return err_; }
     int fail(int code, const std::string& msg);
@@ -157,14 +173,17 @@ class Batch {
     bool capture_error_ = false;
     std::vector<std::unique_ptr<HostRep>> reps_;   // indexed by slot (nullptr = free)
     std::vector<int> order_;                        // packed replica index -> slot
-    BlockPool pool_;                                 // declared before arena_: outlives it
+    SlabStore slabs_;                                // declared before arena_: outlives it
     std::unique_ptr<DeviceArena> arena_;
+    PinnedStaging staging_;
+    double fp_ratio_ = 1.0;                          // last table's bytes / its footprint estimate
     Dev dev_{};
     Rep* d_rep_ = nullptr;
     RepState* d_st_ = nullptr;
     RepState* h_st_ = nullptr;                      // pinned mirror of the state table
     bool st_fresh_ = false;                         // h_st_ equals the device table (no work since)
     long long* h_tgt_ = nullptr;                    // pinned step targets for extend_targets
+    int h_st_cap_ = 0;                              // replicas h_st_ / h_tgt_ hold
     int* d_bin_rep_ = nullptr;
     int n_pme_blocks_ = 0, n_conv_blocks_ = 0;
     bool any_cons_ = false;  // some replica has distance constraints
@@ -219,6 +238,7 @@ class Batch {
     // Andersen REF override buffers
     int* h_and_flag_ = nullptr;
     double* h_and_v_ = nullptr;
+    long long h_and_cap_ = 0;                       // atoms h_and_flag_ / h_and_v_ hold
     int* d_and_flag_ = nullptr;
     double* d_and_v_ = nullptr;
 };

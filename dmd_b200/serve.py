@@ -70,6 +70,12 @@ def job_mix(n_jobs: int, rate: float, seed: int = 2025, scale: float = 1.0):
     return jobs
 
 
+def _pcts(v):
+    if not v:
+        return None
+    return {"p50": 1e3 * float(np.percentile(v, 50)), "p99": 1e3 * float(np.percentile(v, 99)), "calls": len(v)}
+
+
 def serve(jobs, budget_bytes=150 * 10**9, precision="mixed", profile="phys", chunk=100,
           virtual=False):
     """Run the job stream through one continuously batched device batch.
@@ -80,6 +86,8 @@ def serve(jobs, budget_bytes=150 * 10**9, precision="mixed", profile="phys", chu
     queue = sorted(jobs, key=lambda j: j.arrival)
     running: dict[int, Job] = {}
     step_lat = []              # seconds per step of each device call
+    rebuilt = []               # whether that call rebuilt the device table first
+    configs: dict = {}         # launch configurations the rebuilt tables ran with -> calls
     t0 = time.perf_counter()
     clock_steps = 0
     atom_steps = 0
@@ -109,6 +117,7 @@ def serve(jobs, budget_bytes=150 * 10**9, precision="mixed", profile="phys", chu
                 time.sleep(max(0.0, queue[0].arrival - now()))
             continue
         live = sum(j.n_atoms for j in running.values())
+        rebuilt.append(dirty)
         if dirty:
             # the device table is rebuilt at this call: running jobs carry their
             # state over and rebuild their pair lists (Engine.repack alone)
@@ -119,6 +128,10 @@ def serve(jobs, budget_bytes=150 * 10**9, precision="mixed", profile="phys", chu
         t = time.perf_counter()
         b.step(chunk)
         dt = time.perf_counter() - t
+        if rebuilt[-1]:
+            li = b.launch_info()
+            key = (li["nb_form"], li["nb_blocks_per_sm"], li["tuned"], li["min_image_kernel"])
+            configs[key] = configs.get(key, 0) + 1
         step_lat.append(dt / chunk)
         clock_steps += chunk
         atom_steps += live * chunk
@@ -142,8 +155,16 @@ def serve(jobs, budget_bytes=150 * 10**9, precision="mixed", profile="phys", chu
         "wall_s": wall,
         "step_latency_ms": {"p50": 1e3 * float(np.percentile(step_lat, 50)),
                             "p99": 1e3 * float(np.percentile(step_lat, 99))},
+        # the same split by calls that rebuilt the table first (an admission or
+        # release) and calls that did not: the spread of the steady calls is
+        # the job mix (how many atoms run at once), the difference between the
+        # two the cost of the rebuilds
+        "step_latency_ms_steady": _pcts([t for t, r in zip(step_lat, rebuilt) if not r]),
+        "step_latency_ms_rebuild": _pcts([t for t, r in zip(step_lat, rebuilt) if r]),
         "job_latency": {"p50": float(np.percentile(done, 50)), "p99": float(np.percentile(done, 99)),
                         "unit": "steps" if virtual else "s"},
+        "launch_configs": [{"nb_form": k[0], "nb_blocks_per_sm": k[1], "tuned": k[2],
+                            "min_image_kernel": k[3], "tables": v} for k, v in sorted(configs.items())],
         "work_atom_steps": done_steps,
         "padded_atom_steps": atom_steps,
     }

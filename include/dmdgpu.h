@@ -222,6 +222,24 @@ int64_t dmdgpu_kernel_launches(dmdgpu_ctx *ctx);
  * caller can order its own work or record timing events on it. */
 void *dmdgpu_stream(dmdgpu_ctx *ctx);
 
+/* The launch configuration the current device table runs with: the knobs the
+ * autotuner chose (or took from its cache) and the forms the options and the
+ * systems select.  Valid after the first step (the table is built then). */
+typedef struct dmdgpu_launch_info {
+    int32_t packed;            /* 1: a device table exists (the fields below describe it) */
+    int32_t nb_form;           /* DMDGPU_NB_CHUNK32 or DMDGPU_NB_CLUSTER8 (FP64: CHUNK32) */
+    int32_t nb_blocks_per_sm;  /* persistent pair-kernel blocks per SM */
+    int32_t tuned;             /* 1: blocks per SM measured (now or cached) for this kind
+                                  of table; 0: the untuned default */
+    int32_t min_image_kernel;  /* 1: boxes narrower than twice the list cutoff (or under
+                                  a barostat) also run the minimum-image pair kernel */
+    int32_t n_replicas;
+    int64_t n_atoms;
+    int64_t launches_per_step; /* kernels in one captured step */
+} dmdgpu_launch_info;
+
+int dmdgpu_get_launch_info(dmdgpu_ctx *ctx, dmdgpu_launch_info *out);
+
 /* Device timing of a run of steps. */
 typedef struct dmdgpu_timing {
     double step_ms;            /* summed device time of the n steps (flushes excluded) */
@@ -313,6 +331,7 @@ int dmdgpu_batch_get_state(dmdgpu_batch *b, int32_t slot, int32_t which, double 
 int dmdgpu_batch_get_scalars(dmdgpu_batch *b, int32_t slot, dmdgpu_scalars *out);
 int dmdgpu_batch_release(dmdgpu_batch *b, int32_t slot);
 int64_t dmdgpu_batch_used_bytes(dmdgpu_batch *b);
+int dmdgpu_batch_get_launch_info(dmdgpu_batch *b, dmdgpu_launch_info *out);
 int32_t dmdgpu_batch_active(dmdgpu_batch *b);
 const char *dmdgpu_batch_last_error(const dmdgpu_batch *b);
 void dmdgpu_batch_destroy(dmdgpu_batch *b);

@@ -409,3 +409,53 @@ def test_cluster_form(oracle, system):
     b.run_n(20)
     assert np.array_equal(a.positions, b.positions)
     assert a.potential_energy == b.potential_energy
+
+
+@pytest.mark.parametrize("form", ["chunk32", "cluster8"])
+def test_narrow_box_minimum_image(oracle, form):
+    """A box narrower than twice the list cutoff (100 flexible waters, 1.44 nm
+    against 2 x 1.1 nm): the nearest image of a listed pair changes between
+    list builds, so the mixed path runs these replicas through the
+    minimum-image pair kernel and follows the oracle, which takes the minimum
+    image at every evaluation.  A wide box runs without it; a barostat (which
+    may shrink the box) turns it on."""
+    c = W.water_box(n_mol=100, box=(100 / 33.4) ** (1 / 3), seed=3, spacing=0.1).config()
+    c.thermostat.type = "berendsen"
+    c.dt = 0.001
+    oe = oracle.engine(c, "phys")
+    eng = _engine(c, "mixed", "phys", nb_form=form)
+    L = c.box_size
+    for k in range(3):
+        oe.step(4)
+        eng.run_n(4)
+        assert np.abs(eng.positions - oe.get(0)).max() / L < 1e-6, k
+        assert rel_rms(eng.velocities, oe.get(1)) < 1e-4, k
+    info = eng.launch_info()
+    assert info["packed"] and info["min_image_kernel"], info
+    wide = _engine(_water(1000), "mixed", "phys", nb_form=form)
+    wide.run_n(2)
+    assert not wide.launch_info()["min_image_kernel"]
+    c2 = _water(1000)
+    c2.barostat.type = "berendsen"
+    c2.barostat.tau = 0.5
+    npt = _engine(c2, "mixed", "phys", nb_form=form)
+    npt.run_n(2)
+    assert npt.launch_info()["min_image_kernel"]
+    F, _ = npt.compute_forces()
+    F_o, _ = oracle.forces(c2, "phys")
+    assert rel_rms(F, F_o) < TOL["mixed"]
+
+
+def test_launch_info_reports_tuned_shape():
+    """The launch configuration query after a run: the default chunk form, a
+    blocks-per-SM count inside the tuner's candidates, and the captured step's
+    kernel count equal to what a timed step reports."""
+    eng = _engine(_water(1000), "mixed", "phys")
+    eng.run_n(40)
+    info = eng.launch_info()
+    assert info["packed"] and info["nb_form"] == "chunk32"
+    assert info["nb_blocks_per_sm"] in (1, 2, 3)
+    assert info["n_replicas"] == 1 and info["n_atoms"] == 3000
+    t = eng.step_timed(5, 0)
+    assert info["launches_per_step"] > 0
+    assert t["kernel_launches"] >= 5 * info["launches_per_step"] - 5
