@@ -439,9 +439,8 @@ def test_narrow_box_minimum_image(oracle, form):
     c2.barostat.type = "berendsen"
     c2.barostat.tau = 0.5
     npt = _engine(c2, "mixed", "phys", nb_form=form)
-    npt.run_n(2)
+    F, _ = npt.compute_forces()  # at the starting configuration, as the oracle's
     assert npt.launch_info()["min_image_kernel"]
-    F, _ = npt.compute_forces()
     F_o, _ = oracle.forces(c2, "phys")
     assert rel_rms(F, F_o) < TOL["mixed"]
 
