@@ -174,17 +174,25 @@ Batch::Batch(const dmdgpu_options& opt, long long budget) : opt_(opt), budget_(b
     device_ = opt.device;
     if (cudaSetDevice(device_) != cudaSuccess) throw std::runtime_error("cudaSetDevice failed");
     cudaDeviceGetAttribute(&n_sm_, cudaDevAttrMultiProcessorCount, device_);
-    // The main stream (list rebuild, pair kernel: the critical path) has the
-    // higher priority; the bonded / PME chain on aux_stream_ fills what is left.
+    // The pair kernel is the longest branch of a force evaluation; the bonded
+    // terms and the PME chain (a sequence of short kernels ending in the
+    // gather, which the step waits for) run beside it.  The PME and bonded
+    // streams have the higher priority, so that their blocks are dispatched
+    // first wherever an SM has room (the main stream's own kernels are
+    // ordered by dependencies); in the step graph every kernel node but the
+    // pair kernel's gets the higher priority.
+    configure_nonbonded_kernels();
     int prio_lo = 0, prio_hi = 0;
     if (cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi) != cudaSuccess ||
-        cudaStreamCreateWithPriority(&stream_, cudaStreamNonBlocking, prio_hi) != cudaSuccess ||
-        cudaStreamCreateWithPriority(&aux_stream_, cudaStreamNonBlocking, prio_lo) != cudaSuccess ||
-        cudaStreamCreateWithPriority(&bond_stream_, cudaStreamNonBlocking, prio_lo) != cudaSuccess ||
+        cudaStreamCreateWithPriority(&stream_, cudaStreamNonBlocking, prio_lo) != cudaSuccess ||
+        cudaStreamCreateWithPriority(&aux_stream_, cudaStreamNonBlocking, prio_hi) != cudaSuccess ||
+        cudaStreamCreateWithPriority(&bond_stream_, cudaStreamNonBlocking, prio_hi) != cudaSuccess ||
         cudaEventCreateWithFlags(&ev_fork_, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&ev_join_, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&ev_join_b_, cudaEventDisableTiming) != cudaSuccess)
         throw std::runtime_error("cudaStreamCreate failed");
+    prio_lo_ = prio_lo;
+    prio_hi_ = prio_hi;
 }
 
 Batch::~Batch() {
@@ -1304,6 +1312,34 @@ void Batch::andersen_ref_prepare() {
     cudaMemcpyAsync(d_and_v_, h_and_v_, sizeof(double) * 3 * dev_.n_atoms, cudaMemcpyHostToDevice, stream_);
 }
 
+// Kernel-node priorities of a captured step: the pair kernel low, every other
+// kernel (bonded terms, the PME chain, cuFFT's kernels, integration) high.
+// The graph is instantiated with cudaGraphInstantiateFlagUseNodePriority.
+void Batch::set_node_priorities(cudaGraph_t g) {
+    size_t n = 0;
+    if (cudaGraphGetNodes(g, nullptr, &n) != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        return;
+    }
+    std::vector<cudaGraphNode_t> nodes(n);
+    if (cudaGraphGetNodes(g, nodes.data(), &n) != cudaSuccess) {
+        cudaGetLastError();
+        return;
+    }
+    for (cudaGraphNode_t node : nodes) {
+        cudaGraphNodeType t;
+        if (cudaGraphNodeGetType(node, &t) != cudaSuccess || t != cudaGraphNodeTypeKernel) continue;
+        cudaKernelNodeParams kp{};
+        bool nb = false;
+        if (cudaGraphKernelNodeGetParams(node, &kp) == cudaSuccess) nb = is_nonbonded_kernel(kp.func);
+        else cudaGetLastError();  // a kernel launched through the driver API (cuFFT)
+        cudaKernelNodeAttrValue v{};
+        v.priority = nb ? prio_lo_ : prio_hi_;
+        if (cudaGraphKernelNodeSetAttribute(node, cudaKernelNodeAttributePriority, &v) != cudaSuccess)
+            cudaGetLastError();
+    }
+}
+
 int Batch::run_steps(int n) {
     st_fresh_ = false;  // device work follows: the host mirror is stale
     if (n <= 0) return DMDGPU_OK;
@@ -1359,7 +1395,8 @@ int Batch::run_steps(int n) {
             return fail(DMDGPU_ERR_GPU, "conditional-node capture failed");
         }
         per_step_launches_ = launches_ - before;
-        CK(cudaGraphInstantiate(&graph_, g, 0));
+        set_node_priorities(g);
+        CK(cudaGraphInstantiate(&graph_, g, cudaGraphInstantiateFlagUseNodePriority));
         cudaGraphDestroy(g);
         graph_dirty_ = false;
     }
@@ -1672,8 +1709,17 @@ void Batch::record(cudaEvent_t e, cudaStream_t st) {
     else cudaEventRecord(e, st);
 }
 
-// n steps as one captured graph with timing events around every step and every
-// non-bonded / PME launch; optional L2 flush between steps (outside the events).
+// n steps with device timing.  One step is captured as a graph with event
+// record nodes around every pair-kernel launch and every PME chain; the graph
+// is launched n times from the host, with the step's own events recorded on
+// the main stream between launches (and the optional L2 flush before each,
+// outside the events), and before each launch its event nodes are pointed at
+// fresh events (cudaGraphExecEventRecordNodeSetEvent), so every launch's
+// intervals are kept.  Capturing all n steps into one graph instead, with
+// their events, changes how the graph's branches are scheduled (measured on
+// water 30k: a step period of ~143 us against ~124 us for the step graph
+// that run_n launches); launching the one-step graph keeps the step as
+// run_n runs it.
 int Batch::step_timed(int n, long long flush_bytes, dmdgpu_timing* out) {
     st_fresh_ = false;  // device work follows: the host mirror is stale
     CK(cudaSetDevice(device_));
@@ -1691,36 +1737,24 @@ int Batch::step_timed(int n, long long flush_bytes, dmdgpu_timing* out) {
         --n;
         if (n == 0) return sync_status();
     }
+    if (any_andersen_ref_) return fail(DMDGPU_ERR_INVALID, "timed steps need the step graph (not with a host-drawn Andersen stream)");
     if (flush_bytes > 0 && flush_bytes != flush_bytes_) {
         if (flush_buf_) cudaFree(flush_buf_);
         flush_buf_ = nullptr;
         CK(cudaMalloc(&flush_buf_, flush_bytes));
         flush_bytes_ = flush_bytes;
     }
-    const size_t need = static_cast<size_t>(8 * n + 8);
-    while (ev_pool_.size() < need) {  // events must exist before capture
-        cudaEvent_t ev;
-        CK(cudaEventCreate(&ev));
-        ev_pool_.push_back(ev);
-    }
+    // capture one step with its pair-kernel and PME events
     ev_used_ = 0;
-    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> nb, pme, steps;
-    prof_nb_ = &nb;
-    prof_pme_ = &pme;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> nb0, pme0;
+    prof_nb_ = &nb0;
+    prof_pme_ = &pme0;
     cudaGraph_t g;
-    cudaGraphExec_t ge;
     const long long before = launches_;
     capture_error_ = false;
     cudaError_t e = cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal);
     if (e == cudaSuccess) {
-        for (int i = 0; i < n; ++i) {
-            if (flush_buf_) cudaMemsetAsync(flush_buf_, i & 0xff, flush_bytes_, stream_);
-            cudaEvent_t a = next_event(), b = next_event();
-            record(a, stream_);
-            enqueue_step();
-            record(b, stream_);
-            steps.emplace_back(a, b);
-        }
+        enqueue_step();
         e = cudaStreamEndCapture(stream_, &g);
     }
     prof_nb_ = nullptr;
@@ -1729,12 +1763,82 @@ int Batch::step_timed(int n, long long flush_bytes, dmdgpu_timing* out) {
         cudaGetLastError();
         return fail(DMDGPU_ERR_GPU, std::string("timed capture failed: ") + cudaGetErrorString(e));
     }
-    const long long captured = launches_ - before;
-    CK(cudaGraphInstantiate(&ge, g, 0));
-    cudaGraphDestroy(g);
-    CK(cudaGraphLaunch(ge, stream_));
-    CK(cudaStreamSynchronize(stream_));
+    const long long per_step = launches_ - before;
+    launches_ = before;
+    // the event record nodes, in the order of nb0 / pme0 (start, end)
+    std::vector<cudaGraphNode_t> nb_nodes(2 * nb0.size()), pme_nodes(2 * pme0.size());
+    {
+        size_t nn = 0;
+        cudaGraphGetNodes(g, nullptr, &nn);
+        std::vector<cudaGraphNode_t> nodes(nn);
+        cudaGraphGetNodes(g, nodes.data(), &nn);
+        for (cudaGraphNode_t node : nodes) {
+            cudaGraphNodeType t;
+            if (cudaGraphNodeGetType(node, &t) != cudaSuccess || t != cudaGraphNodeTypeEventRecord) continue;
+            cudaEvent_t ev = nullptr;
+            if (cudaGraphEventRecordNodeGetEvent(node, &ev) != cudaSuccess) continue;
+            for (size_t k = 0; k < nb0.size(); ++k) {
+                if (ev == nb0[k].first) nb_nodes[2 * k] = node;
+                if (ev == nb0[k].second) nb_nodes[2 * k + 1] = node;
+            }
+            for (size_t k = 0; k < pme0.size(); ++k) {
+                if (ev == pme0[k].first) pme_nodes[2 * k] = node;
+                if (ev == pme0[k].second) pme_nodes[2 * k + 1] = node;
+            }
+        }
+        for (cudaGraphNode_t node : nb_nodes)
+            if (!node) {
+                cudaGraphDestroy(g);
+                return fail(DMDGPU_ERR_GPU, "timed capture: pair-kernel event nodes not found");
+            }
+        for (cudaGraphNode_t node : pme_nodes)
+            if (!node) {
+                cudaGraphDestroy(g);
+                return fail(DMDGPU_ERR_GPU, "timed capture: PME event nodes not found");
+            }
+    }
+    set_node_priorities(g);
+    cudaGraphExec_t ge;
+    e = cudaGraphInstantiate(&ge, g, cudaGraphInstantiateFlagUseNodePriority);
+    if (e != cudaSuccess) {
+        cudaGraphDestroy(g);
+        return check_cuda(e, "cudaGraphInstantiate");
+    }
+    // g (whose nodes name the exec graph's event nodes) lives until the end
+    // events for every launch: the step's pair, then the nodes' pairs
+    const size_t per_launch = 2 + nb_nodes.size() + pme_nodes.size();
+    const size_t need = ev_used_ + per_launch * static_cast<size_t>(n);
+    while (ev_pool_.size() < need) {
+        cudaEvent_t ev;
+        CK(cudaEventCreate(&ev));
+        ev_pool_.push_back(ev);
+    }
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> nb, pme, steps;
+    auto point = [&](const std::vector<cudaGraphNode_t>& nodes, std::vector<std::pair<cudaEvent_t, cudaEvent_t>>& out) {
+        for (size_t k = 0; k < nodes.size() && e == cudaSuccess; k += 2) {
+            const cudaEvent_t x = next_event(), y = next_event();
+            e = cudaGraphExecEventRecordNodeSetEvent(ge, nodes[k], x);
+            if (e == cudaSuccess) e = cudaGraphExecEventRecordNodeSetEvent(ge, nodes[k + 1], y);
+            out.emplace_back(x, y);
+        }
+    };
+    for (int i = 0; i < n && e == cudaSuccess; ++i) {
+        if (flush_buf_) cudaMemsetAsync(flush_buf_, i & 0xff, flush_bytes_, stream_);
+        const cudaEvent_t a = next_event(), b = next_event();
+        point(nb_nodes, nb);
+        point(pme_nodes, pme);
+        if (e != cudaSuccess) break;
+        cudaEventRecord(a, stream_);
+        e = cudaGraphLaunch(ge, stream_);
+        cudaEventRecord(b, stream_);
+        steps.emplace_back(a, b);
+        launches_ += per_step;
+    }
+    const cudaError_t e_sync = cudaStreamSynchronize(stream_);
+    if (e == cudaSuccess) e = e_sync;
     cudaGraphExecDestroy(ge);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return check_cuda(e, "timed steps");
     float ms = 0.f;
     for (auto& pr : steps) {
         CK(cudaEventElapsedTime(&ms, pr.first, pr.second));
@@ -1750,7 +1854,7 @@ int Batch::step_timed(int n, long long flush_bytes, dmdgpu_timing* out) {
     }
     out->nonbonded_launches = static_cast<long long>(nb.size());
     int rc = sync_status();
-    out->kernel_launches = captured;
+    out->kernel_launches = per_step * n;
     return rc;
 }
 

@@ -730,6 +730,43 @@ __global__ void __launch_bounds__(256) k_nb_f64(Dev d) {
 
 }  // namespace
 
+namespace {
+const void* const kNbKernels[] = {
+    reinterpret_cast<const void*>(k_nb_f32<true, true, false>),
+    reinterpret_cast<const void*>(k_nb_f32<true, false, false>),
+    reinterpret_cast<const void*>(k_nb_f32<false, true, false>),
+    reinterpret_cast<const void*>(k_nb_f32<false, false, false>),
+    reinterpret_cast<const void*>(k_nb_f32<true, true, true>),
+    reinterpret_cast<const void*>(k_nb_f32<true, false, true>),
+    reinterpret_cast<const void*>(k_nb_f32<false, true, true>),
+    reinterpret_cast<const void*>(k_nb_f32<false, false, true>),
+    reinterpret_cast<const void*>(k_nb8_f32<true, true>),
+    reinterpret_cast<const void*>(k_nb8_f32<true, false>),
+    reinterpret_cast<const void*>(k_nb8_f32<false, true>),
+    reinterpret_cast<const void*>(k_nb8_f32<false, false>),
+    reinterpret_cast<const void*>(k_nb_f64<true>),
+    reinterpret_cast<const void*>(k_nb_f64<false>)};
+}  // namespace
+
+bool is_nonbonded_kernel(const void* f) {
+    for (const void* p : kNbKernels)
+        if (p == f) return true;
+    return false;
+}
+
+// The persistent pair kernel holds its SMs for the whole force evaluation.
+// With the default carveout the SMs it runs on are configured with little
+// more shared memory than its own blocks use, and the PME chain's cuFFT
+// kernels (4-16 KB of shared memory per block) cannot start beside it: on
+// water 30k they waited ~24 us for its last blocks.  A carveout of 60 % of the
+// unified L1 / shared memory as shared memory leaves room for them; the SPME
+// chain then runs during the pair kernel (step period 140 -> 128 us).
+void configure_nonbonded_kernels() {
+    for (const void* k : kNbKernels)
+        if (cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 60) != cudaSuccess)
+            cudaGetLastError();
+}
+
 void launch_nonbonded(const Dev& d, bool fp64, bool phys, int n_sm, int blocks_per_sm, int form,
                       cudaStream_t st, long long* nlaunch) {
     if (fp64) {

@@ -21,6 +21,12 @@ void launch_rebuild(const Dev& d, const int* bin_rep, int n_sm, cudaStream_t st,
 enum NbForm { NB_CHUNK32 = 0, NB_CLUSTER8 = 1 };
 void launch_nonbonded(const Dev& d, bool fp64, bool phys, int n_sm, int blocks_per_sm, int form,
                       cudaStream_t st, long long* nlaunch);
+// Whether a kernel function (cudaGraphKernelNodeGetParams' func) is one of the
+// pair kernels: the step graph gives every other kernel the higher priority.
+bool is_nonbonded_kernel(const void* func);
+// Per-device function attributes of the pair kernels (the shared-memory
+// carveout); called once per context before the first launch.
+void configure_nonbonded_kernels();
 
 // k_forces.cu
 // bonds, angles, dihedrals and the exclusion correction in one launch

@@ -28,6 +28,10 @@ def main():
                     choices=["water30k", "water750k", "argon4k", "batch256"])
     ap.add_argument("--plain", action="store_true",
                     help="run the steps without the profiler (a target for ncu)")
+    ap.add_argument("--timed", action="store_true",
+                    help="profile the timed path (step_timed: events around every step, pair "
+                         "kernel and PME chain, L2 flushed between steps) instead of run_n")
+    ap.add_argument("--flush-mb", type=int, default=512, help="L2 flush buffer of --timed")
     args = ap.parse_args()
     import torch
     from torch.profiler import ProfilerActivity, profile
@@ -64,9 +68,13 @@ def main():
             eng.positions
             return
         with profile(activities=[ProfilerActivity.CUDA]) as prof:
-            eng.run_n(args.steps)
+            if args.timed:
+                eng.step_timed(args.steps, args.flush_mb << 20)
+            else:
+                eng.run_n(args.steps)
             eng.positions
-    ev = [e for e in prof.events() if e.device_type.name == "CUDA" and "Memcpy" not in e.name]
+    ev = [e for e in prof.events() if e.device_type.name == "CUDA" and "Memcpy" not in e.name
+          and "Memset" not in e.name]
     ev.sort(key=lambda e: e.time_range.start)
 
     def short(name):

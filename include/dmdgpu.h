@@ -249,10 +249,13 @@ typedef struct dmdgpu_timing {
     int64_t kernel_launches;   /* this library's kernels executed during the n steps */
 } dmdgpu_timing;
 
-/* dmdgpu_step with device timing: the n steps are issued as one CUDA graph with
- * event records around every step and every non-bonded / PME launch.  When
- * l2_flush_bytes > 0 a buffer of that size is overwritten between steps (outside
- * the timed intervals) so each step starts with a cold L2. */
+/* dmdgpu_step with device timing: the step graph (the one dmdgpu_step launches,
+ * with event records around every non-bonded launch and every PME chain) is
+ * launched n times, each launch between two events on the context's stream.
+ * When l2_flush_bytes > 0 a buffer of that size is overwritten between steps
+ * (outside the timed intervals) so each step starts with a cold L2.  Not
+ * available for a REF Andersen thermostat (its random stream is drawn on the
+ * host every step). */
 int dmdgpu_step_timed(dmdgpu_ctx *ctx, int32_t n_steps, int64_t l2_flush_bytes, dmdgpu_timing *out);
 
 /* Trajectory frames, exported while the run continues.  Replaces the frame
