@@ -301,7 +301,7 @@ def run_single(args, R: Ranks):
     value = R.ws * n_atoms * args.steps / (step_ms / 1e3)
     launch = eng.launch_info()
     s = eng.scalars()
-    evals_per_step = t_mixed["nonbonded_launches"] / args.steps
+    evals_per_step = t_mixed["nonbonded_launches"] / max(t_mixed["sampled_steps"], 1)
     # accuracy is checked at the starting configuration, except on a perfect
     # lattice (argon FCC: every force vanishes by symmetry), where it is checked
     # at the configuration the timed run reached

@@ -93,7 +93,8 @@ FRAME_FN = C.CFUNCTYPE(None, C.POINTER(dmdgpu_frame), C.c_void_p)
 
 class dmdgpu_timing(C.Structure):
     _fields_ = [("step_ms", C.c_double), ("nonbonded_ms", C.c_double), ("pme_ms", C.c_double),
-                ("nonbonded_launches", C.c_int64), ("kernel_launches", C.c_int64)]
+                ("nonbonded_launches", C.c_int64), ("kernel_launches", C.c_int64),
+                ("sampled_steps", C.c_int64)]
 
 
 class dmdgpu_launch_info(C.Structure):

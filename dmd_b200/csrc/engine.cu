@@ -1709,17 +1709,17 @@ void Batch::record(cudaEvent_t e, cudaStream_t st) {
     else cudaEventRecord(e, st);
 }
 
-// n steps with device timing.  One step is captured as a graph with event
-// record nodes around every pair-kernel launch and every PME chain; the graph
-// is launched n times from the host, with the step's own events recorded on
-// the main stream between launches (and the optional L2 flush before each,
-// outside the events), and before each launch its event nodes are pointed at
-// fresh events (cudaGraphExecEventRecordNodeSetEvent), so every launch's
-// intervals are kept.  Capturing all n steps into one graph instead, with
-// their events, changes how the graph's branches are scheduled (measured on
-// water 30k: a step period of ~143 us against ~124 us for the step graph
-// that run_n launches); launching the one-step graph keeps the step as
-// run_n runs it.
+// n steps with device timing.  Every step is one launch of a one-step graph,
+// between two events recorded on the main stream (the optional L2 flush goes
+// before the first event).  Seven of every eight launches are of the step
+// graph run_n uses; every eighth is of a copy with event record nodes around
+// every pair-kernel launch and every PME chain, whose nodes are pointed at
+// fresh events before each launch (cudaGraphExecEventRecordNodeSetEvent), so
+// the pair kernel's and the PME chain's durations are those of the sampled
+// steps.  Event nodes on the critical path add a few microseconds to their
+// step, and capturing all n steps into one graph with their events changed
+// how the branches were scheduled (water 30k: a step period of ~143 us
+// against ~124 us for run_n's graph), hence one step graph and sampling.
 int Batch::step_timed(int n, long long flush_bytes, dmdgpu_timing* out) {
     st_fresh_ = false;  // device work follows: the host mirror is stale
     CK(cudaSetDevice(device_));
@@ -1825,11 +1825,14 @@ int Batch::step_timed(int n, long long flush_bytes, dmdgpu_timing* out) {
     for (int i = 0; i < n && e == cudaSuccess; ++i) {
         if (flush_buf_) cudaMemsetAsync(flush_buf_, i & 0xff, flush_bytes_, stream_);
         const cudaEvent_t a = next_event(), b = next_event();
-        point(nb_nodes, nb);
-        point(pme_nodes, pme);
-        if (e != cudaSuccess) break;
+        const bool sampled = (i % 8) == 7 || (n < 8 && i == n - 1);
+        if (sampled) {
+            point(nb_nodes, nb);
+            point(pme_nodes, pme);
+            if (e != cudaSuccess) break;
+        }
         cudaEventRecord(a, stream_);
-        e = cudaGraphLaunch(ge, stream_);
+        e = cudaGraphLaunch(sampled ? ge : graph_, stream_);
         cudaEventRecord(b, stream_);
         steps.emplace_back(a, b);
         launches_ += per_step;
@@ -1853,6 +1856,7 @@ int Batch::step_timed(int n, long long flush_bytes, dmdgpu_timing* out) {
         out->pme_ms += ms;
     }
     out->nonbonded_launches = static_cast<long long>(nb.size());
+    out->sampled_steps = static_cast<long long>(nb_nodes.empty() ? 0 : nb.size() / (nb_nodes.size() / 2));
     int rc = sync_status();
     out->kernel_launches = per_step * n;
     return rc;

@@ -243,10 +243,12 @@ int dmdgpu_get_launch_info(dmdgpu_ctx *ctx, dmdgpu_launch_info *out);
 /* Device timing of a run of steps. */
 typedef struct dmdgpu_timing {
     double step_ms;            /* summed device time of the n steps (flushes excluded) */
-    double nonbonded_ms;       /* summed device time of every non-bonded pair-kernel launch */
-    double pme_ms;             /* summed device time of the PME chains (spread .. gather) */
-    int64_t nonbonded_launches;
+    double nonbonded_ms;       /* summed device time of the non-bonded pair-kernel launches of
+                                  the sampled steps (every eighth step, and the last of a short run) */
+    double pme_ms;             /* summed device time of the sampled steps' PME chains (spread .. gather) */
+    int64_t nonbonded_launches; /* pair-kernel launches of the sampled steps */
     int64_t kernel_launches;   /* this library's kernels executed during the n steps */
+    int64_t sampled_steps;     /* steps whose pair-kernel and PME launches were timed */
 } dmdgpu_timing;
 
 /* dmdgpu_step with device timing: the step graph (the one dmdgpu_step launches,
