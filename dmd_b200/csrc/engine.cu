@@ -145,7 +145,10 @@ struct TuneChoice {
 std::mutex g_tune_mu;
 std::map<TuneKey, TuneChoice> g_tune;
 constexpr int kTuneSteps = 6;               // timed steps per candidate
-constexpr TuneChoice kTuneCand[] = {{NB_CLUSTER8, 1}, {NB_CLUSTER8, 2}, {NB_CHUNK32, 2}, {NB_CHUNK32, 3}};
+// (4 blocks per SM: the LJ-only chunk kernel only, which a table without
+// real-space Coulomb runs; for the others the launch takes 3)
+constexpr TuneChoice kTuneCand[] = {{NB_CLUSTER8, 1}, {NB_CLUSTER8, 2}, {NB_CHUNK32, 2}, {NB_CHUNK32, 3},
+                                    {NB_CHUNK32, 4}};
 
 // forced: the caller's dmdgpu_options.nb_form (0: the default form)
 TuneKey tune_key(int device, bool fp64, bool pme, long long n_atoms, int forced) {
@@ -785,6 +788,9 @@ int Batch::pack() {
         d.build_work = d.chunk_prefix + R + 2;
         d.nb_work_mi = d.chunk_prefix + R + 3;
         d.mi_split = any_narrow_ ? 1 : 0;
+        d.any_coul = 0;
+        for (int k = 0; k < R; ++k)
+            if (reps_[order_[k]]->rep.flags & F_COUL_REAL) d.any_coul = 1;
         d.grid_bar = A.alloc<unsigned>(2);
         d.build_prefix = A.alloc<int>(4 * (R + 1));
         if (uses_clusters()) {

@@ -324,8 +324,11 @@ constexpr int LJ_SMEM = 512;
 // per evaluation); launched, with its own work counter, only when the table
 // has such replicas (d.mi_split), in which case the main kernel leaves them to
 // it -- so their forms do not weigh on the main kernel's registers.
+// 80 registers (3 blocks of 256 threads per SM) with the real-space Ewald
+// forms; the LJ-only instantiation (PHYS = false: the REF profile, and PHYS
+// tables without real-space Coulomb) fits 64 (4 blocks per SM).
 template <bool PHYS, bool LJS, bool MIK>
-__global__ void __launch_bounds__(256, 3) k_nb_f32(Dev d) {
+__global__ void __launch_bounds__(256, PHYS ? 3 : 4) k_nb_f32(Dev d) {
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
     __shared__ ChunkStage s_stage[8];
@@ -774,9 +777,13 @@ void launch_nonbonded(const Dev& d, bool fp64, bool phys, int n_sm, int blocks_p
         else k_nb_f64<false><<<n_sm * 8, 256, 0, st>>>(d);
     } else {
         const bool ljs = d.n_lj <= LJ_SMEM;
+        // a table without real-space Coulomb runs the LJ-only instantiation
+        // (its replicas take the same LJ form in either)
+        phys = phys && d.any_coul;
+        const int max_bps = phys ? 3 : 4;
         // persistent: up to the blocks per SM its registers allow (2 for the
-        // cluster form, 3 for the chunk form); fewer leave room on every SM for
-        // the bonded / PME kernels running alongside
+        // cluster form, 3 for the chunk form, 4 for its LJ-only instantiation);
+        // fewer leave room on every SM for the bonded / PME kernels alongside
         const int bps = std::max(blocks_per_sm, 1);
         if (form == NB_CLUSTER8 && d.cl_j) {
             const int g = n_sm * std::min(bps, 2);
@@ -788,7 +795,7 @@ void launch_nonbonded(const Dev& d, bool fp64, bool phys, int n_sm, int blocks_p
                 else k_nb8_f32<false, false><<<g, 256, 0, st>>>(d);
             }
         } else {
-            const int g = n_sm * std::min(bps, 3);
+            const int g = n_sm * std::min(bps, max_bps);
             if (phys) {
                 if (ljs) k_nb_f32<true, true, false><<<g, 256, 0, st>>>(d);
                 else k_nb_f32<true, false, false><<<g, 256, 0, st>>>(d);
@@ -798,7 +805,7 @@ void launch_nonbonded(const Dev& d, bool fp64, bool phys, int n_sm, int blocks_p
             }
         }
         if (d.mi_split) {  // narrow-box replicas: their own kernel on the same stream
-            const int g = n_sm * std::min(bps, 3);
+            const int g = n_sm * std::min(bps, max_bps);
             if (phys) {
                 if (ljs) k_nb_f32<true, true, true><<<g, 256, 0, st>>>(d);
                 else k_nb_f32<true, false, true><<<g, 256, 0, st>>>(d);

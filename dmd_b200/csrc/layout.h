@@ -163,6 +163,7 @@ struct Dev {
     int* nb_work;                      // pair-kernel chunk counter (reset per evaluation)
     int* nb_work_mi;                   // the same for the narrow-box pair kernel
     int mi_split;                      // narrow-box replicas go to their own pair kernel
+    int any_coul;                      // some replica has real-space Coulomb (F_COUL_REAL)
     int* build_work;                   // list-build i-tile counter (reset per rebuild)
     int* build_prefix;                 // [3][n_rep + 1] prefixes of the rebuilding replicas'
                                        // atoms, sort cells and tiles

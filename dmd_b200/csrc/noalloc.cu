@@ -298,6 +298,7 @@ extern "C" int dmdgpu_nonbonded_noalloc(const dmdgpu_nb_params* p, const double*
     R.alpha = p->ewald_coeff;
     // a box narrower than twice the list cutoff: minimum image per evaluation
     d.mi_split = L * L < 4.0 * R.rc_list2 ? 1 : 0;
+    d.any_coul = (R.flags & F_COUL_REAL) ? 1 : 0;
     RepState S{};
     S.L = L;
     S.invL = 1.0 / L;
