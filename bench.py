@@ -276,7 +276,7 @@ def roofline(kind_bytes: float, kind_flop: float, nb_ms: float, clocks: dict, tr
 
 def run_single(args, R: Ranks):
     """One system per GPU: water30k, argon4k or water750k."""
-    from dmd_b200.core import Engine
+    from dmd_b200.core import Engine, default_skin
     spec = SINGLE[args.workload]
     w = spec["make"](R.rank)
     cfg = w.config()
@@ -355,7 +355,7 @@ def run_single(args, R: Ranks):
                         ", measured while the bonded + PME chain runs beside it on a second stream"
                         if spec["pme"] else ""))
     config = {"workload": f"{args.workload}", "n_atoms": n_atoms, "box_nm": cfg.box_size,
-              "cutoff_nm": cfg.lj_cutoff, "skin_nm": 0.1, "dt_ps": dt,
+              "cutoff_nm": cfg.lj_cutoff, "skin_nm": default_skin(), "dt_ps": dt,
               "ensemble": spec["ensemble"], "profile": "phys",
               "force_evaluations_per_step": round(evals_per_step, 3),
               "l2": "flushed between timed steps (256 MiB overwrite outside the step events)",
