@@ -186,7 +186,8 @@ SINGLE = {
     "water30k": dict(make=water30k, kind="water", pme=64, ensemble="nose-hoover NVT 300 K",
                      desc="seeded jittered-lattice water, random orientations"),
     "argon4k": dict(make=argon4k, kind="argon", pme=None, ensemble="NVE (velocities at 120 K)",
-                    desc="FCC argon lattice, Maxwell-Boltzmann velocities from a seed"),
+                    desc="FCC argon lattice, Maxwell-Boltzmann velocities from a seed",
+                    skin=0.1),  # the configuration states a 0.1 nm skin
     "water750k": dict(make=water750k, kind="water", pme=192,
                       ensemble="Berendsen T 300 K + Berendsen P 1 bar (NPT)",
                       desc="seeded jittered-lattice water, random orientations"),
@@ -283,8 +284,10 @@ def run_single(args, R: Ranks):
     n_atoms = w.n_atoms
     dt = cfg.dt
 
+    skin = spec.get("skin")  # None: the library's default
+
     def timed(precision):
-        eng = Engine(cfg, precision=precision, profile="phys", device=R.local)
+        eng = Engine(cfg, precision=precision, profile="phys", device=R.local, skin=skin)
         eng.run_n(args.warmup)
         eng.positions  # sync
         R.barrier()
@@ -312,7 +315,7 @@ def run_single(args, R: Ranks):
 
     # end to end through the public API: one run_n(1) call per MD step plus the
     # potential-energy read, host buffers, wall clock
-    eng_e = Engine(cfg, precision="mixed", profile="phys", device=R.local)
+    eng_e = Engine(cfg, precision="mixed", profile="phys", device=R.local, skin=skin)
     eng_e.run_n(args.warmup)
     _ = eng_e.potential_energy
     R.barrier()
@@ -326,14 +329,14 @@ def run_single(args, R: Ranks):
 
     if R.rank != 0:
         return None
-    drift = nve_drift(cfg, R.local, args.drift_steps) if spec["kind"] == "argon" else None
+    drift = nve_drift(cfg, R.local, args.drift_steps, skin) if spec["kind"] == "argon" else None
     # accuracy at the starting configuration against the FP64 CPU oracle
     from oracle.oracle import Oracle
     F_o, e_o = Oracle().forces(cfg, "phys", pos=acc_pos)
     acc = {"configuration": "start" if acc_pos is None else
            f"after the {args.warmup + args.steps}-step timed run"}
     for prec in ("mixed", "fp64"):
-        e0 = Engine(cfg, precision=prec, profile="phys", device=R.local)
+        e0 = Engine(cfg, precision=prec, profile="phys", device=R.local, skin=skin)
         if acc_pos is not None:
             e0.set_positions(acc_pos)
         F, e = e0.compute_forces()
@@ -355,7 +358,8 @@ def run_single(args, R: Ranks):
                         ", measured while the bonded + PME chain runs beside it on a second stream"
                         if spec["pme"] else ""))
     config = {"workload": f"{args.workload}", "n_atoms": n_atoms, "box_nm": cfg.box_size,
-              "cutoff_nm": cfg.lj_cutoff, "skin_nm": default_skin(), "dt_ps": dt,
+              "cutoff_nm": cfg.lj_cutoff, "skin_nm": skin if skin is not None else default_skin(),
+              "dt_ps": dt,
               "ensemble": spec["ensemble"], "profile": "phys",
               "force_evaluations_per_step": round(evals_per_step, 3),
               "l2": "flushed between timed steps (256 MiB overwrite outside the step events)",
@@ -392,7 +396,7 @@ def run_single(args, R: Ranks):
     }
 
 
-def nve_drift(cfg, device: int, steps: int) -> dict:
+def nve_drift(cfg, device: int, steps: int, skin=None) -> dict:
     """NVE energy drift max_t |E(t) - E(0)| / |E(0)| over `steps` steps
     (tests/integration/test_argon_nve.cpp:150-171 of the reference), E = the
     potential energy plus sum(m v^2)/2 read after every step: the GPU paths
@@ -418,7 +422,7 @@ def nve_drift(cfg, device: int, steps: int) -> dict:
                      "forces inside it); the criterion of the reference's "
                      "tests/integration/test_argon_nve.cpp"}
     for prec, prof in (("mixed", "phys"), ("fp64", "phys"), ("mixed", "ref")):
-        eng = Engine(cfg, precision=prec, profile=prof, device=device)
+        eng = Engine(cfg, precision=prec, profile=prof, device=device, skin=skin)
         out[f"gpu_{prec}_{prof}"] = run(lambda: eng.run_n(1), lambda: eng.velocities,
                                         lambda: eng.potential_energy)
         eng.close()
