@@ -133,9 +133,10 @@ void sort_grid(int n, double L, int& nvx, int& nvz) {
 // size with every admission; nearby sizes share a shape).
 namespace {
 struct TuneKey {
-    int device, fp64, pme, bucket, forced;
+    int device, fp64, pme, bucket, forced, dens;
     bool operator<(const TuneKey& o) const {
-        return std::tie(device, fp64, pme, bucket, forced) < std::tie(o.device, o.fp64, o.pme, o.bucket, o.forced);
+        return std::tie(device, fp64, pme, bucket, forced, dens) <
+               std::tie(o.device, o.fp64, o.pme, o.bucket, o.forced, o.dens);
     }
 };
 // A choice: the pair-kernel form (NbForm) and its blocks of 256 threads per SM.
@@ -151,10 +152,13 @@ constexpr TuneChoice kTuneCand[] = {{NB_CLUSTER8, 1}, {NB_CLUSTER8, 2}, {NB_CHUN
                                     {NB_CHUNK32, 4}};
 
 // forced: the caller's dmdgpu_options.nb_form (0: the default form)
-TuneKey tune_key(int device, bool fp64, bool pme, long long n_atoms, int forced) {
+// bucket: atom count in powers of four; dens: the table's atoms per nm^3 in
+// powers of two (LJ fluids ~16-22, water ~100)
+TuneKey tune_key(int device, bool fp64, bool pme, long long n_atoms, int forced, double density) {
     int b = 0;
     while ((1LL << (2 * b + 2)) <= n_atoms) ++b;
-    return TuneKey{device, fp64 ? 1 : 0, pme ? 1 : 0, b, forced};
+    const int dens = density > 0.0 ? static_cast<int>(std::floor(std::log2(density))) : 0;
+    return TuneKey{device, fp64 ? 1 : 0, pme ? 1 : 0, b, forced, dens};
 }
 
 // DMDGPU_NB_* of the options -> NbForm, or -1 for the default form
@@ -788,6 +792,14 @@ int Batch::pack() {
         d.build_work = d.chunk_prefix + R + 2;
         d.nb_work_mi = d.chunk_prefix + R + 3;
         d.mi_split = any_narrow_ ? 1 : 0;
+        {
+            double vol = 0.0;
+            for (int k = 0; k < R; ++k) {
+                const double L = reps_[order_[k]]->sys.box;
+                vol += L * L * L;
+            }
+            density_ = vol > 0.0 ? static_cast<double>(n_atoms) / vol : 0.0;
+        }
         d.any_coul = 0;
         for (int k = 0; k < R; ++k)
             if (reps_[order_[k]]->rep.flags & F_COUL_REAL) d.any_coul = 1;
@@ -1167,7 +1179,7 @@ int Batch::pack() {
     }
     {
         std::lock_guard<std::mutex> lk(g_tune_mu);
-        const TuneKey key = tune_key(device_, fp64_, any_pme_, dev_.n_atoms, opt_.nb_form);
+        const TuneKey key = tune_key(device_, fp64_, any_pme_, dev_.n_atoms, opt_.nb_form, density_);
         auto it = g_tune.find(key);
         if (it == g_tune.end()) {
             // a table of a size not tuned yet takes the shape tuned for the
@@ -1178,7 +1190,7 @@ int Batch::pack() {
                 const TuneKey& k = jt->first;
                 if (k.device != key.device || k.fp64 != key.fp64 || k.pme != key.pme || k.forced != key.forced)
                     continue;
-                const int dist = std::abs(k.bucket - key.bucket);
+                const int dist = 4 * std::abs(k.dens - key.dens) + std::abs(k.bucket - key.bucket);
                 if (dist < best) {
                     best = dist;
                     it = jt;
@@ -1460,7 +1472,7 @@ int Batch::autotune(int max_steps, int* used) {
     nb_blocks_per_sm_ = best.bps;
     tuned_ = true;
     std::lock_guard<std::mutex> lk(g_tune_mu);
-    g_tune[tune_key(device_, fp64_, any_pme_, dev_.n_atoms, opt_.nb_form)] = best;
+    g_tune[tune_key(device_, fp64_, any_pme_, dev_.n_atoms, opt_.nb_form, density_)] = best;
     return DMDGPU_OK;
 }
 

@@ -199,6 +199,7 @@ class Batch {
     bool need_eval1_ = true;
     int nb_blocks_per_sm_ = 2;  // pair-kernel launch shape (autotuned)
     int prio_lo_ = 0, prio_hi_ = 0;  // stream priority range
+    double density_ = 0.0;           // table atoms per nm^3 (autotuner cache key)
     void set_node_priorities(cudaGraph_t g);
     int nb_form_ = 1;           // pair-kernel form (NbForm; autotuned)
     bool tuned_ = false;
