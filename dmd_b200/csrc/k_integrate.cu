@@ -466,69 +466,75 @@ __global__ void k_replica_update(Dev d) {
     }
     block_sum4(v, sh);
     if (threadIdx.x != 0) return;
+    // one thread from here: the replica's records are copied to registers at
+    // once (independent loads) and written back at the end, instead of a chain
+    // of dependent global reads and writes
+    RepState st = *s;
+    const Rep Rr = R;
     const double ke = v[0], w = v[1];
-    s->e_recip = v[2];
-    s->vir_recip = v[3];
+    st.e_recip = v[2];
+    st.vir_recip = v[3];
     // end of the step's second evaluation (k_eval_end's work, at the box it used)
-    if (s->eval) {
-        if (!(R.flags & F_PHYS) && (R.flags & F_LJ)) s->lj_counter += 1;
-        s->have_forces = 1;
-        if (R.flags & F_PME) s->green_L = s->L;
+    if (st.eval) {
+        if (!(Rr.flags & F_PHYS) && (Rr.flags & F_LJ)) st.lj_counter += 1;
+        st.have_forces = 1;
+        if (Rr.flags & F_PME) st.green_L = st.L;
     }
-    const double n = static_cast<double>(R.n_atoms);
-    const double dt = R.dt;
-    auto temp = [&](double ek) { return R.n_atoms < 2 ? 0.0 : 2.0 * ek / ((3.0 * n - 3.0) * KB); };
+    const double n = static_cast<double>(Rr.n_atoms);
+    const double dt = Rr.dt;
+    auto temp = [&](double ek) { return Rr.n_atoms < 2 ? 0.0 : 2.0 * ek / ((3.0 * n - 3.0) * KB); };
     double lam = 1.0;
-    if (R.thermostat == 1) {
-        if (R.t_tau > 0.0 && ke > 0.0) {
+    if (Rr.thermostat == 1) {
+        if (Rr.t_tau > 0.0 && ke > 0.0) {
             const double T = temp(ke);
-            const double l = sqrt(1.0 + dt / R.t_tau * (R.t_temp / T - 1.0));
+            const double l = sqrt(1.0 + dt / Rr.t_tau * (Rr.t_temp / T - 1.0));
             if (!(l <= 0.0)) lam = l;
         }
-    } else if (R.thermostat == 2) {
+    } else if (Rr.thermostat == 2) {
         const double T = temp(ke);
-        s->zeta += 0.5 * dt * KB * (T - R.t_temp) / R.nh_Q;
-        lam = exp(-s->zeta * 0.5 * dt);
-    } else if (R.thermostat == 3) {
-        if (R.t_freq * dt > 0.0) s->andersen_calls += 1;
+        st.zeta += 0.5 * dt * KB * (T - Rr.t_temp) / Rr.nh_Q;
+        lam = exp(-st.zeta * 0.5 * dt);
+    } else if (Rr.thermostat == 3) {
+        if (Rr.t_freq * dt > 0.0) st.andersen_calls += 1;
     }
-    s->vscale = lam;
+    st.vscale = lam;
     const double ke_after = ke * lam * lam;
-    s->ke = ke_after;
-    const double L = s->L;
+    st.ke = ke_after;
+    const double L = st.L;
     const double V = L * (L * L);
     double W;
-    if (R.flags & F_PHYS) W = from_fix(s->e_acc[E_VIR], ESCALE) + s->vir_recip;
+    if (Rr.flags & F_PHYS) W = from_fix(st.e_acc[E_VIR], ESCALE) + st.vir_recip;
     else W = w;
-    s->virial = W;
-    s->pressure = (V <= 0.0) ? 0.0 : (2.0 * ke_after + W) / (3.0 * V);
-    if (R.barostat == 2 && V > 0.0) {
+    st.virial = W;
+    st.pressure = (V <= 0.0) ? 0.0 : (2.0 * ke_after + W) / (3.0 * V);
+    if (Rr.barostat == 2 && V > 0.0) {
         // AndersenBarostat::apply (andersen_barostat.cpp:20-45), ref profile: half a
         // step of piston velocity from 3V (P - P0) / W (P0 in the reference's units),
         // positions and box scale by exp(eps_dot dt) (positions in k_apply_scale),
         // then the second half step with the same forcing
-        const double forcing = 3.0 * V * (s->pressure - R.b_pressure) / R.piston_W;
-        s->eps_dot = s->eps_dot + 0.5 * dt * forcing;
-        const double sc = exp(s->eps_dot * dt);
-        s->pscale = sc;
-        s->L = L * sc;
-        s->invL = 1.0 / s->L;
-        s->eps_dot = s->eps_dot + 0.5 * dt * forcing;
+        const double forcing = 3.0 * V * (st.pressure - Rr.b_pressure) / Rr.piston_W;
+        st.eps_dot = st.eps_dot + 0.5 * dt * forcing;
+        const double sc = exp(st.eps_dot * dt);
+        st.pscale = sc;
+        st.L = L * sc;
+        st.invL = 1.0 / st.L;
+        st.eps_dot = st.eps_dot + 0.5 * dt * forcing;
     }
-    if (R.barostat == 1 && R.b_tau > 0.0 && V > 0.0) {
+    if (Rr.barostat == 1 && Rr.b_tau > 0.0 && V > 0.0) {
         double mu;
-        if (R.flags & F_PHYS) mu = 1.0 - (dt / R.b_tau) * R.b_compress * (R.b_pressure - s->pressure / BAR);
-        else mu = 1.0 - (dt / R.b_tau) * (R.b_compress / BAR) * (R.b_pressure - s->pressure);
+        if (Rr.flags & F_PHYS) mu = 1.0 - (dt / Rr.b_tau) * Rr.b_compress * (Rr.b_pressure - st.pressure / BAR);
+        else mu = 1.0 - (dt / Rr.b_tau) * (Rr.b_compress / BAR) * (Rr.b_pressure - st.pressure);
         if (mu <= 0.0) mu = 0.0;
         const double sc = cbrt(mu);
-        s->pscale = sc;
-        if (!(R.flags & F_PHYS)) {  // REF: positions and box scale now (k_apply_scale)
-            s->L = L * sc;
-            s->invL = 1.0 / s->L;
+        st.pscale = sc;
+        if (!(Rr.flags & F_PHYS)) {  // REF: positions and box scale now (k_apply_scale)
+            st.L = L * sc;
+            st.invL = 1.0 / st.L;
         }
     }
-    s->step += 1;
-    s->time += dt;
+    st.step += 1;
+    st.time += dt;
+    *s = st;
 }
 
 // BerendsenBarostat position scaling (berendsen_barostat.cpp:60-65).
