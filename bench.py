@@ -61,9 +61,9 @@ CPU_MAX_ATOMS = 100_000             # above this the reference's O(N^2) list bui
 # Argon (rc 1.0 nm, 21.0 atoms/nm^3, 44 half-neighbours): 241 B, 1,675 FLOP.
 PAIR_WORK = {"water": (650.0, 14690.0), "argon": (241.0, 1675.0)}
 # DRAM bytes (read + write) of one pair-kernel launch, from the ncu captures in
-# profiles/ (water 30k: 7.05 MB read, 0 written -- the working set stays in L2;
-# water 750k: 177.3 + 13.1 MB; the 256-replica batch: 214.0 + 35.0 MB).
-PAIR_DRAM_BYTES = {"water30k": 7.05e6, "water750k": 190.4e6, "batch256": 249.0e6}
+# profiles/ (water 30k: 7.62 MB read, 0 written -- the working set stays in L2;
+# water 750k: 190.0 + 13.9 MB; the 256-replica batch: 217.3 + 34.0 MB).
+PAIR_DRAM_BYTES = {"water30k": 7.62e6, "water750k": 203.9e6, "batch256": 251.3e6}
 
 
 def lj_pair_work(n: int, box: float, rc: float, flop_per_pair: float = 38.0):
