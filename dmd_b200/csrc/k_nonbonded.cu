@@ -360,8 +360,28 @@ __global__ void __launch_bounds__(256, PHYS ? 3 : 4) k_nb_f32(Dev d) {
         // may become, that narrow)
         const bool mi = 4.0 * R.rc_list2 > s->L * s->L;
         if (!s->eval || MIK != (mi && d.mi_split)) {
-            // a replica this kernel skips: move the counter past its chunks
-            if (lane == 0) atomicMax(counter, d.chunk_prefix[r + 1]);
+            // a replica this kernel skips: move the counter past its chunks.
+            // The minimum-image kernel evaluates few replicas of a table, so it
+            // moves the counter straight to the next one it evaluates (lanes
+            // test 32 replicas at a time) instead of one replica per claim.
+            int next = r + 1;
+            if (MIK) {
+                next = d.n_rep;
+                for (int b = r + 1; b < d.n_rep; b += 32) {
+                    const int q = b + lane;
+                    bool take = false;
+                    if (q < d.n_rep) {
+                        const RepState* sq = d.st + q;
+                        take = sq->eval && 4.0 * d.rep[q].rc_list2 > sq->L * sq->L;
+                    }
+                    const unsigned m = __ballot_sync(FULL, take);
+                    if (m) {
+                        next = b + __ffs(m) - 1;
+                        break;
+                    }
+                }
+            }
+            if (lane == 0) atomicMax(counter, d.chunk_prefix[next]);
             continue;
         }
         const int c = R.chunk_begin + (w - d.chunk_prefix[r]);
