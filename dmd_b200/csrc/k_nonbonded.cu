@@ -146,6 +146,7 @@ __device__ __forceinline__ void nb_chunk(const Dev& d, const Rep& R, RepState* s
     const int si = 32 * I + lane;
     const float4 xi = d.xq32[si];
     const int ti = d.type_s[si];
+    const int ai = d.atom_of_slot[si];  // loaded with the chunk's other inputs, used at its end
     const uint32_t e = d.chunk_j[32 * c + lane];
     const uint32_t mk = d.chunk_mask[32 * c + lane];
     const int js = static_cast<int>(e & 0x03FFFFFFu);
@@ -262,7 +263,6 @@ __device__ __forceinline__ void nb_chunk(const Dev& d, const Rep& R, RepState* s
         rm >>= 8;
     }
     // after 32 rounds lane l holds the forces of entry l again
-    const int ai = d.atom_of_slot[si];
     while (band) {  // pairs at a cutoff (rare): FP64 reference membership
         const int k = __ffs(band) - 1;
         band &= band - 1;
